@@ -1,0 +1,139 @@
+/*
+ * qe_b200 — C ABI of the B200 Kohn–Sham H|psi> / Davidson hot path.
+ *
+ * Every entry point takes plain pointers, sizes and a CUDA stream handle
+ * (passed as void*; NULL = legacy default stream) and returns an int status:
+ * 0 on success, negative on failure (see QEB_E* below; qeb_last_error()
+ * returns a message for the calling thread).  Nothing throws across the ABI.
+ * Device pointers are caller-owned; no call keeps a device allocation alive
+ * beyond its plan object.  Complex values are interleaved (re, im) pairs
+ * (complex128 = 16 bytes, complex64 = 8 bytes).  Matrices are column-major
+ * ("Fortran order") with an explicit leading dimension, as qepy-pw's
+ * Davidson stores them (qepy_pw/diagonalization.py:632-635).
+ *
+ * Each declaration names the reference interface it replaces, as
+ * path:line inside the sjhong6230/QE_python (qepy-pw 1.0.2) tree.
+ */
+#ifndef QE_B200_H
+#define QE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QEB_ABI_VERSION 1
+
+/* precisions of a local plan */
+#define QEB_F64 0 /* complex128 psi, float64 V(r) and kinetic */
+#define QEB_F32 1 /* complex64 psi, float32 V(r) and kinetic */
+
+/* status codes */
+#define QEB_STATUS_OK 0
+#define QEB_STATUS_EINVAL -1      /* bad shape, pointer, stride or alignment */
+#define QEB_STATUS_EUNSUPPORTED -2 /* size outside what the kernels handle */
+#define QEB_STATUS_ECUDA -3       /* CUDA runtime or launch error */
+#define QEB_STATUS_ESCRATCH -4    /* caller scratch smaller than required */
+#define QEB_STATUS_ENOPLAN -5     /* null plan */
+
+/* Message of the last failed call on this thread. */
+const char* qeb_last_error(void);
+/* QEB_ABI_VERSION of the loaded library. */
+int qeb_version(void);
+
+/* ------------------------------------------------------------------------
+ * Local potential operator on the FFT grid (sticks / planes).
+ * ---------------------------------------------------------------------- */
+typedef struct qeb_local_plan qeb_local_plan;
+
+/* Build the device index maps of one plane-wave basis on an (nx, ny, nz)
+ * grid from its z-major slots z*nx*ny + x*ny + y (host int64 array, npw).
+ * Replaces the per-k serial maps of LocalPotentialWorkspace.__init__
+ * (qepy_pw/basis.py:510-555: z_major_slots, serial_stick_positions) and the
+ * FFTW plan pair NativeFFTWPlan (qepy_pw/_native_fft.pyx:1973-2086).
+ * The grid lengths must be 2-3-5 smooth (qepy_pw/basis.py:27-37). */
+int qeb_local_plan_create(qeb_local_plan** plan, int nx, int ny, int nz, int64_t npw,
+                          const int64_t* z_major_slots, int precision);
+int qeb_local_plan_destroy(qeb_local_plan* plan);
+/* info[0..7] = nx, ny, nz, npw, sticks, active y rows, precision, device. */
+int qeb_local_plan_info(const qeb_local_plan* plan, int64_t* info, int n);
+/* Bytes of caller scratch needed for nbands (the stick buffer
+ * nbands*nz*sticks complex values); the role of the grid scratch argument
+ * of apply_serial_spatial (qepy_pw/_native_fft.pyx:2458-2471). */
+int64_t qeb_local_scratch_bytes(const qeb_local_plan* plan, int64_t nbands);
+
+/* out[:, b] = FFT^-( V . FFT^+(psi[:, b]) )[slots] / N_r + kinetic * psi[:, b]
+ * for b < nbands.  potential is the native (nz, nx, ny) real grid; kinetic
+ * may be NULL.  Replaces apply_serial_spatial / apply_serial
+ * (qepy_pw/_native_fft.pyx:2458-2534, 2338-2455; operator at :58-135). */
+int qeb_apply_local(const qeb_local_plan* plan, void* scratch, int64_t scratch_bytes,
+                    const void* psi, int64_t ld_psi, int64_t nbands,
+                    const void* potential_native, const void* kinetic, void* out,
+                    int64_t ld_out, void* stream);
+
+/* density[(x*ny + y)*nz + z] += sum_b weights[b] |FFT^+(psi[:, b])(x,y,z)|^2
+ * (float64 accumulation; weights is a device float64 array of nbands).
+ * Replaces accumulate_density_serial(_spatial)
+ * (qepy_pw/_native_fft.pyx:2537-2648; operator at :137-193). */
+int qeb_accumulate_density(const qeb_local_plan* plan, void* scratch, int64_t scratch_bytes,
+                           const void* psi, int64_t ld_psi, int64_t nbands,
+                           const double* weights, double* density, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Complex GEMM: C = alpha * op(A) * B + beta * C, column-major.
+ * op(A) = A (QEB_OP_N; A is M x K) or A^H (QEB_OP_C; A is K x M).
+ * alpha, beta: host pointers to {re, im} doubles.  With QEB_OP_C the long
+ * K dimension is split across blocks when `scratch` holds at least
+ * qeb_zgemm_scratch_bytes(); partial tiles are reduced in a fixed order.
+ * qeb_zgemm: complex128; qeb_cgemm: complex64 with FP32 FMA.
+ * Replace projector_overlaps (ZGEMM ConjTrans, qepy_pw/_native_fft.pyx
+ * :694-731), add_projector_product (ZGEMM beta=1, :782-836), the Davidson
+ * reduced matrices V^H HV, V^H V and Ritz products V c, HV c
+ * (qepy_pw/diagonalization.py:658-726) and coupling @ overlaps (:348).
+ * ---------------------------------------------------------------------- */
+#define QEB_OP_N 0
+#define QEB_OP_C 1
+int64_t qeb_zgemm_scratch_bytes(int opa, int M, int N, int K, int precision);
+int qeb_zgemm(int opa, int M, int N, int K, const double* alpha, const void* A, int64_t lda,
+              const void* B, int64_t ldb, const double* beta, void* C, int64_t ldc,
+              void* scratch, int64_t scratch_bytes, void* stream);
+int qeb_cgemm(int opa, int M, int N, int K, const double* alpha, const void* A, int64_t lda,
+              const void* B, int64_t ldb, const double* beta, void* C, int64_t ldc,
+              void* scratch, int64_t scratch_bytes, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Davidson column kernels (precision QEB_F64 / QEB_F32 selects the vector
+ * type; reductions accumulate in FP64; eigenvalues, diagonals and norms
+ * are device float64 arrays).
+ * ---------------------------------------------------------------------- */
+/* out[b] = sum_g |v[g,b]|^2 — column_squared_norms (qepy_pw/_native_fft.pyx:1153-1190) */
+int qeb_column_squared_norms(int precision, int64_t rows, int64_t cols, const void* v,
+                             int64_t ld, double* out, void* stream);
+/* out[b] = sum_g diag[g] |v[g,b]|^2 — column_diagonal_expectations (:1294-1343) */
+int qeb_column_diagonal_expectations(int precision, int64_t rows, int64_t cols, const void* v,
+                                     int64_t ld, const double* diag, double* out, void* stream);
+/* out[b] = sum_g conj(l[g,b]) r[g,b] as {re, im} — column_inner_products (:1237-1291) */
+int qeb_column_inner_products(int precision, int64_t rows, int64_t cols, const void* left,
+                              int64_t ldl, const void* right, int64_t ldr, double* out_complex,
+                              void* stream);
+/* QE g_psi: x = 2(diag_g - e_b), d = (1 + x + sqrt(1 + (x-1)^2))/2,
+ * out = 2 r / d — qe_precondition (:852-899) */
+int qeb_precondition(int precision, int64_t rows, int64_t cols, const void* residuals,
+                     int64_t ldr, const double* eigenvalues, const double* diagonal, void* out,
+                     int64_t ldo, void* stream);
+/* out[:, j] = v[:, sel[j]] / sqrt(norms2[sel[j]]) (sel may be NULL = identity)
+ * — normalize_selected_columns (:1495-1530) */
+int qeb_normalize_columns(int precision, int64_t rows, int64_t cols, const void* v, int64_t ldv,
+                          const double* norms2, const int64_t* selected, void* out, int64_t ldo,
+                          void* stream);
+/* residual[:, b] -= energies[b] v[:, b] — subtract_band_energies (:1193-1234) */
+int qeb_subtract_band_energies(int precision, int64_t rows, int64_t cols, void* residual,
+                               int64_t ldr, const void* v, int64_t ldv, const double* energies,
+                               void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QE_B200_H */

@@ -1,0 +1,558 @@
+// Band-batched local H|psi> and density accumulation on the FFT grid.
+//
+// Restates, for one GPU, the operator of qepy_pw/_native_fft.pyx
+// qepy_apply_serial_spatial (:58-135) and apply_serial (:2338-2455):
+//   Hpsi[g, b] = FFT^-( V(r) * FFT^+(psi[:, b]) )[slot_g] / N_r + T_g psi[g, b]
+// factorised the way QE/FFTXlib (and the reference's spatial path) do it:
+//   pass A : per occupied (x, y) stick, gather psi(G) and inverse-FFT along z;
+//   pass B : per (z plane, band) inverse 2-D FFT, multiply by V(x, y, z),
+//            forward 2-D FFT, keep only the stick columns;
+//   pass C : per stick forward FFT along z, gather, scale by 1/N_r and add the
+//            kinetic term.
+// Inside pass B the 2-D transform is pruned: the x transforms run only on the
+// "active" y rows (those containing sticks), the y transforms on every x
+// column; both directions keep the plane in shared memory.
+//
+// HBM layout:
+//   psi, out : column-major (npw, nbands), leading dimension ld (complex T)
+//   V        : native (nz, nx, ny) real T      (reference "native layout")
+//   sticks   : scratch (nbands, nz, nst) complex T
+//   density  : C-order (nx, ny, nz) float64 (reference serial layout)
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include "qeb_common.cuh"
+#include "../../include/qe_b200.h"
+
+using qeb::C2;
+using qeb::FftDesc;
+
+struct qeb_local_plan {
+  int nx, ny, nz;
+  int64_t npw;
+  int nst;       // occupied (x, y) sticks
+  int nay;       // active y rows
+  int nx_pad;    // shared-memory row stride of the active-row plane
+  int ny_pad;    // shared-memory stride of the column lines
+  int nz_pad;    // shared-memory stride of the stick lines
+  int precision; // QEB_F64 or QEB_F32
+  int device;
+  FftDesc fx, fy, fz;
+  // device arrays (plan-owned)
+  int32_t* entry_g;      // npw: plane-wave row, CSR-ordered by (stick, z)
+  int32_t* entry_z;      // npw: z slot
+  int32_t* entry_stick;  // npw: stick index
+  int32_t* stick_off;    // nst + 1
+  int32_t* stick_pos;    // nst: ay * nx_pad + x (shared-memory plane position)
+  int32_t* ay_to_y;      // nay
+  int32_t* y_to_ay;      // ny (-1 when the row holds no stick)
+  void* tw;              // forward twiddles: nx, then ny, then nz entries (complex T)
+};
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kSticksPerBlock = 32;  // pass A/C
+constexpr int kRowBatch = 16;        // pass B column batch
+
+inline int odd_pad(int n) { return (n % 2 == 0) ? n + 1 : n; }
+
+template <typename T>
+size_t pass_b_smem(const qeb_local_plan* p) {
+  return sizeof(C2<T>) * ((size_t)p->nay * p->nx_pad + (size_t)kRowBatch * p->ny_pad +
+                          (size_t)p->nx + p->ny);
+}
+
+template <typename T>
+size_t pass_ac_smem(const qeb_local_plan* p) {
+  return sizeof(C2<T>) * ((size_t)kSticksPerBlock * p->nz_pad + p->nz);
+}
+
+// ---------------------------------------------------------------------------
+// Pass A: scatter psi(G) into z lines of the occupied sticks, inverse FFT.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) pass_a_kernel(
+    const C2<T>* __restrict__ psi, int64_t ld, int nst, int nz, int nz_pad, FftDesc fz,
+    const int32_t* __restrict__ entry_g, const int32_t* __restrict__ entry_z,
+    const int32_t* __restrict__ entry_stick, const int32_t* __restrict__ stick_off,
+    const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2<T>* lines = reinterpret_cast<C2<T>*>(smem_raw);
+  C2<T>* tw = lines + kSticksPerBlock * nz_pad;
+  const int s0 = blockIdx.x * kSticksPerBlock;
+  const int nsl = min(kSticksPerBlock, nst - s0);
+  const int64_t band = blockIdx.y;
+  for (int i = threadIdx.x; i < nz; i += blockDim.x) tw[i] = tw_z[i];
+  for (int i = threadIdx.x; i < kSticksPerBlock * nz_pad; i += blockDim.x) lines[i] = qeb::mk<T>(0, 0);
+  __syncthreads();
+  const int e0 = stick_off[s0], e1 = stick_off[s0 + nsl];
+  const C2<T>* col = psi + band * ld;
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    lines[(entry_stick[e] - s0) * nz_pad + entry_z[e]] = col[entry_g[e]];
+  }
+  __syncthreads();
+  qeb::fft_lines<T, 2>(lines, nsl, nz_pad, 1, fz, tw, true);
+  C2<T>* out = sticks + band * (int64_t)nz * nst;
+  for (int i = threadIdx.x; i < nz * nsl; i += blockDim.x) {
+    const int z = i / nsl, sl = i - z * nsl;
+    out[(int64_t)z * nst + s0 + sl] = lines[sl * nz_pad + z];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass C: forward FFT of the stick lines along z, gather, 1/N and T*psi.
+template <typename T>
+__global__ void __launch_bounds__(kThreads) pass_c_kernel(
+    const C2<T>* __restrict__ sticks, int nst, int nz, int nz_pad, FftDesc fz,
+    const int32_t* __restrict__ entry_g, const int32_t* __restrict__ entry_z,
+    const int32_t* __restrict__ entry_stick, const int32_t* __restrict__ stick_off,
+    const C2<T>* __restrict__ tw_z, const C2<T>* __restrict__ psi, int64_t ld,
+    const T* __restrict__ kinetic, T inv_n, C2<T>* __restrict__ out, int64_t ldo) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2<T>* lines = reinterpret_cast<C2<T>*>(smem_raw);
+  C2<T>* tw = lines + kSticksPerBlock * nz_pad;
+  const int s0 = blockIdx.x * kSticksPerBlock;
+  const int nsl = min(kSticksPerBlock, nst - s0);
+  const int64_t band = blockIdx.y;
+  for (int i = threadIdx.x; i < nz; i += blockDim.x) tw[i] = tw_z[i];
+  const C2<T>* in = sticks + band * (int64_t)nz * nst;
+  for (int i = threadIdx.x; i < nz * nsl; i += blockDim.x) {
+    const int z = i / nsl, sl = i - z * nsl;
+    lines[sl * nz_pad + z] = in[(int64_t)z * nst + s0 + sl];
+  }
+  __syncthreads();
+  qeb::fft_lines<T, 2>(lines, nsl, nz_pad, 1, fz, tw, false);
+  const int e0 = stick_off[s0], e1 = stick_off[s0 + nsl];
+  const C2<T>* col = psi + band * ld;
+  C2<T>* dst = out + band * ldo;
+  for (int e = e0 + threadIdx.x; e < e1; e += blockDim.x) {
+    const int g = entry_g[e];
+    C2<T> v = qeb::scale(lines[(entry_stick[e] - s0) * nz_pad + entry_z[e]], inv_n);
+    if (kinetic != nullptr) {
+      const T t = kinetic[g];
+      const C2<T> p = col[g];
+      v.re += t * p.re;
+      v.im += t * p.im;
+    }
+    dst[g] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Pass B: one (z plane, band) per block; 2-D FFT^+ . V . FFT^- in shared memory.
+// mode 0: local potential (sticks rewritten in place);
+// mode 1: density, rho[(x*ny+y)*nz+z] += w_b |psi_b(r)|^2 (sticks untouched).
+template <typename T, int MODE>
+__global__ void __launch_bounds__(kThreads) pass_b_kernel(
+    C2<T>* __restrict__ sticks, int nst, int nx, int ny, int nz, int nay, int nx_pad,
+    int ny_pad, FftDesc fx, FftDesc fy, const int32_t* __restrict__ stick_pos,
+    const int32_t* __restrict__ ay_to_y, const int32_t* __restrict__ y_to_ay,
+    const C2<T>* __restrict__ tw_x, const C2<T>* __restrict__ tw_y,
+    const T* __restrict__ potential, const double* __restrict__ weights,
+    double* __restrict__ density) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2<T>* plane = reinterpret_cast<C2<T>*>(smem_raw);  // [nay][nx_pad]
+  C2<T>* cols = plane + (size_t)nay * nx_pad;           // [kRowBatch][ny_pad]
+  C2<T>* twx = cols + (size_t)kRowBatch * ny_pad;
+  C2<T>* twy = twx + nx;
+  const int z = blockIdx.x;
+  const int64_t band = blockIdx.y;
+  for (int i = threadIdx.x; i < nx; i += blockDim.x) twx[i] = tw_x[i];
+  for (int i = threadIdx.x; i < ny; i += blockDim.x) twy[i] = tw_y[i];
+  for (int i = threadIdx.x; i < nay * nx_pad; i += blockDim.x) plane[i] = qeb::mk<T>(0, 0);
+  __syncthreads();
+  C2<T>* srow = sticks + (band * nz + z) * (int64_t)nst;
+  for (int s = threadIdx.x; s < nst; s += blockDim.x) plane[stick_pos[s]] = srow[s];
+  __syncthreads();
+  // inverse transform along x of the active rows
+  qeb::fft_lines<T, 2>(plane, nay, nx_pad, 1, fx, twx, true);
+  double w = 0.0;
+  if (MODE == 1) w = weights[band];
+  for (int x0 = 0; x0 < nx; x0 += kRowBatch) {
+    const int nb = min(kRowBatch, nx - x0);
+    for (int i = threadIdx.x; i < nb * ny; i += blockDim.x) {
+      const int r = i / ny, y = i - r * ny;
+      const int ay = y_to_ay[y];
+      cols[r * ny_pad + y] = (ay >= 0) ? plane[ay * nx_pad + x0 + r] : qeb::mk<T>(0, 0);
+    }
+    __syncthreads();
+    qeb::fft_lines<T, 2>(cols, nb, ny_pad, 1, fy, twy, true);
+    if (MODE == 0) {
+      const T* vrow = potential + ((int64_t)z * nx + x0) * ny;
+      for (int i = threadIdx.x; i < nb * ny; i += blockDim.x) {
+        const int r = i / ny, y = i - r * ny;
+        cols[r * ny_pad + y] = qeb::scale(cols[r * ny_pad + y], vrow[(int64_t)r * ny + y]);
+      }
+      __syncthreads();
+      qeb::fft_lines<T, 2>(cols, nb, ny_pad, 1, fy, twy, false);
+      for (int i = threadIdx.x; i < nb * nay; i += blockDim.x) {
+        const int r = i / nay, ay = i - r * nay;
+        plane[ay * nx_pad + x0 + r] = cols[r * ny_pad + ay_to_y[ay]];
+      }
+      __syncthreads();
+    } else {
+      for (int i = threadIdx.x; i < nb * ny; i += blockDim.x) {
+        const int r = i / ny, y = i - r * ny;
+        const C2<T> v = cols[r * ny_pad + y];
+        const double m = (double)v.re * (double)v.re + (double)v.im * (double)v.im;
+        atomicAdd(density + ((int64_t)(x0 + r) * ny + y) * nz + z, w * m);
+      }
+      __syncthreads();
+    }
+  }
+  if (MODE == 0) {
+    qeb::fft_lines<T, 2>(plane, nay, nx_pad, 1, fx, twx, false);
+    for (int s = threadIdx.x; s < nst; s += blockDim.x) srow[s] = plane[stick_pos[s]];
+  }
+}
+
+template <typename T>
+int set_smem_limits(const qeb_local_plan* p) {
+  const size_t b = pass_b_smem<T>(p), ac = pass_ac_smem<T>(p);
+  cudaError_t err;
+  err = cudaFuncSetAttribute(pass_b_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+  if (err != cudaSuccess) return qeb::cuda_status(err, "pass B smem attribute");
+  err = cudaFuncSetAttribute(pass_b_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+  if (err != cudaSuccess) return qeb::cuda_status(err, "pass B (density) smem attribute");
+  err = cudaFuncSetAttribute(pass_a_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ac);
+  if (err != cudaSuccess) return qeb::cuda_status(err, "pass A smem attribute");
+  err = cudaFuncSetAttribute(pass_c_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ac);
+  if (err != cudaSuccess) return qeb::cuda_status(err, "pass C smem attribute");
+  return QEB_OK;
+}
+
+template <typename T>
+const C2<T>* tw_ptr(const qeb_local_plan* p, int which) {
+  const C2<T>* base = static_cast<const C2<T>*>(p->tw);
+  if (which == 0) return base;
+  if (which == 1) return base + p->nx;
+  return base + p->nx + p->ny;
+}
+
+template <typename T>
+int launch_apply(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64_t ld,
+                 int64_t nb, const T* potential, const T* kinetic, C2<T>* out, int64_t ldo,
+                 cudaStream_t stream) {
+  if (nb == 0) return QEB_OK;
+  if (nb > 65535) {
+    qeb::set_error("apply_local: at most 65535 bands per call (got %lld)", (long long)nb);
+    return QEB_EINVAL;
+  }
+  const dim3 grid_ac((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
+  const dim3 grid_b(p->nz, (unsigned)nb);
+  pass_a_kernel<T><<<grid_ac, kThreads, pass_ac_smem<T>(p), stream>>>(
+      psi, ld, p->nst, p->nz, p->nz_pad, p->fz, p->entry_g, p->entry_z, p->entry_stick,
+      p->stick_off, tw_ptr<T>(p, 2), sticks);
+  pass_b_kernel<T, 0><<<grid_b, kThreads, pass_b_smem<T>(p), stream>>>(
+      sticks, p->nst, p->nx, p->ny, p->nz, p->nay, p->nx_pad, p->ny_pad, p->fx, p->fy,
+      p->stick_pos, p->ay_to_y, p->y_to_ay, tw_ptr<T>(p, 0), tw_ptr<T>(p, 1), potential,
+      nullptr, nullptr);
+  const T inv_n = T(1.0 / ((double)p->nx * p->ny * p->nz));
+  pass_c_kernel<T><<<grid_ac, kThreads, pass_ac_smem<T>(p), stream>>>(
+      sticks, p->nst, p->nz, p->nz_pad, p->fz, p->entry_g, p->entry_z, p->entry_stick,
+      p->stick_off, tw_ptr<T>(p, 2), psi, ld, kinetic, inv_n, out, ldo);
+  return qeb::cuda_status(cudaGetLastError(), "apply_local launch");
+}
+
+template <typename T>
+int launch_density(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64_t ld,
+                   int64_t nb, const double* weights, double* density, cudaStream_t stream) {
+  if (nb == 0) return QEB_OK;
+  if (nb > 65535) {
+    qeb::set_error("accumulate_density: at most 65535 bands per call (got %lld)", (long long)nb);
+    return QEB_EINVAL;
+  }
+  const dim3 grid_ac((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
+  const dim3 grid_b(p->nz, (unsigned)nb);
+  pass_a_kernel<T><<<grid_ac, kThreads, pass_ac_smem<T>(p), stream>>>(
+      psi, ld, p->nst, p->nz, p->nz_pad, p->fz, p->entry_g, p->entry_z, p->entry_stick,
+      p->stick_off, tw_ptr<T>(p, 2), sticks);
+  pass_b_kernel<T, 1><<<grid_b, kThreads, pass_b_smem<T>(p), stream>>>(
+      sticks, p->nst, p->nx, p->ny, p->nz, p->nay, p->nx_pad, p->ny_pad, p->fx, p->fy,
+      p->stick_pos, p->ay_to_y, p->y_to_ay, tw_ptr<T>(p, 0), tw_ptr<T>(p, 1), nullptr,
+      weights, density);
+  return qeb::cuda_status(cudaGetLastError(), "accumulate_density launch");
+}
+
+template <typename T>
+void fill_twiddles(std::vector<C2<T>>& out, int n) {
+  // exp(-2 pi i m / n) evaluated in long double and rounded once.
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  for (int m = 0; m < n; ++m) {
+    const long double a = two_pi * (long double)m / (long double)n;
+    out.push_back(qeb::mk<T>((T)cosl(a), (T)(-sinl(a))));
+  }
+}
+
+void free_plan(qeb_local_plan* p) {
+  if (p == nullptr) return;
+  cudaFree(p->entry_g);
+  cudaFree(p->entry_z);
+  cudaFree(p->entry_stick);
+  cudaFree(p->stick_off);
+  cudaFree(p->stick_pos);
+  cudaFree(p->ay_to_y);
+  cudaFree(p->y_to_ay);
+  cudaFree(p->tw);
+  delete p;
+}
+
+template <typename V>
+int upload(V** dst, const std::vector<V>& src) {
+  const size_t bytes = std::max<size_t>(1, src.size()) * sizeof(V);
+  cudaError_t err = cudaMalloc((void**)dst, bytes);
+  if (err != cudaSuccess) return qeb::cuda_status(err, "plan allocation");
+  if (!src.empty()) {
+    err = cudaMemcpy(*dst, src.data(), src.size() * sizeof(V), cudaMemcpyHostToDevice);
+    if (err != cudaSuccess) return qeb::cuda_status(err, "plan upload");
+  }
+  return QEB_OK;
+}
+
+}  // namespace
+
+extern "C" int qeb_local_plan_create(qeb_local_plan** out, int nx, int ny, int nz, int64_t npw,
+                                     const int64_t* z_major_slots, int precision) {
+  if (out == nullptr) {
+    qeb::set_error("local_plan_create: null output pointer");
+    return QEB_EINVAL;
+  }
+  *out = nullptr;
+  if (nx < 1 || ny < 1 || nz < 1 || npw < 1 || z_major_slots == nullptr) {
+    qeb::set_error("local_plan_create: invalid grid (%d,%d,%d) or basis size %lld", nx, ny, nz,
+                   (long long)npw);
+    return QEB_EINVAL;
+  }
+  if (precision != QEB_F64 && precision != QEB_F32) {
+    qeb::set_error("local_plan_create: unknown precision %d", precision);
+    return QEB_EINVAL;
+  }
+  if (npw > INT32_MAX) {
+    qeb::set_error("local_plan_create: basis too large");
+    return QEB_EINVAL;
+  }
+  qeb_local_plan* p = new (std::nothrow) qeb_local_plan();
+  if (p == nullptr) {
+    qeb::set_error("local_plan_create: host allocation failed");
+    return QEB_ECUDA;
+  }
+  std::memset(p, 0, sizeof(*p));
+  p->nx = nx;
+  p->ny = ny;
+  p->nz = nz;
+  p->npw = npw;
+  p->precision = precision;
+  cudaGetDevice(&p->device);
+  if (!qeb::make_fft_desc(nx, &p->fx) || !qeb::make_fft_desc(ny, &p->fy) ||
+      !qeb::make_fft_desc(nz, &p->fz)) {
+    qeb::set_error("local_plan_create: grid (%d,%d,%d) is not 2-3-5 smooth", nx, ny, nz);
+    delete p;
+    return QEB_EUNSUPPORTED;
+  }
+  const int64_t plane = (int64_t)nx * ny;
+  const int64_t total = plane * nz;
+  // Derive sticks from the z-major slots z*nx*ny + x*ny + y
+  // (qepy_pw/basis.py:530-541): sticks are the sorted unique xy slots.
+  std::vector<int64_t> xy(npw);
+  std::vector<int32_t> zs(npw);
+  for (int64_t g = 0; g < npw; ++g) {
+    const int64_t slot = z_major_slots[g];
+    if (slot < 0 || slot >= total) {
+      qeb::set_error("local_plan_create: slot %lld of row %lld outside the grid", (long long)slot,
+                     (long long)g);
+      delete p;
+      return QEB_EINVAL;
+    }
+    zs[g] = (int32_t)(slot / plane);
+    xy[g] = slot % plane;
+  }
+  std::vector<int64_t> sticks(xy);
+  std::sort(sticks.begin(), sticks.end());
+  sticks.erase(std::unique(sticks.begin(), sticks.end()), sticks.end());
+  const int nst = (int)sticks.size();
+  p->nst = nst;
+  std::vector<int32_t> stick_of(npw);
+  std::vector<int32_t> count(nst + 1, 0);
+  for (int64_t g = 0; g < npw; ++g) {
+    stick_of[g] = (int32_t)(std::lower_bound(sticks.begin(), sticks.end(), xy[g]) - sticks.begin());
+    count[stick_of[g] + 1]++;
+  }
+  for (int s = 0; s < nst; ++s) count[s + 1] += count[s];
+  std::vector<int32_t> stick_off(count);
+  std::vector<int32_t> entry_g(npw), entry_z(npw), entry_stick(npw);
+  {
+    std::vector<int32_t> cursor(count.begin(), count.end() - 1);
+    for (int64_t g = 0; g < npw; ++g) {
+      const int s = stick_of[g];
+      const int e = cursor[s]++;
+      entry_g[e] = (int32_t)g;
+      entry_z[e] = zs[g];
+      entry_stick[e] = s;
+    }
+  }
+  // Detect duplicate (x, y, z) slots: two plane waves cannot share a grid point.
+  for (int s = 0; s < nst; ++s) {
+    std::vector<int32_t> zl(entry_z.begin() + stick_off[s], entry_z.begin() + stick_off[s + 1]);
+    std::sort(zl.begin(), zl.end());
+    if (std::adjacent_find(zl.begin(), zl.end()) != zl.end()) {
+      qeb::set_error("local_plan_create: two plane waves map to one grid point");
+      delete p;
+      return QEB_EINVAL;
+    }
+  }
+  // Active y rows.
+  std::vector<int32_t> y_to_ay(ny, -1), ay_to_y;
+  for (int s = 0; s < nst; ++s) y_to_ay[sticks[s] % ny] = 1;
+  for (int y = 0; y < ny; ++y) {
+    if (y_to_ay[y] >= 0) {
+      y_to_ay[y] = (int32_t)ay_to_y.size();
+      ay_to_y.push_back(y);
+    }
+  }
+  p->nay = (int)ay_to_y.size();
+  p->nx_pad = odd_pad(nx);
+  p->ny_pad = odd_pad(ny);
+  p->nz_pad = odd_pad(nz);
+  std::vector<int32_t> stick_pos(nst);
+  for (int s = 0; s < nst; ++s) {
+    const int x = (int)(sticks[s] / ny), y = (int)(sticks[s] % ny);
+    stick_pos[s] = y_to_ay[y] * p->nx_pad + x;
+  }
+  int rc = QEB_OK;
+  if ((rc = upload(&p->entry_g, entry_g)) || (rc = upload(&p->entry_z, entry_z)) ||
+      (rc = upload(&p->entry_stick, entry_stick)) || (rc = upload(&p->stick_off, stick_off)) ||
+      (rc = upload(&p->stick_pos, stick_pos)) || (rc = upload(&p->ay_to_y, ay_to_y)) ||
+      (rc = upload(&p->y_to_ay, y_to_ay))) {
+    free_plan(p);
+    return rc;
+  }
+  if (precision == QEB_F64) {
+    std::vector<C2<double>> tw;
+    fill_twiddles(tw, nx);
+    fill_twiddles(tw, ny);
+    fill_twiddles(tw, nz);
+    rc = upload(reinterpret_cast<C2<double>**>(&p->tw), tw);
+    if (rc == QEB_OK) rc = set_smem_limits<double>(p);
+    if (rc == QEB_OK && pass_b_smem<double>(p) > 227 * 1024) {
+      qeb::set_error("local_plan_create: FP64 plane of %d x %d active rows exceeds shared memory",
+                     p->nay, nx);
+      rc = QEB_EUNSUPPORTED;
+    }
+  } else {
+    std::vector<C2<float>> tw;
+    fill_twiddles(tw, nx);
+    fill_twiddles(tw, ny);
+    fill_twiddles(tw, nz);
+    rc = upload(reinterpret_cast<C2<float>**>(&p->tw), tw);
+    if (rc == QEB_OK) rc = set_smem_limits<float>(p);
+  }
+  if (rc != QEB_OK) {
+    free_plan(p);
+    return rc;
+  }
+  *out = p;
+  return QEB_OK;
+}
+
+extern "C" int qeb_local_plan_destroy(qeb_local_plan* plan) {
+  free_plan(plan);
+  return QEB_OK;
+}
+
+extern "C" int qeb_local_plan_info(const qeb_local_plan* p, int64_t* info, int n) {
+  if (p == nullptr || info == nullptr || n < 8) {
+    qeb::set_error("local_plan_info: invalid arguments");
+    return QEB_EINVAL;
+  }
+  info[0] = p->nx;
+  info[1] = p->ny;
+  info[2] = p->nz;
+  info[3] = p->npw;
+  info[4] = p->nst;
+  info[5] = p->nay;
+  info[6] = p->precision;
+  info[7] = p->device;
+  return QEB_OK;
+}
+
+extern "C" int64_t qeb_local_scratch_bytes(const qeb_local_plan* p, int64_t nbands) {
+  if (p == nullptr || nbands < 0) return -1;
+  const int64_t elem = (p->precision == QEB_F64) ? 16 : 8;
+  return nbands * (int64_t)p->nz * p->nst * elem;
+}
+
+static int check_call(const qeb_local_plan* p, const void* scratch, int64_t scratch_bytes,
+                      const void* psi, int64_t ld, int64_t nb, const char* who) {
+  if (p == nullptr) {
+    qeb::set_error("%s: null plan", who);
+    return QEB_ENOPLAN;
+  }
+  if (nb < 0 || ld < p->npw) {
+    qeb::set_error("%s: leading dimension %lld below basis size %lld or negative band count", who,
+                   (long long)ld, (long long)p->npw);
+    return QEB_EINVAL;
+  }
+  if (nb > 0 && (psi == nullptr || scratch == nullptr)) {
+    qeb::set_error("%s: null operand", who);
+    return QEB_EINVAL;
+  }
+  if (scratch_bytes < qeb_local_scratch_bytes(p, nb)) {
+    qeb::set_error("%s: scratch of %lld bytes is below the %lld required", who,
+                   (long long)scratch_bytes, (long long)qeb_local_scratch_bytes(p, nb));
+    return QEB_ESCRATCH;
+  }
+  if ((reinterpret_cast<uintptr_t>(scratch) | reinterpret_cast<uintptr_t>(psi)) % 16 != 0) {
+    qeb::set_error("%s: operands must be 16-byte aligned", who);
+    return QEB_EINVAL;
+  }
+  return QEB_OK;
+}
+
+extern "C" int qeb_apply_local(const qeb_local_plan* p, void* scratch, int64_t scratch_bytes,
+                               const void* psi, int64_t ld, int64_t nbands,
+                               const void* potential_native, const void* kinetic, void* out,
+                               int64_t ldo, void* stream) {
+  int rc = check_call(p, scratch, scratch_bytes, psi, ld, nbands, "apply_local");
+  if (rc) return rc;
+  if (nbands > 0 && (potential_native == nullptr || out == nullptr || ldo < p->npw)) {
+    qeb::set_error("apply_local: null potential/output or short output leading dimension");
+    return QEB_EINVAL;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->precision == QEB_F64) {
+    return launch_apply<double>(p, static_cast<C2<double>*>(scratch),
+                                static_cast<const C2<double>*>(psi), ld, nbands,
+                                static_cast<const double*>(potential_native),
+                                static_cast<const double*>(kinetic),
+                                static_cast<C2<double>*>(out), ldo, s);
+  }
+  return launch_apply<float>(p, static_cast<C2<float>*>(scratch),
+                             static_cast<const C2<float>*>(psi), ld, nbands,
+                             static_cast<const float*>(potential_native),
+                             static_cast<const float*>(kinetic), static_cast<C2<float>*>(out),
+                             ldo, s);
+}
+
+extern "C" int qeb_accumulate_density(const qeb_local_plan* p, void* scratch,
+                                      int64_t scratch_bytes, const void* psi, int64_t ld,
+                                      int64_t nbands, const double* weights, double* density,
+                                      void* stream) {
+  int rc = check_call(p, scratch, scratch_bytes, psi, ld, nbands, "accumulate_density");
+  if (rc) return rc;
+  if (nbands > 0 && (weights == nullptr || density == nullptr)) {
+    qeb::set_error("accumulate_density: null weights or density");
+    return QEB_EINVAL;
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->precision == QEB_F64) {
+    return launch_density<double>(p, static_cast<C2<double>*>(scratch),
+                                  static_cast<const C2<double>*>(psi), ld, nbands, weights,
+                                  density, s);
+  }
+  return launch_density<float>(p, static_cast<C2<float>*>(scratch),
+                               static_cast<const C2<float>*>(psi), ld, nbands, weights, density,
+                               s);
+}

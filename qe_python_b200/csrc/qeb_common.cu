@@ -1,0 +1,50 @@
+// Error state and host-side FFT factorisation shared by all qe_b200 kernels.
+#include <cstdarg>
+#include <cstring>
+
+#include "qeb_common.cuh"
+#include "../../include/qe_b200.h"
+
+namespace qeb {
+
+static thread_local char g_last_error[512] = "";
+
+void set_error(const char* fmt, ...) {
+  va_list args;
+  va_start(args, fmt);
+  vsnprintf(g_last_error, sizeof(g_last_error), fmt, args);
+  va_end(args);
+}
+
+int cuda_status(cudaError_t err, const char* where) {
+  if (err == cudaSuccess) return QEB_OK;
+  set_error("%s: %s", where, cudaGetErrorString(err));
+  return QEB_ECUDA;
+}
+
+bool make_fft_desc(int n, FftDesc* d) {
+  if (n < 1 || n > 1024) return false;
+  d->n = n;
+  d->nstages = 0;
+  int rest = n;
+  // Radix 4 first (cheapest butterfly per point), then 2, 3, 5.
+  const int order[4] = {4, 2, 3, 5};
+  for (int i = 0; i < 4; ++i) {
+    const int r = order[i];
+    while (rest % r == 0) {
+      if (d->nstages >= kMaxStages) return false;
+      d->radix[d->nstages++] = r;
+      rest /= r;
+    }
+  }
+  if (n == 1) {
+    d->nstages = 0;
+  }
+  return rest == 1;
+}
+
+}  // namespace qeb
+
+extern "C" const char* qeb_last_error(void) { return qeb::g_last_error; }
+
+extern "C" int qeb_version(void) { return QEB_ABI_VERSION; }

@@ -1,0 +1,274 @@
+// Complex GEMMs of the nonlocal projector and Davidson subspace contractions.
+//
+//   C = alpha * op(A) * B + beta * C,   op(A) = A ("N") or A^H ("C")
+//
+// All matrices are column-major with explicit leading dimensions.  The
+// plain form runs in FP64 (complex128) on the FP64 pipes: a register-tiled
+// SIMT kernel (64 x 64 block tile, 4 x 4 complex micro tile per thread,
+// 16-deep K tiles double-buffered in shared memory).  Contractions over the
+// long plane-wave dimension (calbec beta^H psi, Davidson V^H HV) split K
+// across blocks; the partial tiles go to caller scratch and a second kernel
+// reduces them in a fixed order, so results are deterministic.
+//
+// Reference calls replaced: projector_overlaps (ZGEMM ConjTrans/NoTrans,
+// qepy_pw/_native_fft.pyx:694-731), add_projector_product (ZGEMM beta=1,
+// :782-836), the Davidson reduced-matrix and Ritz products
+// (qepy_pw/diagonalization.py:658-726) and coupling @ overlaps (:348).
+#include "qeb_common.cuh"
+#include "../../include/qe_b200.h"
+
+using qeb::C2;
+
+namespace {
+
+constexpr int BM = 64, BN = 64, BK = 16, THREADS = 256;
+
+template <typename T>
+struct Tile {
+  C2<T> a[2][BK][BM];
+  C2<T> b[2][BK][BN];
+};
+
+template <typename T, bool CONJ_A>
+__device__ __forceinline__ void load_tiles(const C2<T>* __restrict__ A, int64_t lda,
+                                           const C2<T>* __restrict__ B, int64_t ldb, int M,
+                                           int N, int k0, int k1, int m0, int n0,
+                                           C2<T> (&ra)[4], C2<T> (&rb)[4]) {
+  const int t = threadIdx.x;
+  const C2<T> zero = qeb::mk<T>(0, 0);
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    if (CONJ_A) {
+      // op(A)(m, k) = conj(A[k + m*lda]), contiguous along k
+      const int k = t % BK, m = t / BK + 16 * r;
+      const int gk = k0 + k, gm = m0 + m;
+      C2<T> v = zero;
+      if (gk < k1 && gm < M) {
+        v = A[gk + (int64_t)gm * lda];
+        v.im = -v.im;
+      }
+      ra[r] = v;
+    } else {
+      // op(A)(m, k) = A[m + k*lda], contiguous along m
+      const int m = t % BM, k = t / BM + 4 * r;
+      const int gk = k0 + k, gm = m0 + m;
+      ra[r] = (gk < k1 && gm < M) ? A[gm + (int64_t)gk * lda] : zero;
+    }
+    const int k = t % BK, n = t / BK + 16 * r;
+    const int gk = k0 + k, gn = n0 + n;
+    rb[r] = (gk < k1 && gn < N) ? B[gk + (int64_t)gn * ldb] : zero;
+  }
+}
+
+template <typename T, bool CONJ_A>
+__device__ __forceinline__ void store_tiles(Tile<T>& s, int buf, const C2<T> (&ra)[4],
+                                            const C2<T> (&rb)[4]) {
+  const int t = threadIdx.x;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    if (CONJ_A) {
+      s.a[buf][t % BK][t / BK + 16 * r] = ra[r];
+    } else {
+      s.a[buf][t / BM + 4 * r][t % BM] = ra[r];
+    }
+    s.b[buf][t % BK][t / BK + 16 * r] = rb[r];
+  }
+}
+
+// One block computes a BM x BN tile of op(A) B over K range [kbeg, kend).
+// split == 0: C = alpha*acc + beta*C.  split > 0: write acc to the partial
+// buffer P (slice blockIdx.z, ldp = M).
+template <typename T, bool CONJ_A>
+__global__ void __launch_bounds__(THREADS) gemm_kernel(int M, int N, int K, int kchunk,
+                                                       C2<T> alpha, const C2<T>* __restrict__ A,
+                                                       int64_t lda, const C2<T>* __restrict__ B,
+                                                       int64_t ldb, C2<T> beta, C2<T>* C,
+                                                       int64_t ldc, C2<T>* __restrict__ P) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  Tile<T>& s = *reinterpret_cast<Tile<T>*>(smem_raw);
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int kbeg = blockIdx.z * kchunk;
+  const int kend = min(K, kbeg + kchunk);
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+  C2<T> acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = qeb::mk<T>(0, 0);
+  C2<T> ra[4], rb[4];
+  int buf = 0;
+  if (kbeg < kend) {
+    load_tiles<T, CONJ_A>(A, lda, B, ldb, M, N, kbeg, kend, m0, n0, ra, rb);
+    store_tiles<T, CONJ_A>(s, 0, ra, rb);
+  }
+  __syncthreads();
+  for (int k0 = kbeg; k0 < kend; k0 += BK) {
+    const bool more = k0 + BK < kend;
+    if (more) load_tiles<T, CONJ_A>(A, lda, B, ldb, M, N, k0 + BK, kend, m0, n0, ra, rb);
+#pragma unroll 4
+    for (int kk = 0; kk < BK; ++kk) {
+      C2<T> av[4], bv[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) av[i] = s.a[buf][kk][ty + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) bv[j] = s.b[buf][kk][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j].re = fma(av[i].re, bv[j].re, acc[i][j].re);
+          acc[i][j].re = fma(-av[i].im, bv[j].im, acc[i][j].re);
+          acc[i][j].im = fma(av[i].re, bv[j].im, acc[i][j].im);
+          acc[i][j].im = fma(av[i].im, bv[j].re, acc[i][j].im);
+        }
+    }
+    if (more) store_tiles<T, CONJ_A>(s, buf ^ 1, ra, rb);
+    __syncthreads();
+    buf ^= 1;
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int gm = m0 + ty + 16 * i;
+    if (gm >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int gn = n0 + tx + 16 * j;
+      if (gn >= N) continue;
+      if (P != nullptr) {
+        P[(int64_t)blockIdx.z * M * N + gm + (int64_t)gn * M] = acc[i][j];
+      } else {
+        C2<T> v = qeb::cmul(alpha, acc[i][j]);
+        C2<T>* c = C + gm + (int64_t)gn * ldc;
+        if (beta.re != T(0) || beta.im != T(0)) v = v + qeb::cmul(beta, *c);
+        *c = v;
+      }
+    }
+  }
+}
+
+// C = alpha * sum_s P[s] + beta * C, slices summed in ascending order.
+template <typename T>
+__global__ void reduce_partials(int M, int N, int splits, const C2<T>* __restrict__ P,
+                                C2<T> alpha, C2<T> beta, C2<T>* C, int64_t ldc) {
+  const int64_t total = (int64_t)M * N;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    C2<T> sum = P[i];
+    for (int s = 1; s < splits; ++s) sum = sum + P[(int64_t)s * total + i];
+    const int64_t m = i % M, n = i / M;
+    C2<T> v = qeb::cmul(alpha, sum);
+    C2<T>* c = C + m + n * ldc;
+    if (beta.re != T(0) || beta.im != T(0)) v = v + qeb::cmul(beta, *c);
+    *c = v;
+  }
+}
+
+int g_sm_count = 0;
+
+int sm_count() {
+  if (g_sm_count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_sm_count, cudaDevAttrMultiProcessorCount, dev);
+    if (g_sm_count <= 0) g_sm_count = 148;
+  }
+  return g_sm_count;
+}
+
+// Number of K slices: enough blocks for ~2 waves, each slice >= 256 deep.
+int choose_splits(int M, int N, int K) {
+  const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+  const int want = (2 * sm_count() + tiles - 1) / tiles;
+  int by_depth = K / 256;
+  if (by_depth < 1) by_depth = 1;
+  int s = want < by_depth ? want : by_depth;
+  if (s > 64) s = 64;
+  return s < 1 ? 1 : s;
+}
+
+template <typename T>
+int gemm(int opa, int M, int N, int K, const double* alpha, const void* A, int64_t lda,
+         const void* B, int64_t ldb, const double* beta, void* C, int64_t ldc, void* scratch,
+         int64_t scratch_bytes, cudaStream_t stream) {
+  if (M < 0 || N < 0 || K < 0 || (opa != QEB_OP_N && opa != QEB_OP_C)) {
+    qeb::set_error("zgemm: invalid sizes or op");
+    return QEB_EINVAL;
+  }
+  if (M == 0 || N == 0) return QEB_OK;
+  const int64_t a_rows = (opa == QEB_OP_N) ? M : K;
+  if (lda < (a_rows > 0 ? a_rows : 1) || ldb < (K > 0 ? K : 1) || ldc < M) {
+    qeb::set_error("zgemm: leading dimension too small (lda=%lld ldb=%lld ldc=%lld)",
+                   (long long)lda, (long long)ldb, (long long)ldc);
+    return QEB_EINVAL;
+  }
+  if (C == nullptr || (K > 0 && (A == nullptr || B == nullptr))) {
+    qeb::set_error("zgemm: null operand");
+    return QEB_EINVAL;
+  }
+  const C2<T> al = qeb::mk<T>((T)alpha[0], (T)alpha[1]);
+  const C2<T> be = qeb::mk<T>((T)beta[0], (T)beta[1]);
+  const size_t smem = sizeof(Tile<T>);
+  static bool configured[2] = {false, false};
+  if (!configured[opa]) {
+    cudaFuncSetAttribute(gemm_kernel<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    cudaFuncSetAttribute(gemm_kernel<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)smem);
+    configured[opa] = true;
+  }
+  int splits = (opa == QEB_OP_C) ? choose_splits(M, N, K) : 1;
+  const int64_t slice_bytes = (int64_t)M * N * (int64_t)sizeof(C2<T>);
+  if (splits > 1) {
+    const int64_t fit = (scratch == nullptr) ? 0 : scratch_bytes / slice_bytes;
+    if (fit < splits) splits = (int)(fit < 1 ? 1 : fit);
+  }
+  int kchunk = K;
+  if (splits > 1) {
+    kchunk = (K + splits - 1) / splits;
+    kchunk = (kchunk + BK - 1) / BK * BK;
+    splits = (K + kchunk - 1) / kchunk;
+  }
+  if (K == 0) kchunk = 1;
+  const dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, splits);
+  C2<T>* partials = (splits > 1) ? static_cast<C2<T>*>(scratch) : nullptr;
+  if (opa == QEB_OP_C) {
+    gemm_kernel<T, true><<<grid, THREADS, smem, stream>>>(
+        M, N, K, kchunk, al, static_cast<const C2<T>*>(A), lda, static_cast<const C2<T>*>(B),
+        ldb, be, static_cast<C2<T>*>(C), ldc, partials);
+  } else {
+    gemm_kernel<T, false><<<grid, THREADS, smem, stream>>>(
+        M, N, K, kchunk, al, static_cast<const C2<T>*>(A), lda, static_cast<const C2<T>*>(B),
+        ldb, be, static_cast<C2<T>*>(C), ldc, partials);
+  }
+  if (splits > 1) {
+    const int64_t total = (int64_t)M * N;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 4 * sm_count()) blocks = 4 * sm_count();
+    reduce_partials<T><<<blocks, 256, 0, stream>>>(M, N, splits, partials, al, be,
+                                                   static_cast<C2<T>*>(C), ldc);
+  }
+  return qeb::cuda_status(cudaGetLastError(), "zgemm launch");
+}
+
+}  // namespace
+
+extern "C" int64_t qeb_zgemm_scratch_bytes(int opa, int M, int N, int K, int precision) {
+  if (opa != QEB_OP_C || M <= 0 || N <= 0 || K <= 0) return 0;
+  const int64_t elem = (precision == QEB_F64) ? 16 : 8;
+  const int splits = choose_splits(M, N, K);
+  return splits > 1 ? (int64_t)splits * M * N * elem : 0;
+}
+
+extern "C" int qeb_zgemm(int opa, int M, int N, int K, const double* alpha, const void* A,
+                         int64_t lda, const void* B, int64_t ldb, const double* beta, void* C,
+                         int64_t ldc, void* scratch, int64_t scratch_bytes, void* stream) {
+  return gemm<double>(opa, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, scratch, scratch_bytes,
+                      static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int qeb_cgemm(int opa, int M, int N, int K, const double* alpha, const void* A,
+                         int64_t lda, const void* B, int64_t ldb, const double* beta, void* C,
+                         int64_t ldc, void* scratch, int64_t scratch_bytes, void* stream) {
+  return gemm<float>(opa, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, scratch, scratch_bytes,
+                     static_cast<cudaStream_t>(stream));
+}

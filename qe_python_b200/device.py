@@ -1,0 +1,78 @@
+"""Device helpers: column-major torch CUDA tensors and the launching stream.
+
+Matrices on the hot path are column-major (the layout qepy-pw's Davidson
+allocates, qepy_pw/diagonalization.py:632-635): a tensor of shape (rows, cols)
+with strides (1, ld), ld >= rows.  PyTorch supplies device memory, streams and
+copies; every computation runs in libqeb200.so.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+COMPLEX_OF = {torch.float64: torch.complex128, torch.float32: torch.complex64}
+REAL_OF = {torch.complex128: torch.float64, torch.complex64: torch.float32}
+
+
+def require_cuda() -> torch.device:
+    if not torch.cuda.is_available():
+        raise RuntimeError(
+            "qe_b200 needs a CUDA device: the hot path has no CPU fallback"
+        )
+    return torch.device("cuda", torch.cuda.current_device())
+
+
+def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
+    stream = stream if stream is not None else torch.cuda.current_stream()
+    return int(stream.cuda_stream)
+
+
+def is_column_major(t: torch.Tensor) -> bool:
+    if t.dim() == 1:
+        return t.stride(0) == 1
+    return t.dim() == 2 and t.stride(0) == 1 and (t.shape[1] <= 1 or t.stride(1) >= t.shape[0])
+
+
+def leading_dimension(t: torch.Tensor) -> int:
+    """Column stride of a column-major matrix (any value >= rows for one column)."""
+    if t.dim() == 1:
+        return max(1, t.shape[0])
+    if t.shape[1] <= 1:
+        return max(1, t.shape[0], t.stride(1))
+    return t.stride(1)
+
+
+def empty_f(rows: int, cols: int, dtype, device=None, ld: int | None = None) -> torch.Tensor:
+    """Uninitialised column-major (rows, cols) tensor."""
+    device = device if device is not None else require_cuda()
+    ld = rows if ld is None else ld
+    storage = torch.empty((cols, ld), dtype=dtype, device=device)
+    return storage.T[:rows]
+
+
+def zeros_f(rows: int, cols: int, dtype, device=None) -> torch.Tensor:
+    device = device if device is not None else require_cuda()
+    return torch.zeros((cols, rows), dtype=dtype, device=device).T
+
+
+def to_device_f(values, dtype, device=None) -> torch.Tensor:
+    """Column-major device copy (no copy if already a matching tensor)."""
+    device = device if device is not None else require_cuda()
+    if isinstance(values, torch.Tensor):
+        t = values
+        if t.device != device or t.dtype != dtype:
+            t = t.to(device=device, dtype=dtype)
+        if t.dim() == 2 and not is_column_major(t):
+            t = t.T.contiguous().T
+        elif t.dim() == 1 and t.stride(0) != 1:
+            t = t.contiguous()
+        return t
+    array = np.asarray(values)
+    t = torch.from_numpy(np.asfortranarray(array) if array.ndim == 2 else np.ascontiguousarray(array))
+    return to_device_f(t.to(dtype=dtype), dtype, device)
+
+
+def as_numpy(t: torch.Tensor) -> np.ndarray:
+    array = t.detach().cpu().numpy()
+    return np.asfortranarray(array) if array.ndim == 2 else array

@@ -1,0 +1,164 @@
+"""Torch-tensor front end of the C ABI (GEMMs and Davidson column kernels).
+
+Each function validates shapes, resolves leading dimensions and launches on
+the current torch stream.  Matrices are column-major torch CUDA tensors
+(strides (1, ld)); scalars in FP64.
+"""
+
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+from .device import empty_f, is_column_major, leading_dimension, stream_handle
+
+OP_N = 0
+OP_C = 1
+
+_PREC = {torch.complex128: _lib.QEB_F64, torch.complex64: _lib.QEB_F32}
+
+
+class _Scratch:
+    """Grow-only device scratch for split-K partial tiles (per device)."""
+
+    def __init__(self) -> None:
+        self._buffers: dict[torch.device, torch.Tensor] = {}
+
+    def get(self, nbytes: int, device: torch.device) -> torch.Tensor:
+        current = self._buffers.get(device)
+        if current is None or current.numel() < nbytes:
+            current = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+            self._buffers[device] = current
+        return current
+
+
+_SCRATCH = _Scratch()
+
+
+def _precision(t: torch.Tensor) -> int:
+    try:
+        return _PREC[t.dtype]
+    except KeyError as exc:
+        raise TypeError(f"complex128 or complex64 tensor required, got {t.dtype}") from exc
+
+
+def _check_matrix(name: str, t: torch.Tensor) -> None:
+    if t.dim() != 2 or not t.is_cuda or not is_column_major(t):
+        raise ValueError(f"{name} must be a column-major 2-D CUDA tensor")
+
+
+def gemm(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None,
+         alpha: complex = 1.0, beta: complex = 0.0) -> torch.Tensor:
+    """c = alpha op(a) b + beta c with op(a) = a (OP_N) or a^H (OP_C)."""
+    _check_matrix("a", a)
+    _check_matrix("b", b)
+    if a.dtype != b.dtype:
+        raise TypeError("operands must share a dtype")
+    prec = _precision(a)
+    if op_a == OP_N:
+        m, k = a.shape
+    elif op_a == OP_C:
+        k, m = a.shape
+    else:
+        raise ValueError("op_a must be OP_N or OP_C")
+    if b.shape[0] != k:
+        raise ValueError(f"inner dimensions disagree: op(a) is {m}x{k}, b is {tuple(b.shape)}")
+    n = b.shape[1]
+    if c is None:
+        c = empty_f(m, n, a.dtype, a.device)
+        beta = 0.0
+    else:
+        _check_matrix("c", c)
+        if tuple(c.shape) != (m, n) or c.dtype != a.dtype:
+            raise ValueError("c has the wrong shape or dtype")
+    if m == 0 or n == 0:
+        return c
+    lib = _lib.load()
+    al = (ctypes.c_double * 2)(complex(alpha).real, complex(alpha).imag)
+    be = (ctypes.c_double * 2)(complex(beta).real, complex(beta).imag)
+    need = int(lib.qeb_zgemm_scratch_bytes(op_a, m, n, k, prec))
+    scratch = _SCRATCH.get(need, a.device) if need > 0 else None
+    fn = lib.qeb_zgemm if prec == _lib.QEB_F64 else lib.qeb_cgemm
+    status = fn(op_a, m, n, k, al, a.data_ptr(), leading_dimension(a), b.data_ptr(),
+                leading_dimension(b), be, c.data_ptr(), leading_dimension(c),
+                0 if scratch is None else scratch.data_ptr(), need, stream_handle())
+    _lib.check("qeb_zgemm" if prec == _lib.QEB_F64 else "qeb_cgemm", status)
+    return c
+
+
+def column_squared_norms(v: torch.Tensor) -> torch.Tensor:
+    _check_matrix("v", v)
+    out = torch.empty(v.shape[1], dtype=torch.float64, device=v.device)
+    _lib.check("qeb_column_squared_norms", _lib.load().qeb_column_squared_norms(
+        _precision(v), v.shape[0], v.shape[1], v.data_ptr(), leading_dimension(v),
+        out.data_ptr(), stream_handle()))
+    return out
+
+
+def column_diagonal_expectations(v: torch.Tensor, diagonal: torch.Tensor) -> torch.Tensor:
+    _check_matrix("v", v)
+    d = diagonal.to(dtype=torch.float64).contiguous()
+    out = torch.empty(v.shape[1], dtype=torch.float64, device=v.device)
+    _lib.check("qeb_column_diagonal_expectations", _lib.load().qeb_column_diagonal_expectations(
+        _precision(v), v.shape[0], v.shape[1], v.data_ptr(), leading_dimension(v),
+        d.data_ptr(), out.data_ptr(), stream_handle()))
+    return out
+
+
+def column_inner_products(left: torch.Tensor, right: torch.Tensor) -> torch.Tensor:
+    _check_matrix("left", left)
+    _check_matrix("right", right)
+    if left.shape != right.shape or left.dtype != right.dtype:
+        raise ValueError("inner-product matrices disagree")
+    out = torch.empty((left.shape[1], 2), dtype=torch.float64, device=left.device)
+    _lib.check("qeb_column_inner_products", _lib.load().qeb_column_inner_products(
+        _precision(left), left.shape[0], left.shape[1], left.data_ptr(), leading_dimension(left),
+        right.data_ptr(), leading_dimension(right), out.data_ptr(), stream_handle()))
+    return torch.view_as_complex(out)
+
+
+def precondition(residuals: torch.Tensor, eigenvalues: torch.Tensor, diagonal: torch.Tensor,
+                 out: torch.Tensor | None = None) -> torch.Tensor:
+    """QE g_psi (qepy_pw/_native_fft.pyx:852-899)."""
+    _check_matrix("residuals", residuals)
+    rows, cols = residuals.shape
+    e = eigenvalues.to(dtype=torch.float64).contiguous()
+    d = diagonal.to(dtype=torch.float64).contiguous()
+    if e.numel() != cols or d.numel() != rows:
+        raise ValueError("eigenvalues/diagonal do not match the residual block")
+    if out is None:
+        out = empty_f(rows, cols, residuals.dtype, residuals.device)
+    _lib.check("qeb_precondition", _lib.load().qeb_precondition(
+        _precision(residuals), rows, cols, residuals.data_ptr(), leading_dimension(residuals),
+        e.data_ptr(), d.data_ptr(), out.data_ptr(), leading_dimension(out), stream_handle()))
+    return out
+
+
+def normalize_columns(v: torch.Tensor, norms2: torch.Tensor, selected: torch.Tensor | None,
+                      out: torch.Tensor) -> torch.Tensor:
+    _check_matrix("v", v)
+    _check_matrix("out", out)
+    n2 = norms2.to(dtype=torch.float64).contiguous()
+    sel = None if selected is None else selected.to(dtype=torch.int64).contiguous()
+    cols = out.shape[1]
+    _lib.check("qeb_normalize_columns", _lib.load().qeb_normalize_columns(
+        _precision(v), v.shape[0], cols, v.data_ptr(), leading_dimension(v), n2.data_ptr(),
+        0 if sel is None else sel.data_ptr(), out.data_ptr(), leading_dimension(out),
+        stream_handle()))
+    return out
+
+
+def subtract_band_energies(residual: torch.Tensor, v: torch.Tensor,
+                           energies: torch.Tensor) -> torch.Tensor:
+    _check_matrix("residual", residual)
+    _check_matrix("v", v)
+    e = energies.to(dtype=torch.float64).contiguous()
+    if residual.shape != v.shape or e.numel() != v.shape[1]:
+        raise ValueError("residual matrices disagree")
+    _lib.check("qeb_subtract_band_energies", _lib.load().qeb_subtract_band_energies(
+        _precision(v), v.shape[0], v.shape[1], residual.data_ptr(), leading_dimension(residual),
+        v.data_ptr(), leading_dimension(v), e.data_ptr(), stream_handle()))
+    return residual
