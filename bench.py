@@ -1,0 +1,444 @@
+"""Benchmark of the B200 Kohn-Sham H|psi> hot path (one JSON line on rank 0).
+
+Workload (one "step"): one full H|psi> application
+  H psi = T psi + FFT^-(V . FFT^+ psi) + beta D beta^H psi
+on the H|psi> microbenchmark cell: cubic L = 15.8 bohr, 64^3 grid,
+11 019 plane waves, 256 bands, 64 atoms x 8 projectors (P = 512); seeded
+synthetic inputs (qe_python_b200/workloads.py).
+
+  value      H|psi> bands/s of the mixed form (FP32 FFT passes and FP32
+             projector GEMMs), inputs resident in HBM; L2 is flushed before
+             every timed step (a 256 MiB write).
+  fp64       the same for the plain FP64 form.
+  e2e        bands/s through the public PlaneWaveHamiltonian.apply call with
+             pinned host buffers: H2D of psi and D2H of H psi in the timed region.
+  roofline   the dominant kernel's algorithmic bytes (FFT passes) or flops
+             (GEMMs) per launch over its CUDA-event duration.
+  cpu_baseline  the oracle (NumPy/SciPy restatement of the reference's
+             serial apply_serial + ZGEMM projector path) on host cores.
+
+Multi-GPU: the operator does not shard across GPUs in this tier, so N GPUs
+run N independent replicas ("scaling": "weak"); value is the sum of bands
+over the max-over-ranks time.
+
+``--impl reference`` times the reference algorithm's CPU port (the oracle,
+all host threads) on the same workload, a bounded band sample per step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+REPO = Path(__file__).resolve().parent
+sys.path.insert(0, str(REPO))
+
+METRIC = "SCF time to 1e-8 Ry and H|psi> bands/s: mixed+batched vs FP64 plain, 1 B200"
+WORKLOAD = ("H|psi> microbenchmark: cubic L=15.8 bohr, ecutwfc 30 Ry, 64^3 grid, "
+            "11019 plane waves, 256 bands, 64 atoms x 8 projectors (P=512)")
+L2_FLUSH_BYTES = 256 << 20
+
+
+def parse_args():
+    p = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=20)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=("b200", "reference"), default="b200")
+    p.add_argument("--bands", type=int, default=256)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=10.0,
+                   help="approximate CPU time budget of the cpu_baseline sample")
+    return p.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas only)
+
+def init_distributed(backend: str):
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1 and not dist.is_initialized():
+        from datetime import timedelta
+
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        dist.init_process_group(backend=backend, timeout=timedelta(seconds=120))
+    return world, rank, local
+
+
+def max_over_ranks(value: float, world: int, device) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int) -> None:
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+# ---------------------------------------------------------------------------
+# clocks sampled during the timed region
+
+class ClockSampler:
+    QUERY = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.samples: list[list[str]] = []
+        self._proc = None
+        self._thread = None
+
+    def __enter__(self):
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._thread = threading.Thread(target=self._read, daemon=True)
+            self._thread.start()
+        except (OSError, ValueError):
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            self.samples.append([v.strip() for v in line.split(",")])
+
+    def __exit__(self, *exc):
+        if self._proc is not None:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self._proc.kill()
+        return False
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for row in self.samples:
+            if len(row) < 6:
+                continue
+            try:
+                sm.append(float(row[0]))
+                smax.append(float(row[1]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, row[2:6]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {
+            "sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(smax) if smax else None,
+            "reasons": sorted(reasons),
+            "samples": len(sm),
+        }
+
+
+def measured_peaks() -> dict:
+    path = REPO / "MEASURED_PEAKS.json"
+    if path.exists():
+        data = json.loads(path.read_text())
+        return {"hbm_gbs": float(data["hbm_gbs"]), "source": "measured"}
+    return {"hbm_gbs": 6650.0, "source": "fallback"}
+
+
+# ---------------------------------------------------------------------------
+# CPU side: the oracle (reference algorithm restated in NumPy/SciPy)
+
+def cpu_hpsi_rate(work, bands: int, seconds: float, threads: int) -> dict:
+    """Bands/s of the oracle H|psi> (apply_serial + projector ZGEMMs)."""
+    from oracle import native_fft as oracle
+    from qe_python_b200.basis import grid_slots
+
+    oracle.set_workers(threads)
+    try:
+        from threadpoolctl import threadpool_limits
+        limiter = threadpool_limits(limits=threads)
+    except Exception:  # pragma: no cover - threadpoolctl is optional
+        limiter = None
+    linear, *_ = grid_slots(work.miller, work.shape)
+    size = int(np.prod(work.shape))
+    psi = np.asfortranarray(work.psi[:, :bands])
+    grid = np.zeros((bands, size), dtype=np.complex128)
+    plan = oracle.NativeFFTWPlan(grid, work.shape, bands, 1, size)
+    result = np.zeros_like(psi)
+    beta = np.asfortranarray(work.beta)
+    coupling = work.coupling.astype(np.complex128)
+
+    def one():
+        oracle.apply_serial(grid, psi, work.potential, linear, plan, size, size, result, 0,
+                            work.kinetic)
+        becp = oracle.projector_overlaps(beta, psi)
+        coupled = np.asfortranarray(coupling @ becp)
+        oracle.add_projector_product(result, beta, coupled)
+
+    one()  # warm
+    done, start = 0, time.perf_counter()
+    while True:
+        one()
+        done += 1
+        elapsed = time.perf_counter() - start
+        if elapsed >= seconds:
+            break
+    if limiter is not None:
+        limiter.unregister() if hasattr(limiter, "unregister") else None
+    return {"value": done * bands / elapsed, "repeats": done, "elapsed_s": elapsed}
+
+
+def run_reference(args) -> None:
+    world, rank, _local = init_distributed("gloo")
+    if rank != 0:
+        return
+    from qe_python_b200.workloads import hpsi_microbench
+
+    threads = os.cpu_count() or 1
+    work = hpsi_microbench(nbands=args.bands)
+    sample = min(32, args.bands)
+    per_step = max(1.0, 60.0 / max(1, args.steps + args.warmup))
+    for _ in range(args.warmup):
+        cpu_hpsi_rate(work, sample, 0.0, threads)
+    rates = [cpu_hpsi_rate(work, sample, per_step, threads)["value"] for _ in range(args.steps)]
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "bands/s",
+        "n_gpus": args.gpus,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1000.0 * sample / value,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "complex128",
+        "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD, "parallelism": "host threads"},
+        "cpu_baseline": {
+            "value": value, "unit": "bands/s", "cores": threads, "kind": "port",
+            "sample": f"{sample} of {args.bands} bands per step, repeated for ~{per_step:.0f} s; "
+                      "oracle restatement of apply_serial + projector ZGEMMs (SciPy pocketfft, "
+                      "NumPy BLAS)",
+        },
+        "e2e": {"value": value, "unit": "bands/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# GPU side
+
+def run_b200(args) -> None:
+    import torch
+
+    world, rank, local = init_distributed("nccl")
+    torch.cuda.set_device(local)
+    device = torch.device("cuda", local)
+    from qe_python_b200 import _lib
+    from qe_python_b200 import kernels as K
+    from qe_python_b200.basis import LocalPotentialWorkspace, make_bases
+    from qe_python_b200.device import to_device_f
+    from qe_python_b200.diagonalization import PlaneWaveHamiltonian
+    from qe_python_b200.workloads import hpsi_microbench
+
+    lib = _lib.load()
+    work = hpsi_microbench(nbands=args.bands)
+    npw, nb = work.npw, work.nbands
+    basis = make_bases(work.reciprocal, np.zeros(3), 30.0)[0]
+    assert np.array_equal(basis.indices, work.miller)
+    terms = ((work.beta, work.coupling),)
+    forms = {}
+    for name, precision in (("mixed", "f32"), ("fp64", "f64")):
+        ws = LocalPotentialWorkspace(basis, work.shape, precision=precision, device=device)
+        ham = PlaneWaveHamiltonian(basis, None, terms, local_workspace=ws,
+                                   real_potential=torch.from_numpy(work.potential).to(device),
+                                   potential_average=0.0)
+        psi = to_device_f(work.psi, ham.dtype, device)
+        out = torch.empty_like(psi.T).T
+        forms[name] = (ws, ham, psi, out)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device=device)
+    stream = torch.cuda.current_stream()
+
+    def timed_loop(name: str, steps: int, warmup: int, profile: bool):
+        ws, ham, psi, out = forms[name]
+        for _ in range(warmup):
+            ham.apply_into(psi, out)
+        torch.cuda.synchronize()
+        times, stages = [], []
+        launches0 = lib.qeb_launch_count()
+        for _ in range(steps):
+            flush.fill_(1.0)
+            barrier(world)
+            torch.cuda.synchronize()
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            if profile:
+                ws.pass_times = []
+            ev[0].record(stream)
+            # same sequence as PlaneWaveHamiltonian._apply, with events between stages
+            ws._launch_apply(ham._potential, psi, ham._kinetic_kernel, out)
+            ev[1].record(stream)
+            becp = K.gemm(K.OP_C, ham.projectors.beta, psi)
+            ev[2].record(stream)
+            coupled = K.gemm(K.OP_N, ham.projectors.coupling, becp)
+            ev[3].record(stream)
+            K.gemm(K.OP_N, ham.projectors.beta, coupled, out, beta=1.0)
+            ev[4].record(stream)
+            torch.cuda.synchronize()
+            times.append(ev[0].elapsed_time(ev[4]))
+            passes = ws.pass_times[0] if profile else (float("nan"),) * 3
+            stages.append((*passes, ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3]),
+                           ev[3].elapsed_time(ev[4])))
+            ws.pass_times = None
+        launches = lib.qeb_launch_count() - launches0
+        return times, stages, launches
+
+    # timed region of the headline value
+    with ClockSampler(local) as clocks:
+        barrier(world)
+        torch.cuda.synchronize()
+        times, stages, launches = timed_loop("mixed", args.steps, args.warmup, profile=True)
+        barrier(world)
+        torch.cuda.synchronize()
+    step_ms = max_over_ranks(statistics.mean(times), world, device)
+    fp64_times, fp64_stages, _ = timed_loop("fp64", args.steps, args.warmup, profile=True)
+    fp64_ms = max_over_ranks(statistics.mean(fp64_times), world, device)
+
+    # end to end through the public API with pinned host buffers
+    ws, ham, psi_dev, _ = forms["mixed"]
+    # column-major pinned host buffers: the copies are single contiguous DMAs
+    host_in = torch.from_numpy(np.ascontiguousarray(work.psi.T.astype(np.complex64))).pin_memory().T
+    host_out = torch.empty((nb, npw), dtype=torch.complex64, pin_memory=True).T
+    dev_in = torch.empty_like(psi_dev)
+    e2e_times = []
+    for i in range(args.warmup + args.steps):
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        dev_in.copy_(host_in, non_blocking=True)
+        result = ham.apply(dev_in)
+        host_out.copy_(result, non_blocking=True)
+        b.record(stream)
+        torch.cuda.synchronize()
+        if i >= args.warmup:
+            e2e_times.append(a.elapsed_time(b))
+    e2e_ms = max_over_ranks(statistics.mean(e2e_times), world, device)
+
+    # roofline of the dominant kernel in the headline (mixed) form
+    names = ["pass_a", "pass_b", "pass_c", "calbec_gemm", "coupling_gemm", "add_gemm"]
+    mean_stage = [statistics.mean(s[i] for s in stages) for i in range(len(names))]
+    total_stage = sum(mean_stage)
+    shares = {n: round(t / total_stage, 4) for n, t in zip(names, mean_stage)}
+    dominant = names[int(np.argmax(mean_stage))]
+    c = 8  # complex64 bytes
+    nst = ws.stick_count
+    nz = work.shape[2]
+    n_r = int(np.prod(work.shape))
+    P = work.beta.shape[1]
+    algorithmic = {
+        "pass_a": ("hbm", nb * (npw + nst * nz) * c + npw * 12),
+        "pass_b": ("hbm", nb * 2 * nst * nz * c + n_r * 4),
+        "pass_c": ("hbm", nb * (nst * nz + 2 * npw) * c + npw * (12 + 4)),
+        "calbec_gemm": ("flops", 8.0 * npw * P * nb),
+        "coupling_gemm": ("flops", 8.0 * P * P * nb),
+        "add_gemm": ("flops", 8.0 * npw * P * nb),
+    }
+    peaks = measured_peaks()
+    kind, amount = algorithmic[dominant]
+    seconds = mean_stage[names.index(dominant)] / 1e3
+    if kind == "hbm":
+        achieved = amount / seconds / 1e9
+        roofline = {"bound": "hbm", "kernel": dominant, "achieved": achieved,
+                    "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                    "frac": achieved / peaks["hbm_gbs"], "traffic": None,
+                    "peak_source": peaks["source"]}
+    else:
+        achieved = amount / seconds / 1e12
+        # FP32 SIMT pipes: 148 SMs x 128 FMA/clk x 2 flop x 1.965 GHz (nominal)
+        peak = 148 * 128 * 2 * 1.965e9 / 1e12
+        roofline = {"bound": "tensor", "kernel": dominant, "achieved": achieved,
+                    "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                    "traffic": None,
+                    "peak_source": "nominal FP32 FMA peak (the GEMM runs on FP32 pipes, "
+                                   "not tensor cores)"}
+    fft_ms = sum(mean_stage[:3])
+    fft_bytes = sum(algorithmic[n][1] for n in names[:3])
+    line = {
+        "metric": METRIC,
+        "value": world * nb / (step_ms / 1e3),
+        "unit": "bands/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step_ms,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "complex64 FFT/V*psi + complex64 projector GEMMs (FP32 accumulate)",
+        "data": "synthetic (seeded, qe_python_b200/workloads.py)",
+        "config": {"workload": WORKLOAD, "global_batch": world * nb, "parallelism": f"replicas x{world}",
+                   "l2": "flushed (256 MiB write) before every timed step"},
+        "fp64": {"value": world * nb / (fp64_ms / 1e3), "unit": "bands/s", "ms_per_step": fp64_ms},
+        "stages_ms": {n: round(t, 5) for n, t in zip(names, mean_stage)},
+        "kernel_shares": shares,
+        "fft_passes": {"ms": fft_ms, "algorithmic_bytes": fft_bytes,
+                       "GBps": fft_bytes / (fft_ms / 1e3) / 1e9},
+        "roofline": roofline,
+        "gpu_launches": int(launches),
+        "e2e": {"value": world * nb / (e2e_ms / 1e3), "unit": "bands/s",
+                "h2d_bytes_per_step": npw * nb * 8, "d2h_bytes_per_step": npw * nb * 8},
+        "clocks": clocks.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        sample = 16
+        cpu = cpu_hpsi_rate(work, sample, args.cpu_seconds, threads)
+        line["cpu_baseline"] = {
+            "value": cpu["value"], "unit": "bands/s", "cores": threads, "kind": "port",
+            "sample": f"{sample} bands x {cpu['repeats']} repeats ({cpu['elapsed_s']:.1f} s); "
+                      "oracle restatement of apply_serial + projector ZGEMMs, FP64",
+        }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -41,6 +41,8 @@ extern "C" {
 const char* qeb_last_error(void);
 /* QEB_ABI_VERSION of the loaded library. */
 int qeb_version(void);
+/* Kernels launched by this library since it was loaded (all threads). */
+int64_t qeb_launch_count(void);
 
 /* ------------------------------------------------------------------------
  * Local potential operator on the FFT grid (sticks / planes).
@@ -71,6 +73,13 @@ int qeb_apply_local(const qeb_local_plan* plan, void* scratch, int64_t scratch_b
                     const void* psi, int64_t ld_psi, int64_t nbands,
                     const void* potential_native, const void* kinetic, void* out,
                     int64_t ld_out, void* stream);
+/* qeb_apply_local with CUDA events around its three passes on `stream`;
+ * waits for completion and stores the pass durations (ms) in pass_ms[0..2].
+ * Benchmark instrumentation; no reference counterpart. */
+int qeb_apply_local_profiled(const qeb_local_plan* plan, void* scratch, int64_t scratch_bytes,
+                             const void* psi, int64_t ld_psi, int64_t nbands,
+                             const void* potential_native, const void* kinetic, void* out,
+                             int64_t ld_out, void* stream, float* pass_ms);
 
 /* density[(x*ny + y)*nz + z] += sum_b weights[b] |FFT^+(psi[:, b])(x,y,z)|^2
  * (float64 accumulation; weights is a device float64 array of nbands).
@@ -131,6 +140,13 @@ int qeb_normalize_columns(int precision, int64_t rows, int64_t cols, const void*
 int qeb_subtract_band_energies(int precision, int64_t rows, int64_t cols, void* residual,
                                int64_t ldr, const void* v, int64_t ldv, const double* energies,
                                void* stream);
+
+/* diag[g] += multiplicity * Re sum_i coupled[g,i] conj(beta[g,i]) (coupled = beta D)
+ * — accumulate_projector_diagonal (qepy_pw/_native_fft.pyx:734-779) */
+int qeb_accumulate_projector_diagonal(int precision, int64_t rows, int64_t channels,
+                                      const void* coupled, int64_t ldc, const void* beta,
+                                      int64_t ldb, double multiplicity, double* diagonal,
+                                      void* stream);
 
 #ifdef __cplusplus
 }

@@ -32,11 +32,13 @@ _D = ctypes.c_double
 SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_last_error", ctypes.c_char_p, []),
     ("qeb_version", _I, []),
+    ("qeb_launch_count", _L, []),
     ("qeb_local_plan_create", _I, [ctypes.POINTER(_P), _I, _I, _I, _L, _P, _I]),
     ("qeb_local_plan_destroy", _I, [_P]),
     ("qeb_local_plan_info", _I, [_P, _P, _I]),
     ("qeb_local_scratch_bytes", _L, [_P, _L]),
     ("qeb_apply_local", _I, [_P, _P, _L, _P, _L, _L, _P, _P, _P, _L, _P]),
+    ("qeb_apply_local_profiled", _I, [_P, _P, _L, _P, _L, _L, _P, _P, _P, _L, _P, _P]),
     ("qeb_accumulate_density", _I, [_P, _P, _L, _P, _L, _L, _P, _P, _P]),
     ("qeb_zgemm_scratch_bytes", _L, [_I, _I, _I, _I, _I]),
     ("qeb_zgemm", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
@@ -47,6 +49,7 @@ SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_precondition", _I, [_I, _L, _L, _P, _L, _P, _P, _P, _L, _P]),
     ("qeb_normalize_columns", _I, [_I, _L, _L, _P, _L, _P, _P, _P, _L, _P]),
     ("qeb_subtract_band_energies", _I, [_I, _L, _L, _P, _L, _P, _L, _P, _P]),
+    ("qeb_accumulate_projector_diagonal", _I, [_I, _L, _L, _P, _L, _P, _L, _D, _P, _P]),
 ]
 
 

@@ -359,6 +359,8 @@ class LocalPotentialWorkspace:
         self.active_rows = int(info[5])
         self._potential_cache: tuple | None = None
         self._kinetic_cache: tuple | None = None
+        # When a list, each apply batch appends its (A, B, C) pass times in ms.
+        self.pass_times: list | None = None
 
     def __del__(self) -> None:
         plan = getattr(self, "_plan", None)
@@ -460,13 +462,18 @@ class LocalPotentialWorkspace:
         for start in range(0, nb, batch):
             count = min(batch, nb - start)
             scratch, nbytes = self._scratch(count)
-            status = lib.qeb_apply_local(
+            args = (
                 self._plan, scratch.data_ptr(), nbytes,
                 vectors.data_ptr() + start * ld_in * elem, ld_in, count,
                 potential.data_ptr(), 0 if kinetic is None else kinetic.data_ptr(),
                 target.data_ptr() + start * ld_out * elem, ld_out, stream,
             )
-            _lib.check("qeb_apply_local", status)
+            if self.pass_times is None:
+                _lib.check("qeb_apply_local", lib.qeb_apply_local(*args))
+            else:
+                ms = (ctypes.c_float * 3)()
+                _lib.check("qeb_apply_local_profiled", lib.qeb_apply_local_profiled(*args, ms))
+                self.pass_times.append(tuple(float(v) for v in ms))
 
     def accumulate_density(self, density, coefficients, band_weights) -> None:
         """density[x, y, z] += sum_b w_b |psi_b(r)|^2 (float64, C-order grid)."""

@@ -151,6 +151,7 @@ extern "C" int qeb_column_squared_norms(int precision, int64_t rows, int64_t col
                    rows, static_cast<const C2<double>*>(v), ld, nullptr, 0, nullptr, out)),
                (column_reduce<float, 0><<<(unsigned)cols, kReduceThreads, 0, s>>>(
                    rows, static_cast<const C2<float>*>(v), ld, nullptr, 0, nullptr, out)));
+  qeb::count_launches(1);
   return qeb::cuda_status(cudaGetLastError(), "column_squared_norms");
 }
 
@@ -168,6 +169,7 @@ extern "C" int qeb_column_diagonal_expectations(int precision, int64_t rows, int
                    rows, static_cast<const C2<double>*>(v), ld, nullptr, 0, diag, out)),
                (column_reduce<float, 1><<<(unsigned)cols, kReduceThreads, 0, s>>>(
                    rows, static_cast<const C2<float>*>(v), ld, nullptr, 0, diag, out)));
+  qeb::count_launches(1);
   return qeb::cuda_status(cudaGetLastError(), "column_diagonal_expectations");
 }
 
@@ -188,6 +190,7 @@ extern "C" int qeb_column_inner_products(int precision, int64_t rows, int64_t co
                (column_reduce<float, 2><<<(unsigned)cols, kReduceThreads, 0, s>>>(
                    rows, static_cast<const C2<float>*>(left), ldl,
                    static_cast<const C2<float>*>(right), ldr, nullptr, out_complex)));
+  qeb::count_launches(1);
   return qeb::cuda_status(cudaGetLastError(), "column_inner_products");
 }
 
@@ -209,6 +212,7 @@ extern "C" int qeb_precondition(int precision, int64_t rows, int64_t cols, const
                (precondition_kernel<float><<<blocks, 256, 0, s>>>(
                    rows, cols, static_cast<const C2<float>*>(residuals), ldr, eigenvalues,
                    diagonal, static_cast<C2<float>*>(out), ldo)));
+  qeb::count_launches(1);
   return qeb::cuda_status(cudaGetLastError(), "precondition");
 }
 
@@ -230,6 +234,7 @@ extern "C" int qeb_normalize_columns(int precision, int64_t rows, int64_t cols, 
                (normalize_kernel<float><<<blocks, 256, 0, s>>>(
                    rows, cols, static_cast<const C2<float>*>(v), ldv, norms2, selected,
                    static_cast<C2<float>*>(out), ldo)));
+  qeb::count_launches(1);
   return qeb::cuda_status(cudaGetLastError(), "normalize_columns");
 }
 
@@ -250,5 +255,51 @@ extern "C" int qeb_subtract_band_energies(int precision, int64_t rows, int64_t c
                (subtract_kernel<float><<<blocks, 256, 0, s>>>(
                    rows, cols, static_cast<C2<float>*>(residual), ldr,
                    static_cast<const C2<float>*>(v), ldv, energies)));
+  qeb::count_launches(1);
   return qeb::cuda_status(cudaGetLastError(), "subtract_band_energies");
+}
+
+namespace {
+
+// diag[g] += m * Re sum_i coupled[g, i] conj(beta[g, i])
+template <typename T>
+__global__ void projector_diagonal_kernel(int64_t rows, int64_t channels,
+                                          const C2<T>* __restrict__ coupled, int64_t ldc,
+                                          const C2<T>* __restrict__ beta, int64_t ldb,
+                                          double multiplicity, double* __restrict__ diag) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g < rows;
+       g += (int64_t)gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int64_t i = 0; i < channels; ++i) {
+      const C2<T> c = coupled[g + i * ldc], b = beta[g + i * ldb];
+      acc += (double)c.re * b.re + (double)c.im * b.im;
+    }
+    diag[g] += multiplicity * acc;
+  }
+}
+
+}  // namespace
+
+extern "C" int qeb_accumulate_projector_diagonal(int precision, int64_t rows, int64_t channels,
+                                                 const void* coupled, int64_t ldc,
+                                                 const void* beta, int64_t ldb,
+                                                 double multiplicity, double* diagonal,
+                                                 void* stream) {
+  if (rows < 0 || channels < 0 || ldc < rows || ldb < rows ||
+      (rows > 0 && channels > 0 && (!coupled || !beta || !diagonal))) {
+    qeb::set_error("accumulate_projector_diagonal: invalid arguments");
+    return QEB_EINVAL;
+  }
+  if (rows == 0 || channels == 0) return QEB_OK;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  const int blocks = grid_for(rows);
+  QEB_DISPATCH(precision,
+               (projector_diagonal_kernel<double><<<blocks, 256, 0, s>>>(
+                   rows, channels, static_cast<const C2<double>*>(coupled), ldc,
+                   static_cast<const C2<double>*>(beta), ldb, multiplicity, diagonal)),
+               (projector_diagonal_kernel<float><<<blocks, 256, 0, s>>>(
+                   rows, channels, static_cast<const C2<float>*>(coupled), ldc,
+                   static_cast<const C2<float>*>(beta), ldb, multiplicity, diagonal)));
+  qeb::count_launches(1);
+  return qeb::cuda_status(cudaGetLastError(), "accumulate_projector_diagonal");
 }

@@ -235,7 +235,7 @@ const C2<T>* tw_ptr(const qeb_local_plan* p, int which) {
 template <typename T>
 int launch_apply(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64_t ld,
                  int64_t nb, const T* potential, const T* kinetic, C2<T>* out, int64_t ldo,
-                 cudaStream_t stream) {
+                 cudaStream_t stream, cudaEvent_t* events = nullptr) {
   if (nb == 0) return QEB_OK;
   if (nb > 65535) {
     qeb::set_error("apply_local: at most 65535 bands per call (got %lld)", (long long)nb);
@@ -243,17 +243,22 @@ int launch_apply(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64
   }
   const dim3 grid_ac((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
   const dim3 grid_b(p->nz, (unsigned)nb);
+  if (events) cudaEventRecord(events[0], stream);
   pass_a_kernel<T><<<grid_ac, kThreads, pass_ac_smem<T>(p), stream>>>(
       psi, ld, p->nst, p->nz, p->nz_pad, p->fz, p->entry_g, p->entry_z, p->entry_stick,
       p->stick_off, tw_ptr<T>(p, 2), sticks);
+  if (events) cudaEventRecord(events[1], stream);
   pass_b_kernel<T, 0><<<grid_b, kThreads, pass_b_smem<T>(p), stream>>>(
       sticks, p->nst, p->nx, p->ny, p->nz, p->nay, p->nx_pad, p->ny_pad, p->fx, p->fy,
       p->stick_pos, p->ay_to_y, p->y_to_ay, tw_ptr<T>(p, 0), tw_ptr<T>(p, 1), potential,
       nullptr, nullptr);
+  if (events) cudaEventRecord(events[2], stream);
   const T inv_n = T(1.0 / ((double)p->nx * p->ny * p->nz));
   pass_c_kernel<T><<<grid_ac, kThreads, pass_ac_smem<T>(p), stream>>>(
       sticks, p->nst, p->nz, p->nz_pad, p->fz, p->entry_g, p->entry_z, p->entry_stick,
       p->stick_off, tw_ptr<T>(p, 2), psi, ld, kinetic, inv_n, out, ldo);
+  if (events) cudaEventRecord(events[3], stream);
+  qeb::count_launches(3);
   return qeb::cuda_status(cudaGetLastError(), "apply_local launch");
 }
 
@@ -274,6 +279,7 @@ int launch_density(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int
       sticks, p->nst, p->nx, p->ny, p->nz, p->nay, p->nx_pad, p->ny_pad, p->fx, p->fy,
       p->stick_pos, p->ay_to_y, p->y_to_ay, tw_ptr<T>(p, 0), tw_ptr<T>(p, 1), nullptr,
       weights, density);
+  qeb::count_launches(2);
   return qeb::cuda_status(cudaGetLastError(), "accumulate_density launch");
 }
 
@@ -555,4 +561,52 @@ extern "C" int qeb_accumulate_density(const qeb_local_plan* p, void* scratch,
   return launch_density<float>(p, static_cast<C2<float>*>(scratch),
                                static_cast<const C2<float>*>(psi), ld, nbands, weights, density,
                                s);
+}
+
+// Same operator as qeb_apply_local, with CUDA events recorded on `stream`
+// around each pass; waits for them and returns the three pass durations in
+// milliseconds (pass_ms[0..2] = A, B, C).  Used by the benchmark to time
+// the kernels inside its measured loop.
+extern "C" int qeb_apply_local_profiled(const qeb_local_plan* p, void* scratch,
+                                        int64_t scratch_bytes, const void* psi, int64_t ld,
+                                        int64_t nbands, const void* potential_native,
+                                        const void* kinetic, void* out, int64_t ldo,
+                                        void* stream, float* pass_ms) {
+  int rc = check_call(p, scratch, scratch_bytes, psi, ld, nbands, "apply_local_profiled");
+  if (rc) return rc;
+  if (pass_ms == nullptr || (nbands > 0 && (potential_native == nullptr || out == nullptr))) {
+    qeb::set_error("apply_local_profiled: null output");
+    return QEB_EINVAL;
+  }
+  cudaEvent_t ev[4];
+  for (int i = 0; i < 4; ++i) {
+    cudaError_t err = cudaEventCreate(&ev[i]);
+    if (err != cudaSuccess) {
+      for (int j = 0; j < i; ++j) cudaEventDestroy(ev[j]);
+      return qeb::cuda_status(err, "apply_local_profiled events");
+    }
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (p->precision == QEB_F64) {
+    rc = launch_apply<double>(p, static_cast<C2<double>*>(scratch),
+                              static_cast<const C2<double>*>(psi), ld, nbands,
+                              static_cast<const double*>(potential_native),
+                              static_cast<const double*>(kinetic), static_cast<C2<double>*>(out),
+                              ldo, s, ev);
+  } else {
+    rc = launch_apply<float>(p, static_cast<C2<float>*>(scratch),
+                             static_cast<const C2<float>*>(psi), ld, nbands,
+                             static_cast<const float*>(potential_native),
+                             static_cast<const float*>(kinetic), static_cast<C2<float>*>(out),
+                             ldo, s, ev);
+  }
+  if (rc == QEB_OK && nbands > 0) {
+    cudaError_t err = cudaEventSynchronize(ev[3]);
+    for (int i = 0; i < 3 && err == cudaSuccess; ++i) err = cudaEventElapsedTime(&pass_ms[i], ev[i], ev[i + 1]);
+    rc = qeb::cuda_status(err, "apply_local_profiled timing");
+  } else if (rc == QEB_OK) {
+    pass_ms[0] = pass_ms[1] = pass_ms[2] = 0.0f;
+  }
+  for (int i = 0; i < 4; ++i) cudaEventDestroy(ev[i]);
+  return rc;
 }

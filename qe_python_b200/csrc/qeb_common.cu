@@ -1,4 +1,5 @@
 // Error state and host-side FFT factorisation shared by all qe_b200 kernels.
+#include <atomic>
 #include <cstdarg>
 #include <cstring>
 
@@ -21,6 +22,10 @@ int cuda_status(cudaError_t err, const char* where) {
   set_error("%s: %s", where, cudaGetErrorString(err));
   return QEB_ECUDA;
 }
+
+static std::atomic<int64_t> g_launches{0};
+
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 bool make_fft_desc(int n, FftDesc* d) {
   if (n < 1 || n > 1024) return false;
@@ -48,3 +53,5 @@ bool make_fft_desc(int n, FftDesc* d) {
 extern "C" const char* qeb_last_error(void) { return qeb::g_last_error; }
 
 extern "C" int qeb_version(void) { return QEB_ABI_VERSION; }
+
+extern "C" int64_t qeb_launch_count(void) { return qeb::g_launches.load(); }

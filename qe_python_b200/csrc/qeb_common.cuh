@@ -28,6 +28,8 @@ namespace qeb {
 
 void set_error(const char* fmt, ...);
 int cuda_status(cudaError_t err, const char* where);
+// Process-wide count of kernels launched by this library (qeb_launch_count).
+void count_launches(int n);
 
 template <typename T>
 struct alignas(2 * sizeof(T)) C2 {

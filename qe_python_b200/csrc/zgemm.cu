@@ -240,6 +240,7 @@ int gemm(int opa, int M, int N, int K, const double* alpha, const void* A, int64
         M, N, K, kchunk, al, static_cast<const C2<T>*>(A), lda, static_cast<const C2<T>*>(B),
         ldb, be, static_cast<C2<T>*>(C), ldc, partials);
   }
+  qeb::count_launches(splits > 1 ? 2 : 1);
   if (splits > 1) {
     const int64_t total = (int64_t)M * N;
     int blocks = (int)((total + 255) / 256);

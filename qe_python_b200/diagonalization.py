@@ -1,0 +1,467 @@
+"""GPU plane-wave Hamiltonian and block Davidson eigensolver.
+
+Drop-in for qepy_pw/diagonalization.py: ``PlaneWaveHamiltonian`` keeps the
+constructor and ``apply`` / ``apply_into`` / ``diagonal`` of :124-244 and the
+projector term types of :21-43; ``davidson`` keeps the signature and result
+type of :527-548 / :113-121 and follows the algorithm of :527-880 step by
+step.  Vectors are column-major torch CUDA tensors; every contraction runs in
+libqeb200.so (complex GEMMs, FFT passes, column kernels).  The reduced
+Hermitian generalized eigenproblem is solved in FP64 on the device
+(Cholesky reduction + Hermitian eigensolve, the same transformation as
+LAPACK zhegv).
+"""
+
+from __future__ import annotations
+
+from contextlib import nullcontext
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import kernels as K
+from .basis import LocalPotentialWorkspace, PlaneWaveBasis
+from .device import (
+    COMPLEX_OF,
+    REAL_OF,
+    as_numpy,
+    empty_f,
+    require_cuda,
+    to_device_f,
+    zeros_f,
+)
+
+
+@dataclass(frozen=True)
+class FactorizedProjectorTerm:
+    """Species beta functions plus per-atom phase columns (diagonalization.py:21-28)."""
+
+    beta: np.ndarray
+    phases: np.ndarray
+    coupling: np.ndarray
+
+
+@dataclass(frozen=True)
+class PackedProjectorTerm:
+    """Atom-packed beta with a precomputed diagonal (diagonalization.py:31-37)."""
+
+    beta: np.ndarray
+    coupling: np.ndarray
+    diagonal: np.ndarray
+
+
+@dataclass(frozen=True)
+class DavidsonResult:
+    """Same fields as qepy_pw/diagonalization.py:113-121 (eigenvectors on the device)."""
+
+    eigenvalues: np.ndarray
+    eigenvectors: torch.Tensor
+    residual_norms: np.ndarray
+    iterations: float
+    converged: bool
+    number_unconverged: int = 0
+    hamiltonian_applications: int = 0
+
+
+def _timer(timers, name):
+    return timers.measure(name) if timers is not None else nullcontext()
+
+
+class _DeviceProjectors:
+    """All projector terms packed into one device beta (npw, P) and a dense
+    block-diagonal coupling (P, P).
+
+    A factorized term (species beta, per-atom phases) becomes beta * phase per
+    atom: (beta*phase)^H psi equals the reference's conj(beta^T (conj(psi)
+    phase)) (diagonalization.py:294-310) and (beta*phase) D becp equals its
+    (beta D becp) * phase (:362-367).  Packing costs npw*P complex values of
+    HBM, which the GPU holds easily, and turns the per-atom loop into two
+    GEMMs.
+    """
+
+    def __init__(self, terms, npw: int, dtype: torch.dtype, device: torch.device) -> None:
+        betas, couplings, diagonals = [], [], []
+        self.host_diagonal = np.zeros(npw)
+        self.device_diagonal = torch.zeros(npw, dtype=torch.float64, device=device)
+        for term in terms:
+            if isinstance(term, PackedProjectorTerm):
+                beta = to_device_f(term.beta, torch.complex128, device)
+                betas.append(beta)
+                couplings.append(np.asarray(term.coupling))
+                diagonals.append(("packed", term.diagonal))
+            elif isinstance(term, FactorizedProjectorTerm):
+                species = to_device_f(term.beta, torch.complex128, device)
+                phases = to_device_f(term.phases, torch.complex128, device)
+                natoms = phases.shape[1]
+                c = species.shape[1]
+                packed = empty_f(npw, natoms * c, torch.complex128, device)
+                for atom in range(natoms):
+                    packed[:, atom * c:(atom + 1) * c] = species * phases[:, atom:atom + 1]
+                betas.append(packed)
+                couplings.append(np.kron(np.eye(natoms), np.asarray(term.coupling)))
+                diagonals.append(("factorized", species, np.asarray(term.coupling), natoms))
+            else:
+                beta, coupling = term
+                beta = to_device_f(beta, torch.complex128, device)
+                betas.append(beta)
+                couplings.append(np.asarray(coupling))
+                diagonals.append(("materialized", beta, np.asarray(coupling), 1))
+        self.channels = sum(b.shape[1] for b in betas)
+        if self.channels == 0:
+            self.beta = None
+            self.coupling = None
+        else:
+            beta = empty_f(npw, self.channels, torch.complex128, device)
+            coupling = np.zeros((self.channels, self.channels), dtype=np.complex128)
+            offset = 0
+            for b, c in zip(betas, couplings):
+                n = b.shape[1]
+                beta[:, offset:offset + n] = b
+                coupling[offset:offset + n, offset:offset + n] = c
+                offset += n
+            self.beta = beta.to(dtype) if dtype != torch.complex128 else beta
+            if dtype != torch.complex128:
+                self.beta = self.beta.T.contiguous().T
+            self.coupling = to_device_f(coupling, dtype, device)
+        # Preconditioner diagonal (diagonalization.py:205-229).
+        for entry in diagonals:
+            if entry[0] == "packed":
+                self.device_diagonal += to_device_f(entry[1], torch.float64, device)
+                continue
+            _kind, beta, coupling, multiplicity = entry
+            coupled = K.gemm(K.OP_N, beta, to_device_f(coupling.astype(np.complex128),
+                                                       torch.complex128, device))
+            K.accumulate_projector_diagonal(self.device_diagonal, coupled, beta,
+                                            float(multiplicity))
+
+
+class PlaneWaveHamiltonian:
+    """H = T + V_loc + sum |beta> D <beta| applied on the GPU.
+
+    Same constructor as qepy_pw/diagonalization.py:127-203 plus ``precision``
+    ('f64' plain or 'f32' chosen form; taken from ``local_workspace`` when
+    given).
+    """
+
+    def __init__(self, basis: PlaneWaveBasis, potential_g, projector_terms=(),
+                 local_workspace: LocalPotentialWorkspace | None = None, timers=None,
+                 real_potential=None, native_potential_layout: bool = False,
+                 potential_average: float | None = None, precision: str | None = None) -> None:
+        self.basis = basis
+        self.potential_g = potential_g
+        if local_workspace is None:
+            shape = np.asarray(potential_g).shape if np.ndim(potential_g) == 3 else None
+            if shape is None:
+                raise ValueError("a local workspace or a 3-D potential_g is required")
+            local_workspace = LocalPotentialWorkspace(basis, shape, precision=precision or "f64")
+        elif precision is not None and precision != local_workspace.precision:
+            raise ValueError("precision disagrees with the local workspace")
+        self.local_workspace = local_workspace
+        self.precision = local_workspace.precision
+        self.dtype = local_workspace.complex_dtype
+        self.device = local_workspace.device
+        self.timers = timers
+        self.native_potential_layout = bool(native_potential_layout)
+        if real_potential is None:
+            real_potential = local_workspace.prepare_potential(potential_g)
+            self.native_potential_layout = False
+        self.real_potential = real_potential
+        if potential_average is None:
+            potential_average = float(np.real(np.asarray(potential_g).flat[0]))
+        self.potential_average = float(potential_average)
+        self.mpi = None
+        self.local_rows = np.arange(len(basis), dtype=np.int32)
+        kinetic = np.asarray(basis.kinetic, dtype=float)
+        self.local_kinetic = kinetic
+        self._kinetic = torch.from_numpy(kinetic).to(self.device)
+        self._kinetic_kernel = self._kinetic.to(REAL_OF[self.dtype])
+        self._potential = local_workspace.native_potential(real_potential, self.native_potential_layout)
+        self.projectors = _DeviceProjectors(projector_terms, len(basis), self.dtype, self.device)
+        self.projector_terms = tuple(projector_terms)
+        self._diagonal_device = self._kinetic + self.potential_average + self.projectors.device_diagonal
+
+    @property
+    def diagonal(self) -> torch.Tensor:
+        """T + v_of_0 + projector diagonal on the device (usnldiag; :205-229)."""
+        return self._diagonal_device
+
+    def apply(self, coefficients):
+        with _timer(self.timers, "h_psi"):
+            return self._apply(coefficients)
+
+    def apply_into(self, coefficients, out):
+        with _timer(self.timers, "h_psi"):
+            return self._apply(coefficients, out=out)
+
+    def _apply(self, coefficients, out=None):
+        host = not isinstance(coefficients, torch.Tensor)
+        vectors = to_device_f(coefficients, self.dtype, self.device)
+        was_vector = vectors.dim() == 1
+        if was_vector:
+            vectors = vectors[:, None]
+        target = None
+        if out is not None and isinstance(out, torch.Tensor):
+            target = out[:, None] if out.dim() == 1 else out
+        if target is None:
+            target = empty_f(vectors.shape[0], vectors.shape[1], self.dtype, self.device)
+        with _timer(self.timers, "vloc_psi"):
+            self.local_workspace._launch_apply(self._potential, vectors, self._kinetic_kernel, target)
+        if self.projectors.beta is not None and vectors.shape[1] > 0:
+            with _timer(self.timers, "h_psi:calbec"):
+                becp = K.gemm(K.OP_C, self.projectors.beta, vectors)
+            with _timer(self.timers, "add_vuspsi"):
+                coupled = K.gemm(K.OP_N, self.projectors.coupling, becp)
+                K.gemm(K.OP_N, self.projectors.beta, coupled, target, beta=1.0)
+        if host:
+            result = as_numpy(target)
+            if out is not None and not isinstance(out, torch.Tensor):
+                out[...] = result.reshape(out.shape)
+                result = out
+            return result[:, 0] if was_vector and result.ndim == 2 else result
+        return target[:, 0] if was_vector else target
+
+
+# ---------------------------------------------------------------------------
+# Davidson
+
+
+def _hermitize(a: torch.Tensor) -> torch.Tensor:
+    return 0.5 * (a + a.conj().T)
+
+
+def lowest_generalized_eigh(h: torch.Tensor, s: torch.Tensor, roots: int):
+    """Lowest ``roots`` pairs of H x = e S x in FP64 on the device.
+
+    Cholesky S = L L^H, reduced L^-1 H L^-H, Hermitian eigensolve, back
+    transform (the transformation of LAPACK zhegv; reference fallback
+    qepy_pw/diagonalization.py:83-110).
+    """
+    h = h.to(torch.complex128)
+    s = s.to(torch.complex128)
+    lower, info = torch.linalg.cholesky_ex(s)
+    if int(info) != 0:
+        raise np.linalg.LinAlgError("overlap matrix is not positive definite")
+    left = torch.linalg.solve_triangular(lower, h, upper=False)
+    reduced = torch.linalg.solve_triangular(lower, left.conj().T, upper=False).conj().T
+    values, vectors = torch.linalg.eigh(_hermitize(reduced))
+    vectors = torch.linalg.solve_triangular(lower.conj().T, vectors, upper=True)
+    return values[:roots], vectors[:, :roots]
+
+
+def _orthonormalize(block: torch.Tensor, threshold: float = 1.0e-12) -> torch.Tensor:
+    """Rank-revealing orthonormal basis of the block's span (:370-472, serial)."""
+    if block.shape[1] == 0:
+        return block
+    wide = block.to(torch.complex128)
+    if block.shape[1] == 1:
+        norm = float(torch.linalg.vector_norm(wide))
+        if norm == 0.0:
+            return block[:, :0]
+        return (wide / norm).to(block.dtype)
+    gram = _hermitize(K.gemm(K.OP_C, wide, wide))
+    squared, rotation = torch.linalg.eigh(gram)
+    order = torch.argsort(squared, descending=True)
+    squared = torch.clamp(squared[order].real, min=0.0)
+    if squared.numel() == 0 or float(squared[0]) == 0.0:
+        return block[:, :0]
+    rank = int(torch.count_nonzero(squared > threshold ** 2 * squared[0]))
+    transform = rotation[:, order[:rank]] / torch.sqrt(squared[:rank])[None, :]
+    result = K.gemm(K.OP_N, wide, transform.T.contiguous().T)
+    return result.to(block.dtype) if block.dtype != torch.complex128 else result
+
+
+def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
+             tolerance: float = 1.0e-8, max_iterations: int = 40, subspace_multiplier: int = 4,
+             residual_factor: float | None = 10.0, residual_energy_scale: float | None = None,
+             occupied_roots: int | None = None, initial_is_ritz: bool = False,
+             initial_is_orthonormal: bool = False, initial_eigenvalues=None,
+             initial_applied=None, mpi=None, global_dimension: int | None = None,
+             global_row_indices=None, timers=None, operator_into=None,
+             dtype: torch.dtype | None = None) -> DavidsonResult:
+    """Lowest eigenpairs by restarted block Davidson (diagonalization.py:527-880).
+
+    ``operator(C)`` / ``operator_into(C, out)`` act on column-major device
+    tensors.  ``dtype`` selects the basis precision (default complex128, or
+    the dtype of ``initial_vectors`` when it is a tensor).
+    """
+    device = require_cuda()
+    diag = to_device_f(diagonal, torch.float64, device).reshape(-1)
+    local_dimension = diag.numel()
+    dimension = int(global_dimension) if global_dimension is not None else local_dimension
+    if not 1 <= number_of_roots <= dimension:
+        raise ValueError("number_of_roots must be between 1 and the matrix size")
+    if tolerance <= 0.0:
+        raise ValueError("Davidson tolerance must be positive")
+    if max_iterations < 1:
+        raise ValueError("Davidson max_iterations must be at least 1")
+    if subspace_multiplier < 2:
+        raise ValueError("diago_david_ndim must be at least 2")
+    if residual_factor is not None and residual_factor <= 0.0:
+        raise ValueError("Davidson residual_factor must be positive or None")
+    if residual_energy_scale is not None and residual_energy_scale <= 0.0:
+        raise ValueError("Davidson residual_energy_scale must be positive or None")
+    if occupied_roots is None:
+        occupied_roots = number_of_roots
+    if not 0 <= occupied_roots <= number_of_roots:
+        raise ValueError("occupied_roots must be between zero and number_of_roots")
+    root_tolerances = np.full(number_of_roots, max(5.0 * tolerance, 5.0e-6))
+    root_tolerances[:occupied_roots] = tolerance
+    if dtype is None:
+        dtype = initial_vectors.dtype if isinstance(initial_vectors, torch.Tensor) and \
+            initial_vectors.is_complex() else torch.complex128
+
+    if initial_vectors is None:
+        rows = np.arange(local_dimension) if global_row_indices is None else \
+            np.asarray(global_row_indices, dtype=int)
+        trial_host = np.zeros((local_dimension, number_of_roots), dtype=np.complex128, order="F")
+        for column in range(number_of_roots):
+            matches = np.flatnonzero(rows == column)
+            if len(matches):
+                trial_host[matches[0], column] = 1.0
+        trial = to_device_f(trial_host, dtype, device)
+    else:
+        trial = to_device_f(initial_vectors, dtype, device)
+        if trial.dim() != 2 or trial.shape[0] != local_dimension or trial.shape[1] < number_of_roots:
+            raise ValueError("initial_vectors must have shape (matrix size, at least number_of_roots)")
+
+    if initial_is_ritz or initial_is_orthonormal:
+        basis0 = trial[:, :number_of_roots]
+    else:
+        with _timer(timers, "cegterg:over"):
+            basis0 = _orthonormalize(trial)
+    if basis0.shape[1] < number_of_roots:
+        raise ValueError("initial Davidson vectors are linearly dependent")
+    maximum_subspace = min(dimension, max(basis0.shape[1], 2 * number_of_roots,
+                                          subspace_multiplier * number_of_roots))
+    active = basis0.shape[1]
+    basis_storage = empty_f(local_dimension, maximum_subspace, dtype, device)
+    applied_storage = empty_f(local_dimension, maximum_subspace, dtype, device)
+    basis_storage[:, :active] = basis0
+    del basis0, trial
+
+    def apply_into(vectors, destination):
+        if operator_into is not None:
+            operator_into(vectors, destination)
+        else:
+            destination[...] = operator(vectors)
+
+    if initial_applied is None:
+        apply_into(basis_storage[:, :active], applied_storage[:, :active])
+        applications = active
+    else:
+        supplied = to_device_f(initial_applied, dtype, device)
+        if tuple(supplied.shape) != (local_dimension, active):
+            raise ValueError("initial_applied must match the initial Ritz block")
+        applied_storage[:, :active] = supplied
+        applications = 0
+    projected = torch.zeros((maximum_subspace, maximum_subspace), dtype=torch.complex128, device=device)
+    overlap = torch.zeros_like(projected)
+
+    def update_projected(first_new: int) -> None:
+        """New rows/columns of V^H H V and V^H V (:658-695)."""
+        with _timer(timers, "cegterg:over"):
+            new = basis_storage[:, first_new:active]
+            h_rows = K.gemm(K.OP_C, new, applied_storage[:, :active]).to(torch.complex128)
+            s_rows = K.gemm(K.OP_C, new, basis_storage[:, :active]).to(torch.complex128)
+            projected[first_new:active, :active] = h_rows
+            overlap[first_new:active, :active] = s_rows
+            if first_new:
+                projected[:first_new, first_new:active] = h_rows[:, :first_new].conj().T
+                overlap[:first_new, first_new:active] = s_rows[:, :first_new].conj().T
+            block = slice(first_new, active)
+            projected[block, block] = _hermitize(projected[block, block])
+            overlap[block, block] = _hermitize(overlap[block, block])
+
+    def ritz_pairs():
+        """Ritz values, vectors V c and residuals HV c - e V c (:699-726)."""
+        with _timer(timers, "cdiaghg"):
+            roots, coefficients = lowest_generalized_eigh(
+                projected[:active, :active], overlap[:active, :active], number_of_roots)
+        with _timer(timers, "cegterg:upda"):
+            coeff = coefficients.to(dtype).T.contiguous().T
+            vectors = K.gemm(K.OP_N, basis_storage[:, :active], coeff)
+            residual = K.gemm(K.OP_N, applied_storage[:, :active], coeff)
+            K.subtract_band_energies(residual, vectors, roots)
+        return roots.cpu().numpy(), roots, vectors, residual
+
+    update_projected(0)
+    if initial_is_ritz:
+        if initial_eigenvalues is None:
+            values_dev = K.column_inner_products(
+                basis_storage[:, :number_of_roots], applied_storage[:, :number_of_roots]).real
+        else:
+            values_dev = torch.as_tensor(np.asarray(initial_eigenvalues[:number_of_roots], dtype=float),
+                                         device=device)
+        values = values_dev.cpu().numpy()
+        ritz_vectors = basis_storage[:, :number_of_roots].clone()
+        residuals = applied_storage[:, :number_of_roots].clone()
+        K.subtract_band_energies(residuals, ritz_vectors, values_dev)
+    else:
+        values, values_dev, ritz_vectors, residuals = ritz_pairs()
+    track = residual_factor is not None or residual_energy_scale is not None
+
+    def residual_norms_of(block):
+        return np.sqrt(np.maximum(K.column_squared_norms(block).cpu().numpy(), 0.0))
+
+    residual_norms = residual_norms_of(residuals) if track else np.empty(number_of_roots)
+    completed = 0
+    unconverged_count = number_of_roots
+    unconverged = np.ones(number_of_roots, dtype=bool)
+
+    for iteration in range(1, max_iterations + 1):
+        completed = iteration
+        previous = values
+        with _timer(timers, "g_psi"):
+            if unconverged.all():
+                block, energies = residuals, values_dev
+            else:
+                index = torch.as_tensor(np.flatnonzero(unconverged), device=device)
+                block = residuals.index_select(1, index).T.contiguous().T
+                energies = values_dev.index_select(0, index)
+            corrections = K.precondition(block, energies, diag)
+        # Normalise (cegterg), dropping columns below 1e-14 of the largest norm (:500-524).
+        norms2 = K.column_squared_norms(corrections)
+        norms_host = norms2.cpu().numpy()
+        if not len(norms_host):
+            break
+        scale = max(float(np.max(norms_host)), 1.0e-300)
+        keep = np.flatnonzero(norms_host > (1.0e-14 ** 2) * scale)
+        if keep.size == 0:
+            break
+        old = active
+        active += keep.size
+        selected = torch.as_tensor(keep.astype(np.int64), device=device)
+        K.normalize_columns(corrections, norms2, selected, basis_storage[:, old:active])
+        del ritz_vectors, residuals, corrections, block
+        apply_into(basis_storage[:, old:active], applied_storage[:, old:active])
+        applications += keep.size
+        update_projected(old)
+        values, values_dev, ritz_vectors, residuals = ritz_pairs()
+        if track:
+            residual_norms = residual_norms_of(residuals)
+        converged = np.abs(values - previous) < root_tolerances
+        if residual_factor is not None:
+            converged &= residual_norms < residual_factor * root_tolerances
+        if residual_energy_scale is not None:
+            converged &= residual_norms ** 2 < residual_energy_scale * root_tolerances
+        unconverged = ~converged
+        unconverged_count = int(np.count_nonzero(unconverged))
+        if unconverged_count == 0:
+            if not track:
+                residual_norms = residual_norms_of(residuals)
+            return DavidsonResult(values, ritz_vectors, residual_norms, iteration, True, 0,
+                                  applications)
+        if active + unconverged_count > maximum_subspace:
+            # Restart on the Ritz block without a new H application (:843-868).
+            with _timer(timers, "cegterg:last"):
+                active = number_of_roots
+                basis_storage[:, :active] = ritz_vectors
+                # H psi = residual + e psi, rebuilt in place (:855-860).
+                applied_storage[:, :active] = residuals
+                K.subtract_band_energies(applied_storage[:, :active], ritz_vectors, -values_dev)
+                projected[:active, :active] = torch.diag(values_dev.to(torch.complex128))
+                overlap[:active, :active] = torch.eye(active, dtype=torch.complex128, device=device)
+    if not track:
+        residual_norms = residual_norms_of(residuals)
+    return DavidsonResult(values, ritz_vectors, residual_norms, completed, False,
+                          unconverged_count, applications)

@@ -162,3 +162,19 @@ def subtract_band_energies(residual: torch.Tensor, v: torch.Tensor,
         _precision(v), v.shape[0], v.shape[1], residual.data_ptr(), leading_dimension(residual),
         v.data_ptr(), leading_dimension(v), e.data_ptr(), stream_handle()))
     return residual
+
+
+def accumulate_projector_diagonal(diagonal: torch.Tensor, coupled: torch.Tensor,
+                                  beta: torch.Tensor, multiplicity: float) -> torch.Tensor:
+    """diag += m Re sum_i coupled[:, i] conj(beta[:, i]) (qepy_pw/_native_fft.pyx:734-779)."""
+    _check_matrix("coupled", coupled)
+    _check_matrix("beta", beta)
+    if coupled.shape != beta.shape or diagonal.numel() != beta.shape[0]:
+        raise ValueError("projector diagonal operands disagree")
+    if diagonal.dtype != torch.float64 or not diagonal.is_contiguous():
+        raise ValueError("diagonal must be contiguous float64")
+    _lib.check("qeb_accumulate_projector_diagonal", _lib.load().qeb_accumulate_projector_diagonal(
+        _precision(beta), beta.shape[0], beta.shape[1], coupled.data_ptr(),
+        leading_dimension(coupled), beta.data_ptr(), leading_dimension(beta),
+        float(multiplicity), diagonal.data_ptr(), stream_handle()))
+    return diagonal
