@@ -29,6 +29,8 @@ def stream_handle(stream: torch.cuda.Stream | None = None) -> int:
 
 
 def is_column_major(t: torch.Tensor) -> bool:
+    if t.numel() == 0:
+        return t.dim() in (1, 2)
     if t.dim() == 1:
         return t.stride(0) == 1
     return t.dim() == 2 and t.stride(0) == 1 and (t.shape[1] <= 1 or t.stride(1) >= t.shape[0])
@@ -36,7 +38,7 @@ def is_column_major(t: torch.Tensor) -> bool:
 
 def leading_dimension(t: torch.Tensor) -> int:
     """Column stride of a column-major matrix (any value >= rows for one column)."""
-    if t.dim() == 1:
+    if t.dim() == 1 or t.numel() == 0:
         return max(1, t.shape[0])
     if t.shape[1] <= 1:
         return max(1, t.shape[0], t.stride(1))

@@ -1,0 +1,235 @@
+"""Generate the golden fixtures of tests/golden/ from the reference.
+
+Runs in the build container only: imports the reference qepy-pw package
+(QEPY_REFERENCE_ROOT, default the read-only mount) with the NumPy oracle as
+its native module (reference_env.py) and records its outputs:
+
+  index_maps.json       per benchmark cell: k points, weights, FFT grid,
+                        plane waves per k and SHA-256 of every basis' Miller
+                        array and of the shared catalog (bit-exact pins)
+  index_maps_fcc2.npz   full Miller arrays and serial slot maps of scf-fcc2
+  hamiltonian_small.npz reference PlaneWaveHamiltonian.apply on a small cell
+                        (factorized, packed and materialised projector terms)
+  davidson_small.npz    reference davidson on the same operator
+  scf_fcc2.json         reference SCF of scf-fcc2 (energy, bands, iterations)
+  scf_dia8_disp.json    reference SCF + forces of scf-dia8-disp
+  si_regression.json    the reference's own recorded Si regression numbers
+                        (tests/qe_reference/reference/pw_scf/scf.in.out)
+
+Usage: python tests/golden/make_golden.py [--skip-scf]
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import re
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REPO = HERE.parents[1]
+sys.path.insert(0, str(REPO))
+
+from tests.golden.reference_env import REFERENCE_ROOT, load_reference  # noqa: E402
+
+
+def sha(array: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(array, dtype=np.int32).tobytes()).hexdigest()
+
+
+def read_config(name: str, workdir: Path):
+    from qepy_pw.input import read_pw_input
+
+    from qe_python_b200.configs import ELECTRON_OVERRIDES, config_input
+    from qe_python_b200.pseudo import write_synthetic_upf
+
+    write_synthetic_upf(workdir / "X.upf")
+    path = workdir / f"{name}.in"
+    path.write_text(config_input(name, str(workdir)))
+    pw = read_pw_input(path)
+    pw.electrons.update(ELECTRON_OVERRIDES.get(name, {}))
+    return pw
+
+
+def index_maps(workdir: Path) -> None:
+    from qepy_pw.basis import LocalPotentialWorkspace, fft_shape, make_bases
+    from qepy_pw.symmetry import fft_factors
+
+    from qe_python_b200.configs import CONFIGS
+    from qe_python_b200.workloads import hpsi_microbench
+
+    out = {}
+    for name in CONFIGS:
+        pw = read_config(name, workdir)
+        kpoints = np.array([p.crystal for p in pw.kpoints])
+        weights = np.array([p.weight for p in pw.kpoints])
+        ecut = float(pw.system["ecutwfc"])
+        ecutrho = float(pw.system.get("ecutrho", 4.0 * ecut))
+        bases = make_bases(pw.reciprocal, kpoints, ecut)
+        factors = fft_factors(pw.symmetry_operations,
+                              use_all_frac=bool(pw.system.get("use_all_frac", False)))
+        shape = fft_shape(bases, pw.reciprocal, ecutrho, factors)
+        out[name] = {
+            "reciprocal": pw.reciprocal.tolist(),
+            "kpoints": kpoints.tolist(), "weights": weights.tolist(),
+            "ecutwfc": ecut, "ecutrho": ecutrho, "fft_factors": list(map(int, factors)),
+            "fft_shape": list(map(int, shape)), "npw": [len(b) for b in bases],
+            "miller_sha256": [sha(b.indices) for b in bases],
+            "catalog_sha256": sha(bases[0].catalog.indices),
+        }
+        if name == "scf-fcc2":
+            ws = LocalPotentialWorkspace(bases[0], shape, retain_serial_sticks=True)
+            np.savez_compressed(
+                HERE / "index_maps_fcc2.npz",
+                miller=np.concatenate([b.indices for b in bases]),
+                offsets=np.cumsum([0] + [len(b) for b in bases]),
+                linear_slots=ws.linear_slots, z_major_slots=ws.z_major_slots,
+                stick_positions=ws.serial_stick_positions, sticks=ws.sticks,
+            )
+        print(f"{name}: {len(bases)} k, grid {shape}, npw {[len(b) for b in bases][:4]}...")
+    work = hpsi_microbench(nbands=1)
+    from qepy_pw.basis import make_bases as ref_make_bases
+
+    basis = ref_make_bases(work.reciprocal, np.zeros(3), 30.0)[0]
+    shape = fft_shape([basis], work.reciprocal, 150.0)
+    out["hpsi-microbench"] = {
+        "reciprocal": work.reciprocal.tolist(), "kpoints": [[0.0, 0.0, 0.0]], "weights": [2.0],
+        "ecutwfc": 30.0, "ecutrho": 150.0, "fft_factors": [1, 1, 1],
+        "fft_shape": list(map(int, shape)), "npw": [len(basis)],
+        "miller_sha256": [sha(basis.indices)], "catalog_sha256": sha(basis.catalog.indices),
+    }
+    (HERE / "index_maps.json").write_text(json.dumps(out, indent=1))
+
+
+def small_operator():
+    """A small fcc cell with all three projector term kinds (seeded)."""
+    from qepy_pw.basis import fft_shape, make_bases
+
+    lattice = 10.26 / 2.0 * np.array([[-1.0, 0.0, 1.0], [0.0, 1.0, 1.0], [-1.0, 1.0, 0.0]])
+    reciprocal = 2.0 * np.pi * np.linalg.inv(lattice).T
+    k = np.array([0.125, 0.375, -0.25])
+    basis = make_bases(reciprocal, k, 20.0)[0].materialize()
+    shape = fft_shape([basis], reciprocal, 80.0)
+    rng = np.random.default_rng(20261203)
+    npw = len(basis)
+    decay = 0.05 * np.exp(-basis.kinetic / 3.0)[:, None]
+    species = np.asfortranarray((rng.standard_normal((npw, 4)) + 1j * rng.standard_normal((npw, 4))) * decay)
+    positions = rng.uniform(0.0, 5.0, (3, 3))
+    phases = np.asfortranarray(np.exp(-1j * basis.vectors @ positions.T))
+    d = rng.uniform(-1.0, 1.0, (4, 4))
+    coupling = 0.5 * (d + d.T)
+    packed_beta = np.asfortranarray((rng.standard_normal((npw, 6)) + 1j * rng.standard_normal((npw, 6))) * decay)
+    d6 = rng.uniform(-1.0, 1.0, (6, 6))
+    packed_coupling = 0.5 * (d6 + d6.T)
+    packed_diag = np.real(np.einsum("gi,ij,gj->g", packed_beta, packed_coupling, packed_beta.conj()))
+    mat_beta = np.asfortranarray((rng.standard_normal((npw, 2)) + 1j * rng.standard_normal((npw, 2))) * decay)
+    mat_coupling = np.array([[0.7, 0.1], [0.1, -0.4]])
+    potential = np.ascontiguousarray(rng.uniform(-0.6, 0.6, shape))
+    psi = np.asfortranarray(rng.standard_normal((npw, 6)) + 1j * rng.standard_normal((npw, 6)))
+    return dict(reciprocal=reciprocal, k=k, ecut=20.0, shape=np.array(shape), miller=basis.indices,
+                kinetic=basis.kinetic, species=species, phases=phases, coupling=coupling,
+                packed_beta=packed_beta, packed_coupling=packed_coupling, packed_diag=packed_diag,
+                mat_beta=mat_beta, mat_coupling=mat_coupling, potential=potential, psi=psi)
+
+
+def hamiltonian_and_davidson() -> None:
+    from qepy_pw.basis import LocalPotentialWorkspace, PlaneWaveBasis
+    from qepy_pw.diagonalization import (
+        FactorizedProjectorTerm,
+        PackedProjectorTerm,
+        PlaneWaveHamiltonian,
+        davidson,
+    )
+
+    s = small_operator()
+    basis = PlaneWaveBasis(s["miller"], None, s["kinetic"])
+    object.__setattr__(basis, "_legacy_vectors", np.zeros((len(s["miller"]), 3)))
+    shape = tuple(int(v) for v in s["shape"])
+    ws = LocalPotentialWorkspace(s["miller"], shape)
+    terms = (
+        FactorizedProjectorTerm(s["species"], s["phases"], s["coupling"]),
+        PackedProjectorTerm(s["packed_beta"], s["packed_coupling"], s["packed_diag"]),
+        (s["mat_beta"], s["mat_coupling"]),
+    )
+    h = PlaneWaveHamiltonian(basis, np.zeros(shape, dtype=complex), terms, local_workspace=ws,
+                             real_potential=s["potential"], potential_average=0.125)
+    hpsi = h.apply(s["psi"])
+    diagonal = h.diagonal
+    rng = np.random.default_rng(7)
+    start = np.asfortranarray(rng.standard_normal((len(basis), 8)) + 1j * rng.standard_normal((len(basis), 8)))
+    result = davidson(h.apply, diagonal, 8, initial_vectors=start, tolerance=1e-9,
+                      max_iterations=100, subspace_multiplier=2, residual_factor=None,
+                      operator_into=h.apply_into)
+    np.savez_compressed(HERE / "hamiltonian_small.npz", hpsi=hpsi, diagonal=diagonal, **s)
+    np.savez_compressed(HERE / "davidson_small.npz", start=start,
+                        eigenvalues=result.eigenvalues, iterations=result.iterations,
+                        converged=result.converged,
+                        applications=result.hamiltonian_applications)
+    print("davidson:", result.iterations, result.converged, result.eigenvalues[:3])
+
+
+def scf(name: str, workdir: Path, filename: str) -> None:
+    from qepy_pw.scf import run_scf
+
+    pw = read_config(name, workdir)
+    started = time.perf_counter()
+    result = run_scf(pw)
+    elapsed = time.perf_counter() - started
+    record = {
+        "config": name,
+        "total_energy_ry": 2.0 * float(result.iterations[-1].total_energy_ha),
+        "iterations": len(result.iterations),
+        "energies_ry": [2.0 * float(it.total_energy_ha) for it in result.iterations],
+        "estimated_accuracy_ry": [2.0 * float(it.estimated_accuracy_ha) for it in result.iterations],
+        "davidson_thresholds_ha": [float(it.davidson_threshold_ha) for it in result.iterations],
+        "average_davidson_iterations": [float(it.average_diagonalization_iterations)
+                                        for it in result.iterations],
+        "eigenvalues_ry": [[2.0 * float(e) for e in k] for k in result.eigenvalues_ha],
+        "energy_terms_ry": {k: 2.0 * float(v) for k, v in vars(result.energy_terms).items()},
+        "forces_ry_per_bohr": None if result.forces_ha_per_bohr is None
+        else (2.0 * np.asarray(result.forces_ha_per_bohr)).tolist(),
+        "reference_wall_seconds": elapsed,
+        "reference_runner": "reference Python + NumPy oracle native module, 1 process",
+    }
+    (HERE / filename).write_text(json.dumps(record, indent=1))
+    print(f"{name}: E = {record['total_energy_ry']:.10f} Ry in {elapsed:.1f} s, "
+          f"{record['iterations']} iterations")
+
+
+def si_regression() -> None:
+    path = REFERENCE_ROOT / "tests/qe_reference/reference/pw_scf/scf.in.out"
+    text = path.read_text()
+    energy = float(re.search(r"!\s+total energy\s+=\s+(-?\d+\.\d+)\s+Ry", text).group(1))
+    blocks = re.findall(r"k =.*?bands \(ev\):\s*\n\s*\n(.*?)\n\s*\n", text, flags=re.S)
+    bands = [[float(v) for v in b.split()] for b in blocks]
+    record = {"source": "tests/qe_reference/reference/pw_scf/scf.in.out",
+              "input": "tests/qe_reference/upstream/pw_scf/scf.in",
+              "total_energy_ry": energy, "bands_ev": bands,
+              "tolerance_ry": 5.0e-8}
+    (HERE / "si_regression.json").write_text(json.dumps(record, indent=1))
+    print("si regression:", energy, bands)
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--skip-scf", action="store_true")
+    args = parser.parse_args()
+    load_reference()
+    with tempfile.TemporaryDirectory() as tmp:
+        workdir = Path(tmp)
+        index_maps(workdir)
+        hamiltonian_and_davidson()
+        si_regression()
+        if not args.skip_scf:
+            scf("scf-fcc2", workdir, "scf_fcc2.json")
+            scf("scf-dia8-disp", workdir, "scf_dia8_disp.json")
+
+
+if __name__ == "__main__":
+    main()
