@@ -111,6 +111,26 @@ int qeb_cgemm(int opa, int M, int N, int K, const double* alpha, const void* A, 
               const void* B, int64_t ldb, const double* beta, void* C, int64_t ldc,
               void* scratch, int64_t scratch_bytes, void* stream);
 
+/* Allocation-free C = alpha * A^H * B + beta * C (complex128, A is K x M).
+ * No counterpart in the reference: an addition for callers that cannot call
+ * cudaMalloc themselves (code running inside a device memory pool it does
+ * not own, or a host program whose allocator is reserved for its own data).
+ * The split-K partial tiles live in a 16 MiB file-scope __device__ array
+ * that every GPU loading this library holds until the process exits
+ * (qeb_zgemm_static_scratch_capacity() returns its size); the call itself
+ * allocates nothing.  It rejects M*N > capacity/32 (two complex128 partial
+ * slices must fit) with QEB_STATUS_EUNSUPPORTED.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress) with that
+ * device current; make that first call before any stream capture.  All
+ * calls share the one array and each call overwrites every partial entry it
+ * reads, so nothing needs clearing between calls; calls that overlap on the
+ * GPU (different streams, or different host threads) race on the array and
+ * must be serialised by the caller. */
+int64_t qeb_zgemm_static_scratch_capacity(void);
+int qeb_zgemm_static_scratch(int M, int N, int K, const double* alpha, const void* A,
+                             int64_t lda, const void* B, int64_t ldb, const double* beta,
+                             void* C, int64_t ldc, void* stream);
+
 /* ------------------------------------------------------------------------
  * Davidson column kernels (precision QEB_F64 / QEB_F32 selects the vector
  * type; reductions accumulate in FP64; eigenvalues, diagonals and norms

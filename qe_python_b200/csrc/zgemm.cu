@@ -14,6 +14,8 @@
 // qepy_pw/_native_fft.pyx:694-731), add_projector_product (ZGEMM beta=1,
 // :782-836), the Davidson reduced-matrix and Ritz products
 // (qepy_pw/diagonalization.py:658-726) and coupling @ overlaps (:348).
+#include <mutex>
+
 #include "qeb_common.cuh"
 #include "../../include/qe_b200.h"
 
@@ -272,4 +274,67 @@ extern "C" int qeb_cgemm(int opa, int M, int N, int K, const double* alpha, cons
                          int64_t ldc, void* scratch, int64_t scratch_bytes, void* stream) {
   return gemm<float>(opa, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, scratch, scratch_bytes,
                      static_cast<cudaStream_t>(stream));
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the split-K product C = alpha A^H B + beta C.
+//
+// For callers that must not allocate device memory themselves, for example a
+// host code that runs inside a memory pool it does not own, a process whose
+// allocator is reserved for other data, or a driver that forbids cudaMalloc
+// between set-up and shutdown.  Instead of caller scratch, the partial K
+// tiles live in the fixed array below, which every GPU that loads this
+// library holds until the process exits.
+namespace {
+
+constexpr int64_t kStaticPartialBytes = 16ll << 20;  // 16 MiB per device
+constexpr int kMaxDevices = 64;
+
+__device__ __align__(256) unsigned char g_static_partials[kStaticPartialBytes];
+
+std::mutex g_static_mutex;
+void* g_static_address[kMaxDevices] = {nullptr};
+
+// Device address of g_static_partials on the current device.  The host-side
+// symbol is only a stand-in, so the address is looked up once per device
+// (with that device current) and cached.
+int static_partials(void** out) {
+  int device = 0;
+  cudaError_t err = cudaGetDevice(&device);
+  if (err != cudaSuccess) return qeb::cuda_status(err, "zgemm_static_scratch: cudaGetDevice");
+  if (device < 0 || device >= kMaxDevices) {
+    qeb::set_error("zgemm_static_scratch: device index %d above %d", device, kMaxDevices);
+    return QEB_EUNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(g_static_mutex);
+  if (g_static_address[device] == nullptr) {
+    void* address = nullptr;
+    err = cudaGetSymbolAddress(&address, g_static_partials);
+    if (err != cudaSuccess) return qeb::cuda_status(err, "zgemm_static_scratch: cudaGetSymbolAddress");
+    g_static_address[device] = address;
+  }
+  *out = g_static_address[device];
+  return QEB_OK;
+}
+
+}  // namespace
+
+extern "C" int64_t qeb_zgemm_static_scratch_capacity(void) { return kStaticPartialBytes; }
+
+extern "C" int qeb_zgemm_static_scratch(int M, int N, int K, const double* alpha, const void* A,
+                                        int64_t lda, const void* B, int64_t ldb,
+                                        const double* beta, void* C, int64_t ldc, void* stream) {
+  // Two partial slices of M x N complex128 values must fit the array.
+  if (M > 0 && N > 0 && (int64_t)M * N * 16 * 2 > kStaticPartialBytes) {
+    qeb::set_error(
+        "zgemm_static_scratch: M*N = %lld exceeds the %lld complex128 entries the static "
+        "partial buffer allows (M*N*16*2 <= %lld bytes)",
+        (long long)M * N, (long long)(kStaticPartialBytes / 32), (long long)kStaticPartialBytes);
+    return QEB_EUNSUPPORTED;
+  }
+  void* scratch = nullptr;
+  const int rc = static_partials(&scratch);
+  if (rc != QEB_OK) return rc;
+  return gemm<double>(QEB_OP_C, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, scratch,
+                      kStaticPartialBytes, static_cast<cudaStream_t>(stream));
 }
