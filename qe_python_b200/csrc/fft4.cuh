@@ -1,0 +1,156 @@
+// Register-resident four-step line FFTs with compile-time factors.
+//
+// A line of length n = N1 * N2 is owned by G = max(N1, N2) consecutive lanes
+// of one warp ("a line group"); a warp holds floor(32 / G) groups.  Two data
+// distributions are used:
+//   D1: lane j (j < N2) holds x[j + N2 * i], i < N1
+//   D2: lane k (k < N1) holds x[k + N1 * i], i < N2
+// The inverse (sign +1) transform takes D1 to D2, the forward (sign -1)
+// transform takes D2 to D1:
+//   inverse: a[i] = x[j + N2 i]; A = DFT_N1(a); A[k] *= w^(j k)   (lane j)
+//            exchange through the group's shared scratch
+//            b[i] = A_i[k];       X[k + N1 i] = DFT_N2(b)           (lane k)
+//   forward: the mirror image (DFT_N2 first, twiddle w^(k q2), DFT_N1).
+// with w = exp(s 2 pi i / n) read from the per-line table tw[m] (forward
+// sign; conjugated for the inverse).  Small DFTs of length 2..16 run fully
+// unrolled in registers; composite lengths use the same Cooley-Tukey split
+// with their twiddles from __constant__ tables (filled on the host from
+// long-double evaluations, see init_small_dft_twiddles).
+#pragma once
+
+#include "qeb_common.cuh"
+
+namespace qeb {
+
+// Offsets of the composite small-DFT tables: exp(-2 pi i m / N), m < N.
+template <int N> struct SmallTw;
+template <> struct SmallTw<6> { static constexpr int off = 0; };
+template <> struct SmallTw<8> { static constexpr int off = 6; };
+template <> struct SmallTw<9> { static constexpr int off = 14; };
+template <> struct SmallTw<10> { static constexpr int off = 23; };
+template <> struct SmallTw<12> { static constexpr int off = 33; };
+template <> struct SmallTw<15> { static constexpr int off = 45; };
+template <> struct SmallTw<16> { static constexpr int off = 60; };
+constexpr int kSmallTwTotal = 76;
+
+// Defined here (one translation unit includes this header; the library is
+// built without relocatable device code, so each module owns its tables).
+__constant__ double2 c_small_tw64[kSmallTwTotal];
+__constant__ float2 c_small_tw32[kSmallTwTotal];
+
+template <int N> struct Split { static constexpr int A = 1, B = N; };
+template <> struct Split<6> { static constexpr int A = 2, B = 3; };
+template <> struct Split<8> { static constexpr int A = 2, B = 4; };
+template <> struct Split<9> { static constexpr int A = 3, B = 3; };
+template <> struct Split<10> { static constexpr int A = 2, B = 5; };
+template <> struct Split<12> { static constexpr int A = 3, B = 4; };
+template <> struct Split<15> { static constexpr int A = 3, B = 5; };
+template <> struct Split<16> { static constexpr int A = 4, B = 4; };
+
+template <typename T, int N, bool BWD>
+__device__ __forceinline__ C2<T> small_tw(int m) {
+  if constexpr (sizeof(T) == 8) {
+    const double2 w = c_small_tw64[SmallTw<N>::off + m];
+    return mk<T>(w.x, BWD ? -w.y : w.y);
+  } else {
+    const float2 w = c_small_tw32[SmallTw<N>::off + m];
+    return mk<T>(w.x, BWD ? -w.y : w.y);
+  }
+}
+
+// In-register DFT of compile-time length N (sign +1 if BWD else -1).
+template <typename T, int N, bool BWD>
+__device__ __forceinline__ void dft(C2<T>* v) {
+  constexpr T sgn = BWD ? T(1) : T(-1);
+  if constexpr (N == 1) {
+    return;
+  } else if constexpr (N == 2 || N == 3 || N == 4 || N == 5) {
+    dft_small(v, N, sgn);
+  } else {
+    constexpr int A = Split<N>::A, B = Split<N>::B;
+    C2<T> y[B][A];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) {
+      C2<T> u[A];
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) u[n1] = v[B * n1 + n2];
+      dft<T, A, BWD>(u);
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1)
+        y[n2][k1] = (n2 * k1 == 0) ? u[k1] : cmul(u[k1], small_tw<T, N, BWD>(n2 * k1));
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+      C2<T> w[B];
+#pragma unroll
+      for (int n2 = 0; n2 < B; ++n2) w[n2] = y[n2][k1];
+      dft<T, B, BWD>(w);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) v[k1 + A * k2] = w[k2];
+    }
+  }
+}
+
+// Line-group geometry of a four-step transform n = N1 * N2.
+template <int N1_, int N2_>
+struct Four {
+  static constexpr int N1 = N1_, N2 = N2_, n = N1_ * N2_;
+  static constexpr int G = (N1_ > N2_) ? N1_ : N2_;
+  static constexpr int per_warp = 32 / G;
+  static constexpr int R = G;  // registers (complex) per lane
+  // exchange buffer of one group: N1 rows of N2 (+1 pad) values
+  static constexpr int xstride = N2_ + 1;
+  static constexpr int scratch = N1_ * xstride;
+};
+
+// Inverse transform, D1 -> D2.  `v` holds N1 values (D1) on lanes j < N2 and
+// returns N2 values (D2) on lanes k < N1.  `x` is the group's exchange
+// scratch (F::scratch values), `tw` the forward table of length n.
+template <typename T, class F>
+__device__ __forceinline__ void four_inverse(C2<T>* v, int lane, C2<T>* x, const C2<T>* tw,
+                                             unsigned mask) {
+  if (lane < F::N2) {
+    dft<T, F::N1, true>(v);
+#pragma unroll
+    for (int k = 1; k < F::N1; ++k) {
+      C2<T> w = tw[(lane * k) % F::n];
+      w.im = -w.im;
+      v[k] = cmul(v[k], w);
+    }
+#pragma unroll
+    for (int k = 0; k < F::N1; ++k) x[k * F::xstride + lane] = v[k];
+  }
+  __syncwarp(mask);
+  if (lane < F::N1) {
+#pragma unroll
+    for (int i = 0; i < F::N2; ++i) v[i] = x[lane * F::xstride + i];
+    dft<T, F::N2, true>(v);
+  }
+  __syncwarp(mask);
+}
+
+// Forward transform, D2 -> D1.  `v` holds N2 values (D2) on lanes k < N1 and
+// returns N1 values (D1) on lanes j < N2.
+template <typename T, class F>
+__device__ __forceinline__ void four_forward(C2<T>* v, int lane, C2<T>* x, const C2<T>* tw,
+                                             unsigned mask) {
+  if (lane < F::N1) {
+    dft<T, F::N2, false>(v);
+#pragma unroll
+    for (int q = 1; q < F::N2; ++q) v[q] = cmul(v[q], tw[(lane * q) % F::n]);
+#pragma unroll
+    for (int q = 0; q < F::N2; ++q) x[lane * F::xstride + q] = v[q];
+  }
+  __syncwarp(mask);
+  if (lane < F::N2) {
+#pragma unroll
+    for (int k = 0; k < F::N1; ++k) v[k] = x[k * F::xstride + lane];
+    dft<T, F::N1, false>(v);
+  }
+  __syncwarp(mask);
+}
+
+// Host: upload the composite small-DFT twiddles to the current device.
+int init_small_dft_twiddles();
+
+}  // namespace qeb

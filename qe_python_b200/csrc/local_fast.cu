@@ -1,0 +1,486 @@
+// Four-step register FFT versions of the local H|psi> passes (sm_100a).
+//
+// Same operator and HBM layout as the generic kernels of local_hpsi.cu
+// (qepy_pw/_native_fft.pyx qepy_apply_serial_spatial :58-135), with every
+// line transform done by one warp-resident line group (fft4.cuh): the index
+// arithmetic is compile time, each line needs one shared-memory exchange and
+// only warp-level synchronisation, and block-wide barriers separate the
+// stages (scatter, row transforms, column transforms, gather).
+//   pass A : z transforms of the occupied sticks          (grid: sticks/32 x bands)
+//   pass B : per (z, band) plane: inverse x transforms of the active rows,
+//            per column inverse y transform . V . forward y transform (in
+//            registers), forward x transforms, gather the sticks
+//   pass C : forward z transforms, gather, 1/N and the kinetic term
+// Used when the line length has a listed factorisation n = N1 * N2 (pass B:
+// nx == ny); other grids take the generic Stockham kernels.
+#include <mutex>
+
+#include "fft4.cuh"
+#include "local_plan.cuh"
+#include "../../include/qe_b200.h"
+
+using qeb::C2;
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kSticksPerBlock = 32;
+
+// n, N1, N2 of every four-step variant (index = position in this list).
+#define QEB_FOUR_SIZES(X) \
+  X(16, 4, 4)             \
+  X(24, 4, 6)             \
+  X(32, 4, 8)             \
+  X(36, 6, 6)             \
+  X(48, 6, 8)             \
+  X(64, 8, 8)             \
+  X(72, 8, 9)             \
+  X(90, 9, 10)            \
+  X(96, 8, 12)            \
+  X(108, 9, 12)           \
+  X(128, 8, 16)           \
+  X(135, 9, 15)           \
+  X(144, 12, 12)          \
+  X(180, 12, 15)
+
+constexpr int kFourLengths[] = {
+#define QEB_LEN(n, a, b) n,
+    QEB_FOUR_SIZES(QEB_LEN)
+#undef QEB_LEN
+};
+constexpr int kFourCount = sizeof(kFourLengths) / sizeof(int);
+
+template <class F>
+struct GroupIds {
+  int lig, gid, ngroups;
+  unsigned mask;
+  bool valid;
+  __device__ GroupIds() {
+    const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+    const int gw = lane / F::G;
+    lig = lane - gw * F::G;
+    valid = gw < F::per_warp;
+    gid = warp * F::per_warp + gw;
+    ngroups = kWarps * F::per_warp;
+    mask = (F::G == 32 ? 0xffffffffu : ((1u << F::G) - 1u)) << (gw * F::G);
+  }
+};
+
+template <typename T, class F>
+constexpr size_t ac_smem(int nz_pad) {
+  return sizeof(C2<T>) * ((size_t)kSticksPerBlock * nz_pad + F::n +
+                          (size_t)kWarps * F::per_warp * F::scratch);
+}
+
+template <typename T, class F>
+size_t b_smem(const qeb_local_plan* p) {
+  return sizeof(C2<T>) * ((size_t)p->nay * p->nx_pad + F::n +
+                          (size_t)kWarps * F::per_warp * F::scratch) +
+         sizeof(int) * F::n;
+}
+
+// ---------------------------------------------------------------------------
+template <typename T, class F>
+__global__ void __launch_bounds__(kThreads) four_pass_a(
+    const C2<T>* __restrict__ psi, int64_t ld, int nst, int nz_pad,
+    const int32_t* __restrict__ entry_g, const int32_t* __restrict__ entry_z,
+    const int32_t* __restrict__ entry_stick, const int32_t* __restrict__ stick_off,
+    const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks) {
+  constexpr int nz = F::n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2<T>* lines = reinterpret_cast<C2<T>*>(smem_raw);
+  C2<T>* tw = lines + kSticksPerBlock * nz_pad;
+  C2<T>* xbuf = tw + nz;
+  const int s0 = blockIdx.x * kSticksPerBlock;
+  const int nsl = min(kSticksPerBlock, nst - s0);
+  const int64_t band = blockIdx.y;
+  for (int i = threadIdx.x; i < nz; i += kThreads) tw[i] = tw_z[i];
+  for (int i = threadIdx.x; i < kSticksPerBlock * nz_pad; i += kThreads) lines[i] = qeb::mk<T>(0, 0);
+  __syncthreads();
+  const int e0 = stick_off[s0], e1 = stick_off[s0 + nsl];
+  const C2<T>* col = psi + band * ld;
+  for (int e = e0 + threadIdx.x; e < e1; e += kThreads)
+    lines[(entry_stick[e] - s0) * nz_pad + entry_z[e]] = col[entry_g[e]];
+  __syncthreads();
+  const GroupIds<F> g;
+  if (g.valid) {
+    C2<T>* x = xbuf + g.gid * F::scratch;
+    for (int s = g.gid; s < nsl; s += g.ngroups) {
+      C2<T>* line = lines + s * nz_pad;
+      C2<T> v[F::R];
+      if (g.lig < F::N2) {
+#pragma unroll
+        for (int i = 0; i < F::N1; ++i) v[i] = line[g.lig + F::N2 * i];
+      }
+      qeb::four_inverse<T, F>(v, g.lig, x, tw, g.mask);
+      if (g.lig < F::N1) {
+#pragma unroll
+        for (int p = 0; p < F::N2; ++p) line[g.lig + F::N1 * p] = v[p];
+      }
+      __syncwarp(g.mask);
+    }
+  }
+  __syncthreads();
+  C2<T>* out = sticks + band * (int64_t)nz * nst;
+  for (int i = threadIdx.x; i < nz * nsl; i += kThreads) {
+    const int z = i / nsl, sl = i - z * nsl;
+    out[(int64_t)z * nst + s0 + sl] = lines[sl * nz_pad + z];
+  }
+}
+
+template <typename T, class F>
+__global__ void __launch_bounds__(kThreads) four_pass_c(
+    const C2<T>* __restrict__ sticks, int nst, int nz_pad, const int32_t* __restrict__ entry_g,
+    const int32_t* __restrict__ entry_z, const int32_t* __restrict__ entry_stick,
+    const int32_t* __restrict__ stick_off, const C2<T>* __restrict__ tw_z,
+    const C2<T>* __restrict__ psi, int64_t ld, const T* __restrict__ kinetic, T inv_n,
+    C2<T>* __restrict__ out, int64_t ldo) {
+  constexpr int nz = F::n;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2<T>* lines = reinterpret_cast<C2<T>*>(smem_raw);
+  C2<T>* tw = lines + kSticksPerBlock * nz_pad;
+  C2<T>* xbuf = tw + nz;
+  const int s0 = blockIdx.x * kSticksPerBlock;
+  const int nsl = min(kSticksPerBlock, nst - s0);
+  const int64_t band = blockIdx.y;
+  for (int i = threadIdx.x; i < nz; i += kThreads) tw[i] = tw_z[i];
+  const C2<T>* in = sticks + band * (int64_t)nz * nst;
+  for (int i = threadIdx.x; i < nz * nsl; i += kThreads) {
+    const int z = i / nsl, sl = i - z * nsl;
+    lines[sl * nz_pad + z] = in[(int64_t)z * nst + s0 + sl];
+  }
+  __syncthreads();
+  const GroupIds<F> g;
+  if (g.valid) {
+    C2<T>* x = xbuf + g.gid * F::scratch;
+    for (int s = g.gid; s < nsl; s += g.ngroups) {
+      C2<T>* line = lines + s * nz_pad;
+      C2<T> v[F::R];
+      if (g.lig < F::N1) {
+#pragma unroll
+        for (int p = 0; p < F::N2; ++p) v[p] = line[g.lig + F::N1 * p];
+      }
+      qeb::four_forward<T, F>(v, g.lig, x, tw, g.mask);
+      if (g.lig < F::N2) {
+#pragma unroll
+        for (int i = 0; i < F::N1; ++i) line[g.lig + F::N2 * i] = v[i];
+      }
+      __syncwarp(g.mask);
+    }
+  }
+  __syncthreads();
+  const int e0 = stick_off[s0], e1 = stick_off[s0 + nsl];
+  const C2<T>* colp = psi + band * ld;
+  C2<T>* dst = out + band * ldo;
+  for (int e = e0 + threadIdx.x; e < e1; e += kThreads) {
+    const int gidx = entry_g[e];
+    C2<T> v = qeb::scale(lines[(entry_stick[e] - s0) * nz_pad + entry_z[e]], inv_n);
+    if (kinetic != nullptr) {
+      const T t = kinetic[gidx];
+      const C2<T> pv = colp[gidx];
+      v.re += t * pv.re;
+      v.im += t * pv.im;
+    }
+    dst[gidx] = v;
+  }
+}
+
+// MODE 0: local potential; MODE 1: density accumulation.
+template <typename T, class F, int MODE>
+__global__ void __launch_bounds__(kThreads) four_pass_b(
+    C2<T>* __restrict__ sticks, int nst, int nz, int nay, int nx_pad,
+    const int32_t* __restrict__ stick_pos, const int32_t* __restrict__ y_to_ay,
+    const C2<T>* __restrict__ tw_xy, const T* __restrict__ potential,
+    const double* __restrict__ weights, double* __restrict__ density) {
+  constexpr int n = F::n;  // nx == ny
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2<T>* plane = reinterpret_cast<C2<T>*>(smem_raw);  // [nay][nx_pad]
+  C2<T>* tw = plane + (size_t)nay * nx_pad;
+  C2<T>* xbuf = tw + n;
+  int* yay = reinterpret_cast<int*>(xbuf + kWarps * F::per_warp * F::scratch);
+  const int z = blockIdx.x;
+  const int64_t band = blockIdx.y;
+  for (int i = threadIdx.x; i < n; i += kThreads) {
+    tw[i] = tw_xy[i];
+    yay[i] = y_to_ay[i];
+  }
+  for (int i = threadIdx.x; i < nay * nx_pad; i += kThreads) plane[i] = qeb::mk<T>(0, 0);
+  __syncthreads();
+  C2<T>* srow = sticks + (band * nz + z) * (int64_t)nst;
+  for (int s = threadIdx.x; s < nst; s += kThreads) plane[stick_pos[s]] = srow[s];
+  __syncthreads();
+  const GroupIds<F> g;
+  C2<T>* x = xbuf + g.gid * F::scratch;
+  // inverse transforms along x of the active rows (D1 in, D2 out, in place)
+  if (g.valid) {
+    for (int r = g.gid; r < nay; r += g.ngroups) {
+      C2<T>* row = plane + r * nx_pad;
+      C2<T> v[F::R];
+      if (g.lig < F::N2) {
+#pragma unroll
+        for (int i = 0; i < F::N1; ++i) v[i] = row[g.lig + F::N2 * i];
+      }
+      qeb::four_inverse<T, F>(v, g.lig, x, tw, g.mask);
+      if (g.lig < F::N1) {
+#pragma unroll
+        for (int p = 0; p < F::N2; ++p) row[g.lig + F::N1 * p] = v[p];
+      }
+      __syncwarp(g.mask);
+    }
+  }
+  __syncthreads();
+  // columns: inverse y transform, V (or |psi|^2), forward y transform
+  double w = 0.0;
+  if (MODE == 1) w = weights[band];
+  if (g.valid) {
+    for (int col = g.gid; col < n; col += g.ngroups) {
+      C2<T> v[F::R];
+      if (g.lig < F::N2) {
+#pragma unroll
+        for (int i = 0; i < F::N1; ++i) {
+          const int ay = yay[g.lig + F::N2 * i];
+          v[i] = (ay >= 0) ? plane[ay * nx_pad + col] : qeb::mk<T>(0, 0);
+        }
+      }
+      qeb::four_inverse<T, F>(v, g.lig, x, tw, g.mask);
+      if (MODE == 0) {
+        if (g.lig < F::N1) {
+          const T* vcol = potential + ((int64_t)z * n + col) * n;
+#pragma unroll
+          for (int p = 0; p < F::N2; ++p) v[p] = qeb::scale(v[p], __ldg(vcol + g.lig + F::N1 * p));
+        }
+        qeb::four_forward<T, F>(v, g.lig, x, tw, g.mask);
+        if (g.lig < F::N2) {
+#pragma unroll
+          for (int i = 0; i < F::N1; ++i) {
+            const int ay = yay[g.lig + F::N2 * i];
+            if (ay >= 0) plane[ay * nx_pad + col] = v[i];
+          }
+        }
+      } else {
+        if (g.lig < F::N1) {
+#pragma unroll
+          for (int p = 0; p < F::N2; ++p) {
+            const int y = g.lig + F::N1 * p;
+            const double m = (double)v[p].re * v[p].re + (double)v[p].im * v[p].im;
+            atomicAdd(density + ((int64_t)col * n + y) * nz + z, w * m);
+          }
+        }
+      }
+      __syncwarp(g.mask);
+    }
+  }
+  if (MODE == 1) return;
+  __syncthreads();
+  // forward transforms along x of the active rows (D2 in, D1 out, in place)
+  if (g.valid) {
+    for (int r = g.gid; r < nay; r += g.ngroups) {
+      C2<T>* row = plane + r * nx_pad;
+      C2<T> v[F::R];
+      if (g.lig < F::N1) {
+#pragma unroll
+        for (int p = 0; p < F::N2; ++p) v[p] = row[g.lig + F::N1 * p];
+      }
+      qeb::four_forward<T, F>(v, g.lig, x, tw, g.mask);
+      if (g.lig < F::N2) {
+#pragma unroll
+        for (int i = 0; i < F::N1; ++i) row[g.lig + F::N2 * i] = v[i];
+      }
+      __syncwarp(g.mask);
+    }
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < nst; s += kThreads) srow[s] = plane[stick_pos[s]];
+}
+
+template <typename T>
+const C2<T>* tw_at(const qeb_local_plan* p, int which) {
+  const C2<T>* base = static_cast<const C2<T>*>(p->tw);
+  return which == 0 ? base : (which == 1 ? base + p->nx : base + p->nx + p->ny);
+}
+
+// Calls `fn.template operator()<F>()` with the four-step type of variant v.
+template <class Fn>
+int with_variant(int v, Fn&& fn) {
+  int index = 0;
+#define QEB_CASE(n, a, b)                                    \
+  if (v == index) return fn.template operator()<qeb::Four<a, b>>(); \
+  ++index;
+  QEB_FOUR_SIZES(QEB_CASE)
+#undef QEB_CASE
+  qeb::set_error("four-step variant %d does not exist", v);
+  return QEB_EUNSUPPORTED;
+}
+
+template <typename T>
+struct SetLimits {
+  const qeb_local_plan* p;
+  template <class F>
+  int operator()() const {
+    cudaError_t err = cudaSuccess;
+    if (p->fast_z >= 0 && F::n == p->nz) {
+      const int s = (int)ac_smem<T, F>(p->nz_pad);
+      err = cudaFuncSetAttribute(four_pass_a<T, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+      if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(four_pass_c<T, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+    }
+    if (err == cudaSuccess && p->fast_xy >= 0 && F::n == p->nx) {
+      const size_t s = b_smem<T, F>(p);
+      if (s > 227 * 1024) {
+        qeb::set_error("four-step pass B needs %zu bytes of shared memory", s);
+        return QEB_EUNSUPPORTED;
+      }
+      err = cudaFuncSetAttribute(four_pass_b<T, F, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s);
+      if (err == cudaSuccess)
+        err = cudaFuncSetAttribute(four_pass_b<T, F, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s);
+    }
+    return qeb::cuda_status(err, "four-step shared memory attribute");
+  }
+};
+
+template <typename T>
+struct PassA {
+  const qeb_local_plan* p; C2<T>* sticks; const C2<T>* psi; int64_t ld; int64_t nb; cudaStream_t s;
+  template <class F>
+  int operator()() const {
+    const dim3 grid((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
+    four_pass_a<T, F><<<grid, kThreads, ac_smem<T, F>(p->nz_pad), s>>>(
+        psi, ld, p->nst, p->nz_pad, p->entry_g, p->entry_z, p->entry_stick, p->stick_off,
+        tw_at<T>(p, 2), sticks);
+    return QEB_OK;
+  }
+};
+
+template <typename T>
+struct PassC {
+  const qeb_local_plan* p; const C2<T>* sticks; const C2<T>* psi; int64_t ld; int64_t nb;
+  const T* kinetic; C2<T>* out; int64_t ldo; cudaStream_t s;
+  template <class F>
+  int operator()() const {
+    const dim3 grid((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
+    const T inv_n = T(1.0 / ((double)p->nx * p->ny * p->nz));
+    four_pass_c<T, F><<<grid, kThreads, ac_smem<T, F>(p->nz_pad), s>>>(
+        sticks, p->nst, p->nz_pad, p->entry_g, p->entry_z, p->entry_stick, p->stick_off,
+        tw_at<T>(p, 2), psi, ld, kinetic, inv_n, out, ldo);
+    return QEB_OK;
+  }
+};
+
+template <typename T, int MODE>
+struct PassB {
+  const qeb_local_plan* p; C2<T>* sticks; int64_t nb; const T* potential;
+  const double* weights; double* density; cudaStream_t s;
+  template <class F>
+  int operator()() const {
+    const dim3 grid(p->nz, (unsigned)nb);
+    four_pass_b<T, F, MODE><<<grid, kThreads, b_smem<T, F>(p), s>>>(
+        sticks, p->nst, p->nz, p->nay, p->nx_pad, p->stick_pos, p->y_to_ay, tw_at<T>(p, 0),
+        potential, weights, density);
+    return QEB_OK;
+  }
+};
+
+template <typename T>
+int apply_t(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64_t ld, int64_t nb,
+            const T* potential, const T* kinetic, C2<T>* out, int64_t ldo, cudaStream_t s,
+            cudaEvent_t* ev) {
+  int rc;
+  if (ev) cudaEventRecord(ev[0], s);
+  if ((rc = with_variant(p->fast_z, PassA<T>{p, sticks, psi, ld, nb, s}))) return rc;
+  if (ev) cudaEventRecord(ev[1], s);
+  if ((rc = with_variant(p->fast_xy, PassB<T, 0>{p, sticks, nb, potential, nullptr, nullptr, s})))
+    return rc;
+  if (ev) cudaEventRecord(ev[2], s);
+  if ((rc = with_variant(p->fast_z, PassC<T>{p, sticks, psi, ld, nb, kinetic, out, ldo, s})))
+    return rc;
+  if (ev) cudaEventRecord(ev[3], s);
+  qeb::count_launches(3);
+  return qeb::cuda_status(cudaGetLastError(), "four-step apply_local launch");
+}
+
+template <typename T>
+int density_t(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64_t ld, int64_t nb,
+              const double* weights, double* density, cudaStream_t s) {
+  int rc;
+  if ((rc = with_variant(p->fast_z, PassA<T>{p, sticks, psi, ld, nb, s}))) return rc;
+  if ((rc = with_variant(p->fast_xy, PassB<T, 1>{p, sticks, nb, nullptr, weights, density, s})))
+    return rc;
+  qeb::count_launches(2);
+  return qeb::cuda_status(cudaGetLastError(), "four-step accumulate_density launch");
+}
+
+std::mutex g_tw_mutex;
+bool g_tw_ready[64] = {false};
+
+}  // namespace
+
+namespace qeb {
+
+int four_variant(int n) {
+  for (int i = 0; i < kFourCount; ++i)
+    if (kFourLengths[i] == n) return i;
+  return -1;
+}
+
+int init_small_dft_twiddles() {
+  int device = 0;
+  cudaGetDevice(&device);
+  if (device < 0 || device >= 64) return QEB_EUNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_tw_mutex);
+  if (g_tw_ready[device]) return QEB_OK;
+  double2 t64[kSmallTwTotal];
+  float2 t32[kSmallTwTotal];
+  const int sizes[] = {6, 8, 9, 10, 12, 15, 16};
+  const long double two_pi = 6.283185307179586476925286766559005768L;
+  int off = 0;
+  for (int n : sizes) {
+    for (int m = 0; m < n; ++m) {
+      const long double a = two_pi * (long double)m / (long double)n;
+      t64[off + m] = make_double2((double)cosl(a), (double)(-sinl(a)));
+      t32[off + m] = make_float2((float)cosl(a), (float)(-sinl(a)));
+    }
+    off += n;
+  }
+  cudaError_t err = cudaMemcpyToSymbol(c_small_tw64, t64, sizeof(t64));
+  if (err == cudaSuccess) err = cudaMemcpyToSymbol(c_small_tw32, t32, sizeof(t32));
+  if (err != cudaSuccess) return cuda_status(err, "small DFT twiddle upload");
+  g_tw_ready[device] = true;
+  return QEB_OK;
+}
+
+int fast_smem_limits(const qeb_local_plan* p) {
+  int rc = init_small_dft_twiddles();
+  if (rc) return rc;
+  for (int v : {p->fast_z, p->fast_xy}) {
+    if (v < 0) continue;
+    rc = (p->precision == QEB_F64) ? with_variant(v, SetLimits<double>{p})
+                                   : with_variant(v, SetLimits<float>{p});
+    if (rc) return rc;
+  }
+  return QEB_OK;
+}
+
+int fast_apply(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
+               const void* potential, const void* kinetic, void* out, int64_t ldo,
+               cudaStream_t stream, cudaEvent_t* events) {
+  if (p->precision == QEB_F64)
+    return apply_t<double>(p, static_cast<C2<double>*>(sticks), static_cast<const C2<double>*>(psi),
+                           ld, nb, static_cast<const double*>(potential),
+                           static_cast<const double*>(kinetic), static_cast<C2<double>*>(out), ldo,
+                           stream, events);
+  return apply_t<float>(p, static_cast<C2<float>*>(sticks), static_cast<const C2<float>*>(psi), ld,
+                        nb, static_cast<const float*>(potential), static_cast<const float*>(kinetic),
+                        static_cast<C2<float>*>(out), ldo, stream, events);
+}
+
+int fast_density(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
+                 const double* weights, double* density, cudaStream_t stream) {
+  if (p->precision == QEB_F64)
+    return density_t<double>(p, static_cast<C2<double>*>(sticks),
+                             static_cast<const C2<double>*>(psi), ld, nb, weights, density, stream);
+  return density_t<float>(p, static_cast<C2<float>*>(sticks), static_cast<const C2<float>*>(psi),
+                          ld, nb, weights, density, stream);
+}
+
+}  // namespace qeb

@@ -20,37 +20,17 @@
 //   density  : C-order (nx, ny, nz) float64 (reference serial layout)
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <vector>
 
+#include "local_plan.cuh"
 #include "qeb_common.cuh"
 #include "../../include/qe_b200.h"
 
 using qeb::C2;
 using qeb::FftDesc;
-
-struct qeb_local_plan {
-  int nx, ny, nz;
-  int64_t npw;
-  int nst;       // occupied (x, y) sticks
-  int nay;       // active y rows
-  int nx_pad;    // shared-memory row stride of the active-row plane
-  int ny_pad;    // shared-memory stride of the column lines
-  int nz_pad;    // shared-memory stride of the stick lines
-  int precision; // QEB_F64 or QEB_F32
-  int device;
-  FftDesc fx, fy, fz;
-  // device arrays (plan-owned)
-  int32_t* entry_g;      // npw: plane-wave row, CSR-ordered by (stick, z)
-  int32_t* entry_z;      // npw: z slot
-  int32_t* entry_stick;  // npw: stick index
-  int32_t* stick_off;    // nst + 1
-  int32_t* stick_pos;    // nst: ay * nx_pad + x (shared-memory plane position)
-  int32_t* ay_to_y;      // nay
-  int32_t* y_to_ay;      // ny (-1 when the row holds no stick)
-  void* tw;              // forward twiddles: nx, then ny, then nz entries (complex T)
-};
 
 namespace {
 
@@ -241,6 +221,8 @@ int launch_apply(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64
     qeb::set_error("apply_local: at most 65535 bands per call (got %lld)", (long long)nb);
     return QEB_EINVAL;
   }
+  if (p->fast_xy >= 0 && p->fast_z >= 0)
+    return qeb::fast_apply(p, sticks, psi, ld, nb, potential, kinetic, out, ldo, stream, events);
   const dim3 grid_ac((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
   const dim3 grid_b(p->nz, (unsigned)nb);
   if (events) cudaEventRecord(events[0], stream);
@@ -270,6 +252,8 @@ int launch_density(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int
     qeb::set_error("accumulate_density: at most 65535 bands per call (got %lld)", (long long)nb);
     return QEB_EINVAL;
   }
+  if (p->fast_xy >= 0 && p->fast_z >= 0)
+    return qeb::fast_density(p, sticks, psi, ld, nb, weights, density, stream);
   const dim3 grid_ac((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
   const dim3 grid_b(p->nz, (unsigned)nb);
   pass_a_kernel<T><<<grid_ac, kThreads, pass_ac_smem<T>(p), stream>>>(
@@ -422,6 +406,15 @@ extern "C" int qeb_local_plan_create(qeb_local_plan** out, int nx, int ny, int n
   p->nx_pad = odd_pad(nx);
   p->ny_pad = odd_pad(ny);
   p->nz_pad = odd_pad(nz);
+  // Four-step kernels when both the plane (nx == ny) and the z lines have a
+  // listed factorisation; QEB_FORCE_GENERIC=1 selects the Stockham kernels.
+  const char* force_generic = std::getenv("QEB_FORCE_GENERIC");
+  p->fast_xy = (nx == ny) ? qeb::four_variant(nx) : -1;
+  p->fast_z = qeb::four_variant(nz);
+  if (p->fast_xy < 0 || p->fast_z < 0 || (force_generic && force_generic[0] == '1')) {
+    p->fast_xy = -1;
+    p->fast_z = -1;
+  }
   std::vector<int32_t> stick_pos(nst);
   for (int s = 0; s < nst; ++s) {
     const int x = (int)(sticks[s] / ny), y = (int)(sticks[s] % ny);
@@ -455,6 +448,7 @@ extern "C" int qeb_local_plan_create(qeb_local_plan** out, int nx, int ny, int n
     rc = upload(reinterpret_cast<C2<float>**>(&p->tw), tw);
     if (rc == QEB_OK) rc = set_smem_limits<float>(p);
   }
+  if (rc == QEB_OK && p->fast_xy >= 0) rc = qeb::fast_smem_limits(p);
   if (rc != QEB_OK) {
     free_plan(p);
     return rc;
@@ -510,8 +504,11 @@ static int check_call(const qeb_local_plan* p, const void* scratch, int64_t scra
                    (long long)scratch_bytes, (long long)qeb_local_scratch_bytes(p, nb));
     return QEB_ESCRATCH;
   }
-  if ((reinterpret_cast<uintptr_t>(scratch) | reinterpret_cast<uintptr_t>(psi)) % 16 != 0) {
-    qeb::set_error("%s: operands must be 16-byte aligned", who);
+  // complex values are accessed as one 8-byte (complex64) or 16-byte
+  // (complex128) word, so operands must be aligned to their element size
+  const uintptr_t align = (p->precision == QEB_F64) ? 16 : 8;
+  if ((reinterpret_cast<uintptr_t>(scratch) | reinterpret_cast<uintptr_t>(psi)) % align != 0) {
+    qeb::set_error("%s: operands must be %d-byte aligned", who, (int)align);
     return QEB_EINVAL;
   }
   return QEB_OK;

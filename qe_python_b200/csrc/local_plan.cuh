@@ -1,0 +1,49 @@
+// Plan object of the local H|psi> operator, shared by the generic
+// (local_hpsi.cu) and the register four-step (local_fast.cu) kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+#include "qeb_common.cuh"
+
+struct qeb_local_plan {
+  int nx, ny, nz;
+  int64_t npw;
+  int nst;       // occupied (x, y) sticks
+  int nay;       // active y rows
+  int nx_pad;    // shared-memory row stride of the active-row plane
+  int ny_pad;    // shared-memory stride of the column lines
+  int nz_pad;    // shared-memory stride of the stick lines
+  int precision; // QEB_F64 or QEB_F32
+  int device;
+  qeb::FftDesc fx, fy, fz;
+  int fast_xy;   // four-step variant of nx (== ny), or -1: generic pass B
+  int fast_z;    // four-step variant of nz, or -1: generic passes A and C
+  // device arrays (plan-owned)
+  int32_t* entry_g;      // npw: plane-wave row, CSR-ordered by (stick, z)
+  int32_t* entry_z;      // npw: z slot
+  int32_t* entry_stick;  // npw: stick index
+  int32_t* stick_off;    // nst + 1
+  int32_t* stick_pos;    // nst: ay * nx_pad + x (shared-memory plane position)
+  int32_t* ay_to_y;      // nay
+  int32_t* y_to_ay;      // ny (-1 when the row holds no stick)
+  void* tw;              // forward twiddles: nx, then ny, then nz entries (complex T)
+};
+
+namespace qeb {
+
+// Four-step variant index of a line length (-1 when only the generic
+// Stockham engine handles it).
+int four_variant(int n);
+
+// Launchers of the four-step kernels (local_fast.cu).  Each returns QEB_OK
+// or an error status; events may be null.
+int fast_smem_limits(const qeb_local_plan* p);
+int fast_apply(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
+               const void* potential, const void* kinetic, void* out, int64_t ldo,
+               cudaStream_t stream, cudaEvent_t* events);
+int fast_density(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
+                 const double* weights, double* density, cudaStream_t stream);
+
+}  // namespace qeb

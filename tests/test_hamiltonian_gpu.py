@@ -100,7 +100,9 @@ def _system(seed=3, nproj_atoms=2, k=(0.125, 0.125, 0.375), ecut=20.0):
         vg[idx] += rng.uniform(-0.3, 0.3)
     vr = np.real(np.fft.ifftn(vg) * np.prod(shape))
     vr = 0.5 * (vr + vr)  # real part of a non-Hermitian vg is a valid real potential
-    species = (rng.standard_normal((npw, 4)) + 1j * rng.standard_normal((npw, 4))) * np.exp(-basis.kinetic / 4)[:, None]
+    # amplitude 0.05 keeps the nonlocal eigenvalues O(1) Ha, like real projectors
+    species = (rng.standard_normal((npw, 4)) + 1j * rng.standard_normal((npw, 4))) \
+        * 0.05 * np.exp(-basis.kinetic / 4)[:, None]
     positions = rng.uniform(0, 5, (nproj_atoms, 3))
     phases = np.exp(-1j * basis.vectors @ positions.T)
     d = rng.uniform(-1, 1, (4, 4))
@@ -163,12 +165,63 @@ def test_davidson_matches_dense_eigenvalues(cuda_device, precision, tol):
     start = rng.standard_normal((len(basis), 8)) + 1j * rng.standard_normal((len(basis), 8))
     start *= (1.0 / (1.0 + basis.kinetic))[:, None]
     dtype = torch.complex128 if precision == "f64" else torch.complex64
+    # FP32 residual norms floor near 1e-6 |H|: the FP32 form converges on the
+    # eigenvalue change alone (residual_factor=None, as the SCF driver calls it)
     result = davidson(h.apply, h.diagonal, 8, initial_vectors=_f(start).to(dtype),
-                      tolerance=1e-11 if precision == "f64" else 1e-7, max_iterations=200,
-                      subspace_multiplier=4, operator_into=h.apply_into)
+                      tolerance=1e-11 if precision == "f64" else 1e-6, max_iterations=200,
+                      subspace_multiplier=4, operator_into=h.apply_into,
+                      residual_factor=10.0 if precision == "f64" else None)
     assert result.converged
     np.testing.assert_allclose(result.eigenvalues, exact, atol=tol)
     # Ritz vectors are H-eigenvectors: ||H x - e x|| small
     hx = h.apply(result.eigenvectors)
     res = (hx - result.eigenvectors * torch.as_tensor(result.eigenvalues, device="cuda").to(hx.real.dtype)[None, :]).abs().max()
     assert float(res) < (1e-6 if precision == "f64" else 5e-3)
+
+
+def test_hamiltonian_matches_reference_golden(cuda_device):
+    """Reference PlaneWaveHamiltonian.apply (factorized + packed + materialised
+    terms; tests/golden/hamiltonian_small.npz) against the GPU operator."""
+    from pathlib import Path
+
+    g = np.load(Path(__file__).resolve().parent / "golden" / "hamiltonian_small.npz")
+    shape = tuple(int(v) for v in g["shape"])
+    from qe_python_b200.basis import PlaneWaveBasis
+
+    basis = PlaneWaveBasis(g["miller"], np.zeros((len(g["miller"]), 3)), g["kinetic"])
+    ws = LocalPotentialWorkspace(basis, shape)
+    terms = (FactorizedProjectorTerm(g["species"], g["phases"], g["coupling"]),
+             PackedProjectorTerm(g["packed_beta"], g["packed_coupling"], g["packed_diag"]),
+             (g["mat_beta"], g["mat_coupling"]))
+    h = PlaneWaveHamiltonian(basis, None, terms, local_workspace=ws, real_potential=g["potential"],
+                             potential_average=0.125)
+    got = h.apply(_f(g["psi"])).cpu().numpy()
+    assert np.max(np.abs(got - g["hpsi"])) <= 1e-12 * np.max(np.abs(g["hpsi"]))
+    np.testing.assert_allclose(h.diagonal.cpu().numpy(), g["diagonal"], rtol=1e-12, atol=1e-13)
+
+
+def test_davidson_matches_reference_golden(cuda_device):
+    """Same operator, start vectors and settings as the reference davidson run
+    of tests/golden/davidson_small.npz (tolerance 1e-9 Ha, ndim 2)."""
+    from pathlib import Path
+
+    here = Path(__file__).resolve().parent / "golden"
+    g = np.load(here / "hamiltonian_small.npz")
+    d = np.load(here / "davidson_small.npz")
+    shape = tuple(int(v) for v in g["shape"])
+    from qe_python_b200.basis import PlaneWaveBasis
+
+    basis = PlaneWaveBasis(g["miller"], np.zeros((len(g["miller"]), 3)), g["kinetic"])
+    ws = LocalPotentialWorkspace(basis, shape)
+    terms = (FactorizedProjectorTerm(g["species"], g["phases"], g["coupling"]),
+             PackedProjectorTerm(g["packed_beta"], g["packed_coupling"], g["packed_diag"]),
+             (g["mat_beta"], g["mat_coupling"]))
+    h = PlaneWaveHamiltonian(basis, None, terms, local_workspace=ws, real_potential=g["potential"],
+                             potential_average=0.125)
+    result = davidson(h.apply, h.diagonal, 8, initial_vectors=_f(d["start"]), tolerance=1e-9,
+                      max_iterations=100, subspace_multiplier=2, residual_factor=None,
+                      operator_into=h.apply_into)
+    assert result.converged == bool(d["converged"])
+    np.testing.assert_allclose(result.eigenvalues, d["eigenvalues"], atol=5e-9)
+    # the trajectory follows the reference's within a couple of iterations
+    assert abs(result.iterations - float(d["iterations"])) <= 2
