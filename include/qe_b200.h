@@ -132,6 +132,42 @@ int qeb_zgemm_static_scratch(int M, int N, int K, const double* alpha, const voi
                              void* C, int64_t ldc, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Split-TF32 complex GEMM on tcgen05 tensor cores (the chosen form of the
+ * projector and subspace contractions; replaces the same ZGEMM calls as
+ * qeb_zgemm, in FP32 precision).
+ *
+ * qeb_tf32_pack turns a complex matrix into two K-major FP32 planes
+ * hi = tf32(x), lo = tf32(x - hi), rows of kp = roundup(2K, 32) reals with
+ * each complex value as two consecutive reals, transformed by `layout`:
+ *   RAW [re, im], SWAPNEG [im, -re], NEGIM [re, -im], SWAP [im, re].
+ * transposed = 0: source column r (K contiguous values, leading dim ld) is
+ * packed row r; transposed = 1: source row r of a column-major rows x K
+ * matrix is packed row r.  precision: QEB_F64 or QEB_F32 source.
+ *
+ * qeb_tf32_gemm: C = alpha (A B0^T + i A B1^T) + beta C with A (M x kp) and
+ * B0, B1 (N x kp) packed operands (row strides lda, ldb floats), C complex64
+ * column-major.  Each real product is hi.hi + hi.lo + lo.hi on
+ * tcgen05.mma.kind::tf32 with FP32 accumulation in tensor memory.  With
+ * scratch of qeb_tf32_gemm_scratch_bytes() the K range is split over CTAs.
+ *   beta^H psi  : A = pack(beta, RAW), B0 = pack(psi, RAW), B1 = pack(psi, SWAPNEG)
+ *   beta coupled: A = pack(beta, RAW, transposed), B0 = pack(c, NEGIM), B1 = pack(c, SWAP)
+ * All waits inside the kernel are bounded; qeb_tf32_gemm_error() returns a
+ * non-zero code (and clears it) if any timed out.
+ * ---------------------------------------------------------------------- */
+#define QEB_PACK_RAW 0
+#define QEB_PACK_SWAPNEG 1
+#define QEB_PACK_NEGIM 2
+#define QEB_PACK_SWAP 3
+int qeb_tf32_pack(int precision, int layout, int transposed, int rows, int K, const void* src,
+                  int64_t ld, void* hi, void* lo, int64_t ldp, void* stream);
+int64_t qeb_tf32_gemm_scratch_bytes(int M, int N, int kp);
+int qeb_tf32_gemm(int M, int N, int kp, const void* a_hi, const void* a_lo, int64_t lda,
+                  const void* b0_hi, const void* b0_lo, const void* b1_hi, const void* b1_lo,
+                  int64_t ldb, const double* alpha, const double* beta, void* C, int64_t ldc,
+                  void* scratch, int64_t scratch_bytes, void* stream);
+int qeb_tf32_gemm_error(int* out);
+
+/* ------------------------------------------------------------------------
  * Davidson column kernels (precision QEB_F64 / QEB_F32 selects the vector
  * type; reductions accumulate in FP64; eigenvalues, diagonals and norms
  * are device float64 arrays).

@@ -123,6 +123,13 @@ class _DeviceProjectors:
             if dtype != torch.complex128:
                 self.beta = self.beta.T.contiguous().T
             self.coupling = to_device_f(coupling, dtype, device)
+        # Split-TF32 operands of the chosen form, packed once per Hamiltonian:
+        # beta^H (calbec) and beta (the H psi update, rows = plane waves).
+        self.packed_conj = None
+        self.packed_plain = None
+        if self.beta is not None and dtype == torch.complex64:
+            self.packed_conj = K.tf32_pack(self.beta, K.PACK_RAW)
+            self.packed_plain = K.tf32_pack(self.beta, K.PACK_RAW, transposed=True)
         # Preconditioner diagonal (diagonalization.py:205-229).
         for entry in diagonals:
             if entry[0] == "packed":
@@ -177,8 +184,29 @@ class PlaneWaveHamiltonian:
         self._kinetic_kernel = self._kinetic.to(REAL_OF[self.dtype])
         self._potential = local_workspace.native_potential(real_potential, self.native_potential_layout)
         self.projectors = _DeviceProjectors(projector_terms, len(basis), self.dtype, self.device)
+        # chosen form: projector GEMMs as split-TF32 tcgen05 products
+        self.tensor_gemm = self.dtype == torch.complex64
         self.projector_terms = tuple(projector_terms)
         self._diagonal_device = self._kinetic + self.potential_average + self.projectors.device_diagonal
+
+    # The three nonlocal stages (reference: diagonalization.py:280-368).
+    def calbec(self, vectors: torch.Tensor) -> torch.Tensor:
+        """becp = beta^H psi (projector_overlaps, _native_fft.pyx:694-731)."""
+        p = self.projectors
+        if p.packed_conj is not None and self.tensor_gemm:
+            return K.gemm_tf32(K.OP_C, p.beta, vectors, a_packed=p.packed_conj)
+        return K.gemm(K.OP_C, p.beta, vectors)
+
+    def couple(self, becp: torch.Tensor) -> torch.Tensor:
+        """coupled = D becp with the block-diagonal 0.5 D_Ry (diagonalization.py:348)."""
+        return K.gemm(K.OP_N, self.projectors.coupling, becp)
+
+    def add_projectors(self, coupled: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
+        """target += beta coupled (add_projector_product, _native_fft.pyx:782-836)."""
+        p = self.projectors
+        if p.packed_plain is not None and self.tensor_gemm:
+            return K.gemm_tf32(K.OP_N, p.beta, coupled, target, beta=1.0, a_packed=p.packed_plain)
+        return K.gemm(K.OP_N, p.beta, coupled, target, beta=1.0)
 
     @property
     def diagonal(self) -> torch.Tensor:
@@ -208,10 +236,9 @@ class PlaneWaveHamiltonian:
             self.local_workspace._launch_apply(self._potential, vectors, self._kinetic_kernel, target)
         if self.projectors.beta is not None and vectors.shape[1] > 0:
             with _timer(self.timers, "h_psi:calbec"):
-                becp = K.gemm(K.OP_C, self.projectors.beta, vectors)
+                becp = self.calbec(vectors)
             with _timer(self.timers, "add_vuspsi"):
-                coupled = K.gemm(K.OP_N, self.projectors.coupling, becp)
-                K.gemm(K.OP_N, self.projectors.beta, coupled, target, beta=1.0)
+                self.add_projectors(self.couple(becp), target)
         if host:
             result = as_numpy(target)
             if out is not None and not isinstance(out, torch.Tensor):

@@ -89,6 +89,97 @@ def gemm(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = N
     return c
 
 
+PACK_RAW, PACK_SWAPNEG, PACK_NEGIM, PACK_SWAP = 0, 1, 2, 3
+
+
+def tf32_width(k: int) -> int:
+    """Packed row length: 2K reals rounded up to the 32-wide K tile."""
+    return (2 * int(k) + 31) // 32 * 32
+
+
+class PackedOperand:
+    """K-major hi/lo FP32 planes of a complex operand (qeb_tf32_pack)."""
+
+    def __init__(self, rows: int, k: int, device) -> None:
+        self.rows, self.k, self.kp = int(rows), int(k), tf32_width(k)
+        self.hi = torch.empty((max(self.rows, 1), self.kp), dtype=torch.float32, device=device)
+        self.lo = torch.empty_like(self.hi)
+
+
+def tf32_pack(src: torch.Tensor, layout: int, transposed: bool = False,
+              out: PackedOperand | None = None) -> PackedOperand:
+    """Pack columns (or, transposed, rows) of a complex matrix for qeb_tf32_gemm."""
+    _check_matrix("src", src)
+    rows, k = (src.shape[0], src.shape[1]) if transposed else (src.shape[1], src.shape[0])
+    if out is None or out.rows != rows or out.k != k:
+        out = PackedOperand(rows, k, src.device)
+    _lib.check("qeb_tf32_pack", _lib.load().qeb_tf32_pack(
+        _precision(src), layout, int(transposed), rows, k, src.data_ptr(), leading_dimension(src),
+        out.hi.data_ptr(), out.lo.data_ptr(), out.kp, stream_handle()))
+    return out
+
+
+def tf32_gemm(a: PackedOperand, b0: PackedOperand, b1: PackedOperand, c: torch.Tensor,
+              alpha: complex = 1.0, beta: complex = 0.0) -> torch.Tensor:
+    """c = alpha (A B0^T + i A B1^T) + beta c on tcgen05 (split TF32)."""
+    _check_matrix("c", c)
+    if c.dtype != torch.complex64:
+        raise TypeError("the split-TF32 GEMM writes complex64")
+    if a.kp != b0.kp or b0.kp != b1.kp or b0.rows != b1.rows:
+        raise ValueError("packed operands disagree")
+    m, n = a.rows, b0.rows
+    if tuple(c.shape) != (m, n):
+        raise ValueError("c has the wrong shape")
+    if m == 0 or n == 0:
+        return c
+    lib = _lib.load()
+    al = (ctypes.c_double * 2)(complex(alpha).real, complex(alpha).imag)
+    be = (ctypes.c_double * 2)(complex(beta).real, complex(beta).imag)
+    need = int(lib.qeb_tf32_gemm_scratch_bytes(m, n, a.kp))
+    scratch = _SCRATCH.get(need, c.device) if need > 0 else None
+    _lib.check("qeb_tf32_gemm", lib.qeb_tf32_gemm(
+        m, n, a.kp, a.hi.data_ptr(), a.lo.data_ptr(), a.kp, b0.hi.data_ptr(), b0.lo.data_ptr(),
+        b1.hi.data_ptr(), b1.lo.data_ptr(), b0.kp, al, be, c.data_ptr(), leading_dimension(c),
+        0 if scratch is None else scratch.data_ptr(), need, stream_handle()))
+    return c
+
+
+def tf32_error() -> int:
+    """Non-zero if a bounded wait inside the tcgen05 GEMM timed out (synchronises)."""
+    value = ctypes.c_int(0)
+    _lib.check("qeb_tf32_gemm_error", _lib.load().qeb_tf32_gemm_error(ctypes.byref(value)))
+    return int(value.value)
+
+
+def gemm_tf32(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None,
+              alpha: complex = 1.0, beta: complex = 0.0,
+              a_packed: PackedOperand | None = None) -> torch.Tensor:
+    """Complex c = alpha op(a) b + beta c with split-TF32 tensor-core products.
+
+    op_a = OP_C: a is K x M (op(a) = a^H); OP_N: a is M x K.  ``a_packed``
+    reuses an operand packed earlier with the matching layout.
+    """
+    _check_matrix("b", b)
+    if op_a == OP_C:
+        a_op = a_packed if a_packed is not None else tf32_pack(a, PACK_RAW)
+        b0, b1 = tf32_pack(b, PACK_RAW), tf32_pack(b, PACK_SWAPNEG)
+    elif op_a == OP_N:
+        a_op = a_packed if a_packed is not None else tf32_pack(a, PACK_RAW, transposed=True)
+        b0, b1 = tf32_pack(b, PACK_NEGIM), tf32_pack(b, PACK_SWAP)
+    else:
+        raise ValueError("op_a must be OP_N or OP_C")
+    if a_op.k != b.shape[0]:
+        raise ValueError("inner dimensions disagree")
+    if c is None:
+        c = empty_f(a_op.rows, b.shape[1], torch.complex64, b.device)
+        beta = 0.0
+        if a_op.k == 0:
+            return c.zero_()
+    elif a_op.k == 0:  # empty contraction: c = beta c
+        return c.mul_(beta)
+    return tf32_gemm(a_op, b0, b1, c, alpha, beta)
+
+
 def column_squared_norms(v: torch.Tensor) -> torch.Tensor:
     _check_matrix("v", v)
     out = torch.empty(v.shape[1], dtype=torch.float64, device=v.device)

@@ -1,0 +1,285 @@
+"""Radial tables, structure-dependent set-up terms and the LDA functional.
+
+Host-side set-up of the SCF (once per run or per k point), restated from the
+reference so that the GPU Hamiltonian sees the same operator:
+  * V_loc(|G|): dq = 0.01 table of the short-range part with the analytic
+    -Z erf(r)/r tail restored, G = 0 "alpha Z" term (qepy_pw/upf.py:107-222)
+  * beta_l(|k+G|): dq = 0.01 radial transform table, 4-point Lagrange
+    interpolation, 4 pi / sqrt(Omega) normalisation (qepy_pw/upf.py:270-326)
+  * projector columns (-i)^l Y_lm beta_l (qepy_pw/upf.py:483-556,
+    _native_fft.pyx:1702-1791)
+  * Ewald energy (qepy_pw/ewald.py:49-143, QE ewald.f90)
+  * PZ81 LDA (Perdew-Zunger 1981 parametrisation of Ceperley-Alder,
+    unpolarised; the reference's qepy_pw/xc.py:862-929).
+Energies are in Hartree internally.
+"""
+
+from __future__ import annotations
+
+import math
+
+import numpy as np
+from scipy.special import erf, erfc
+
+DQ = 0.01
+
+
+def qe_simpson(values: np.ndarray, rab: np.ndarray) -> np.ndarray:
+    """QE simpsn on a radial mesh (qepy_pw/upf.py:917-943): weights 1,4,2,...,4,1
+    times rab/3 along the last axis; an even-length mesh corrects the last
+    three weights."""
+    n = rab.size
+    if n < 3 or values.shape[-1] != n:
+        raise ValueError("Simpson integration needs matching arrays of length >= 3")
+    w = np.zeros(n)
+    w[0] = w[-1] = 1.0
+    w[1:-1:2] = 4.0
+    w[2:-1:2] = 2.0
+    if n % 2 == 0:
+        w[-3] -= 0.25
+        w[-2] += 1.0
+        w[-1] = 1.25
+    return np.tensordot(values, rab * w / 3.0, axes=([-1], [0]))
+
+
+def spherical_jn(l: int, x: np.ndarray) -> np.ndarray:
+    """j_l(x) for l <= 1: power series for |x| < l + 1 (at least 1), closed
+    form above, as the reference's special.spherical_jn does for these orders."""
+    x = np.asarray(x, dtype=float)
+    out = np.empty_like(x)
+    small = np.abs(x) < max(1.0, float(l + 1))
+    if np.any(small):
+        xs = x[small]
+        odd = 1.0
+        for k in range(1, 2 * l + 2, 2):
+            odd *= k
+        term = xs**l / odd
+        total = term.copy()
+        for i in range(1, 80):
+            term = term * (-xs * xs / (2.0 * i * (2.0 * l + 2.0 * i + 1.0)))
+            total += term
+            if np.all(np.abs(term) <= 2.0e-16 * (1.0 + np.abs(total))):
+                break
+        out[small] = total
+    if np.any(~small):
+        xl = x[~small]
+        j0 = np.sin(xl) / xl
+        out[~small] = j0 if l == 0 else j0 / xl - np.cos(xl) / xl
+    if l > 1:
+        raise ValueError("only l <= 1 projectors are used by the benchmark cells")
+    return out
+
+
+def lagrange4(table: np.ndarray, q: np.ndarray) -> np.ndarray:
+    """QE four-point interpolation of a dq table (_native_fft.pyx:1556-1600)."""
+    scaled = q / DQ
+    lower = np.floor(scaled).astype(np.int64)
+    f = scaled - lower
+    u, v, w = 1.0 - f, 2.0 - f, 3.0 - f
+    if table.ndim == 1:
+        return (table[lower] * u * v * w / 6.0 + table[lower + 1] * f * v * w / 2.0
+                - table[lower + 2] * f * u * w / 2.0 + table[lower + 3] * f * u * v / 6.0)
+    return (table[lower] * (u * v * w / 6.0)[:, None] + table[lower + 1] * (f * v * w / 2.0)[:, None]
+            - table[lower + 2] * (f * u * w / 2.0)[:, None]
+            + table[lower + 3] * (f * u * v / 6.0)[:, None])
+
+
+class SpeciesTables:
+    """V_loc(q) and beta_l(q) of one pseudopotential in one cell volume."""
+
+    def __init__(self, pseudo, volume: float) -> None:
+        self.pseudo = pseudo
+        self.volume = float(volume)
+        self._vloc = None
+        self._vloc_qmax = -1.0
+        self._beta = None
+        self._beta_qmax = -1.0
+
+    # -- local potential ------------------------------------------------------
+    def _vloc_table(self, qmax: float) -> np.ndarray:
+        if self._vloc is not None and self._vloc_qmax + 1.0e-14 >= qmax:
+            return self._vloc
+        p = self.pseudo
+        beyond = np.flatnonzero(p.r > 10.0)
+        count = int(beyond[0] + 1) if len(beyond) else len(p.r)
+        if count % 2 == 0:
+            count -= 1
+        r, rab = p.r[:count], p.rab[:count]
+        short = r * (0.5 * p.vloc_ry[:count]) + p.z_valence * erf(r)
+        size = int(qmax / DQ + 4)
+        q = np.arange(size) * DQ
+        table = np.empty(size)
+        pref = 4.0 * np.pi / self.volume
+        for b in range(0, size, 128):
+            qb = q[b:b + 128]
+            qr = np.multiply.outer(qb, r)
+            sinc = np.ones_like(qr)
+            np.divide(np.sin(qr), qb[:, None], out=sinc, where=qb[:, None] != 0.0)
+            if b == 0:
+                sinc[0] = r
+            table[b:b + 128] = pref * qe_simpson(sinc * short[None, :], rab)
+        self._vloc, self._vloc_qmax = table, qmax
+        return table
+
+    def vloc(self, q: np.ndarray) -> np.ndarray:
+        """Periodic V_loc(|G|) in Hartree including the 1/Omega factor."""
+        q = np.asarray(q, dtype=float)
+        p = self.pseudo
+        out = np.zeros_like(q)
+        positive = q > 1.0e-12
+        if np.any(~positive):
+            beyond = np.flatnonzero(p.r > 10.0)
+            count = int(beyond[0] + 1) if len(beyond) else len(p.r)
+            if count % 2 == 0:
+                count -= 1
+            r, rab = p.r[:count], p.rab[:count]
+            out[~positive] = 4.0 * np.pi / self.volume * qe_simpson(
+                r * (r * 0.5 * p.vloc_ry[:count] + p.z_valence), rab)
+        if np.any(positive):
+            qp = q[positive]
+            table = self._vloc_table(float(qp.max()))
+            out[positive] = lagrange4(table, qp) - (4.0 * np.pi / self.volume) * p.z_valence \
+                * np.exp(-0.25 * qp**2) / qp**2
+        return out
+
+    # -- projectors -----------------------------------------------------------
+    def _beta_table(self, qmax: float) -> np.ndarray:
+        if self._beta is not None and self._beta_qmax + 1.0e-14 >= qmax:
+            return self._beta
+        p = self.pseudo
+        size = int(np.floor(qmax / DQ + 4.0 + 0.5))
+        q = np.arange(size) * DQ
+        table = np.empty((size, len(p.betas)))
+        pref = 4.0 * np.pi / np.sqrt(self.volume)
+        for column, (rbeta, l, cutoff) in enumerate(zip(p.betas, p.angular_momenta, p.cutoff_indices)):
+            count = min(cutoff, len(p.r), len(rbeta))
+            r = p.r[:count]
+            radial = rbeta[:count] * r
+            for b in range(0, size, 128):
+                bessel = spherical_jn(l, np.multiply.outer(q[b:b + 128], r)) * radial[None, :]
+                table[b:b + 128, column] = pref * qe_simpson(bessel, p.rab[:count])
+        self._beta, self._beta_qmax = table, qmax
+        return table
+
+    @property
+    def channels(self) -> int:
+        return sum(2 * l + 1 for l in self.pseudo.angular_momenta)
+
+    def projectors(self, kg: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """Species beta columns (npw, channels) and the channel coupling
+        0.5 D_Ry (qepy_pw/upf.py:483-556)."""
+        p = self.pseudo
+        q = np.sqrt(kg[:, 0] ** 2 + kg[:, 1] ** 2 + kg[:, 2] ** 2)
+        radial = lagrange4(self._beta_table(float(q.max()) if q.size else 0.0), q)
+        safe = q > 1.0e-14
+        inv = np.where(safe, 1.0 / np.where(safe, q, 1.0), 0.0)
+        x = np.where(safe, kg[:, 0] * inv, 0.0)
+        y = np.where(safe, kg[:, 1] * inv, 0.0)
+        z = np.where(safe, kg[:, 2] * inv, 1.0)
+        s0 = 1.0 / math.sqrt(4.0 * math.pi)
+        s1 = math.sqrt(3.0 / (4.0 * math.pi))
+        columns, ident = [], []
+        for index, l in enumerate(p.angular_momenta):
+            if l == 0:
+                harmonics = (np.full_like(q, s0),)
+            elif l == 1:
+                harmonics = (s1 * z, -s1 * x, -s1 * y)
+            else:
+                raise ValueError("only l <= 1 projectors are supported")
+            for m, h in enumerate(harmonics):
+                columns.append(((-1j) ** l) * radial[:, index] * h)
+                ident.append((index, l, m))
+        beta = np.asfortranarray(np.stack(columns, axis=1))
+        coupling = np.zeros((len(ident), len(ident)))
+        for i, (ri, li, mi) in enumerate(ident):
+            for j, (rj, lj, mj) in enumerate(ident):
+                if li == lj and mi == mj:
+                    coupling[i, j] = 0.5 * p.dij_ry[ri, rj]
+        return beta, coupling
+
+
+def ewald_energy(lattice: np.ndarray, positions: np.ndarray, charges: np.ndarray,
+                 ecutrho_ry: float) -> float:
+    """Ion-ion Ewald energy in Hartree (qepy_pw/ewald.py:49-143)."""
+    lattice = np.asarray(lattice, dtype=float)
+    positions = np.asarray(positions, dtype=float)
+    charges = np.asarray(charges, dtype=float)
+    volume = abs(float(np.linalg.det(lattice)))
+    reciprocal = 2.0 * np.pi * np.linalg.inv(lattice).T
+    total = float(np.sum(charges))
+    alpha = 2.9
+    while True:
+        alpha -= 0.1
+        bound = 2.0 * total**2 * np.sqrt(alpha / np.pi) * erfc(np.sqrt(ecutrho_ry / (4.0 * alpha)))
+        if bound <= 1.0e-7:
+            break
+        if alpha <= 0.0:
+            raise RuntimeError("optimal Ewald alpha not found")
+    # reciprocal-space sum over |G|^2 <= ecutrho (lexicographic Miller order)
+    smin = float(np.linalg.svd(reciprocal, compute_uv=False)[-1])
+    nmax = int(np.ceil(np.sqrt(ecutrho_ry) / smin)) + 1
+    axis = np.arange(-nmax, nmax + 1)
+    recip_sum = -total**2 / (4.0 * alpha)
+    acc = 0.0
+    for i in axis:
+        yz = np.stack(np.meshgrid(axis, axis, indexing="ij"), -1).reshape(-1, 2)
+        miller = np.column_stack((np.full(len(yz), i), yz))
+        g = miller @ reciprocal
+        g2 = np.einsum("ij,ij->i", g, g)
+        keep = (g2 <= ecutrho_ry) & (g2 > 1.0e-14)
+        g, g2 = g[keep], g2[keep]
+        if not g2.size:
+            continue
+        structure = np.exp(-1j * (positions @ g.T)).T @ charges
+        acc += float(np.sum(np.abs(structure) ** 2 * np.exp(-g2 / (4.0 * alpha)) / g2))
+    recip_sum = (recip_sum + acc) * 4.0 * np.pi / volume
+    recip_sum -= float(np.sum(charges**2) * 2.0 * np.sqrt(alpha / np.pi))
+    # real-space sum within 4/sqrt(alpha)
+    radius = 4.0 / np.sqrt(alpha)
+    lmin = float(np.linalg.svd(lattice, compute_uv=False)[-1])
+    real_sum = 0.0
+    sqa = np.sqrt(alpha)
+    for a, qa in zip(positions, charges):
+        d0 = a - positions  # (nat, 3)
+        reach = np.linalg.norm(d0, axis=1)
+        nb = int(np.ceil((radius + reach.max()) / lmin)) + 1
+        rng = np.arange(-nb, nb + 1)
+        images = np.stack(np.meshgrid(rng, rng, rng, indexing="ij"), -1).reshape(-1, 3) @ lattice
+        d = d0[:, None, :] + images[None, :, :]
+        dist = np.linalg.norm(d, axis=2)
+        mask = (dist >= 1.0e-14) & (dist <= radius)
+        contrib = np.where(mask, erfc(sqa * np.where(mask, dist, 1.0)) / np.where(mask, dist, 1.0), 0.0)
+        real_sum += qa * float(np.sum(charges * contrib.sum(axis=1)))
+    return 0.5 * (recip_sum + 0.5 * real_sum)
+
+
+def pz81(rho: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """(eps_xc, v_xc) in Hartree of the unpolarised PZ81 LDA.
+
+    Slater exchange eps_x = -(3/4)(3/pi)^(1/3) rho^(1/3) = -0.458165/r_s and
+    the Perdew-Zunger (1981) correlation: for r_s >= 1
+    eps_c = gamma/(1 + beta1 sqrt(r_s) + beta2 r_s), otherwise
+    eps_c = A ln r_s + B + C r_s ln r_s + D r_s, with gamma = -0.1423,
+    beta1 = 1.0529, beta2 = 0.3334, A = 0.0311, B = -0.048, C = 0.0020,
+    D = -0.0116; v = eps - (r_s/3) d eps/d r_s.  Densities at or below 1e-10
+    give zero, as the reference's LDA driver does.
+    """
+    d = np.abs(np.asarray(rho, dtype=np.float64))
+    active = d > 1.0e-10
+    d = np.maximum(d, 1.0e-10)
+    rs = 0.6203504908994 / np.cbrt(d)
+    eps = -0.687247939924714 * (2.0 / 3.0) / rs
+    v = (4.0 / 3.0) * eps
+    high = rs < 1.0
+    lnrs = np.log(rs)
+    ec_high = 0.0311 * lnrs - 0.048 + 0.0020 * rs * lnrs - 0.0116 * rs
+    vc_high = ec_high - (0.0311 + (0.0020 * (lnrs + 1.0) - 0.0116) * rs) / 3.0
+    sq = np.sqrt(rs)
+    den = 1.0 + 1.0529 * sq + 0.3334 * rs
+    ec_low = -0.1423 / den
+    vc_low = ec_low + (-0.1423 / 3.0) * rs * (0.5 * 1.0529 / sq + 0.3334) / den**2
+    eps = eps + np.where(high, ec_high, ec_low)
+    v = v + np.where(high, vc_high, vc_low)
+    eps[~active] = 0.0
+    v[~active] = 0.0
+    return eps, v
