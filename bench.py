@@ -58,7 +58,36 @@ def parse_args():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=10.0,
                    help="approximate CPU time budget of the cpu_baseline sample")
+    p.add_argument("--scf", default="scf-fcc2",
+                   help="benchmark cell whose SCF-to-1e-8 Ry time is reported beside the "
+                        "H|psi> rate (scf-fcc2, scf-dia8-disp, scf-dia64, scf-dia216, none)")
     return p.parse_args()
+
+
+def scf_times(name: str) -> dict:
+    """Wall time of the GPU SCF to conv_thr = 1e-8 Ry, plain FP64 and mixed."""
+    import torch
+
+    from qe_python_b200.scf import benchmark_system, run_scf
+
+    out = {"cell": name, "conv_thr_ry": 1.0e-8}
+    for precision in ("f64", "mixed"):
+        system = benchmark_system(name)
+        torch.cuda.synchronize()
+        started = time.perf_counter()
+        result = run_scf(system, precision=precision)
+        torch.cuda.synchronize()
+        out[precision] = {
+            "seconds": time.perf_counter() - started,
+            "converged": bool(result.converged),
+            "iterations": result.iterations,
+            "total_energy_ry": result.total_energy_ry,
+            "precision_per_iteration": result.precision_log,
+            "phase_seconds": {k: round(v, 3) for k, v in result.timings.items()},
+        }
+    out["mixed_speedup"] = out["f64"]["seconds"] / out["mixed"]["seconds"]
+    out["energy_difference_ry"] = out["mixed"]["total_energy_ry"] - out["f64"]["total_energy_ry"]
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -424,6 +453,8 @@ def run_b200(args) -> None:
                 "h2d_bytes_per_step": npw * nb * 8, "d2h_bytes_per_step": npw * nb * 8},
         "clocks": clocks.summary(),
     }
+    if args.scf and args.scf != "none":
+        line["scf"] = scf_times(args.scf)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample = 16

@@ -44,6 +44,13 @@ int qeb_version(void);
 /* Kernels launched by this library since it was loaded (all threads). */
 int64_t qeb_launch_count(void);
 
+/* Host routine: QE's randy stream as band-major (amplitude, phase) pairs
+ * for the random starting wavefunctions; first/second are column-major
+ * (plane_waves, bands); table (97 entries), current and seed are updated.
+ * Replaces qe_random_pairs (qepy_pw/_native_fft.pyx:1411-1444). */
+int qeb_qe_random_pairs(int64_t plane_waves, int64_t bands, int64_t* table, int64_t* current,
+                        int64_t* seed, double* first, double* second);
+
 /* ------------------------------------------------------------------------
  * Local potential operator on the FFT grid (sticks / planes).
  * ---------------------------------------------------------------------- */

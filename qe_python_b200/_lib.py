@@ -33,6 +33,7 @@ SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_last_error", ctypes.c_char_p, []),
     ("qeb_version", _I, []),
     ("qeb_launch_count", _L, []),
+    ("qeb_qe_random_pairs", _I, [_L, _L, _P, _P, _P, _P, _P]),
     ("qeb_local_plan_create", _I, [ctypes.POINTER(_P), _I, _I, _I, _L, _P, _I]),
     ("qeb_local_plan_destroy", _I, [_P]),
     ("qeb_local_plan_info", _I, [_P, _P, _I]),

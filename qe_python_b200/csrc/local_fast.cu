@@ -321,9 +321,9 @@ struct SetLimits {
     cudaError_t err = cudaSuccess;
     if (p->fast_z >= 0 && F::n == p->nz) {
       const int s = (int)ac_smem<T, F>(p->nz_pad);
-      err = cudaFuncSetAttribute(four_pass_a<T, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+      err = qeb::raise_smem_limit(four_pass_a<T, F>, s);
       if (err == cudaSuccess)
-        err = cudaFuncSetAttribute(four_pass_c<T, F>, cudaFuncAttributeMaxDynamicSharedMemorySize, s);
+        err = qeb::raise_smem_limit(four_pass_c<T, F>, s);
     }
     if (err == cudaSuccess && p->fast_xy >= 0 && F::n == p->nx) {
       const size_t s = b_smem<T, F>(p);
@@ -331,9 +331,9 @@ struct SetLimits {
         qeb::set_error("four-step pass B needs %zu bytes of shared memory", s);
         return QEB_EUNSUPPORTED;
       }
-      err = cudaFuncSetAttribute(four_pass_b<T, F, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s);
+      err = qeb::raise_smem_limit(four_pass_b<T, F, 0>, s);
       if (err == cudaSuccess)
-        err = cudaFuncSetAttribute(four_pass_b<T, F, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)s);
+        err = qeb::raise_smem_limit(four_pass_b<T, F, 1>, s);
     }
     return qeb::cuda_status(err, "four-step shared memory attribute");
   }

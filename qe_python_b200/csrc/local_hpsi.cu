@@ -193,13 +193,13 @@ template <typename T>
 int set_smem_limits(const qeb_local_plan* p) {
   const size_t b = pass_b_smem<T>(p), ac = pass_ac_smem<T>(p);
   cudaError_t err;
-  err = cudaFuncSetAttribute(pass_b_kernel<T, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+  err = qeb::raise_smem_limit(pass_b_kernel<T, 0>, b);
   if (err != cudaSuccess) return qeb::cuda_status(err, "pass B smem attribute");
-  err = cudaFuncSetAttribute(pass_b_kernel<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)b);
+  err = qeb::raise_smem_limit(pass_b_kernel<T, 1>, b);
   if (err != cudaSuccess) return qeb::cuda_status(err, "pass B (density) smem attribute");
-  err = cudaFuncSetAttribute(pass_a_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ac);
+  err = qeb::raise_smem_limit(pass_a_kernel<T>, ac);
   if (err != cudaSuccess) return qeb::cuda_status(err, "pass A smem attribute");
-  err = cudaFuncSetAttribute(pass_c_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ac);
+  err = qeb::raise_smem_limit(pass_c_kernel<T>, ac);
   if (err != cudaSuccess) return qeb::cuda_status(err, "pass C smem attribute");
   return QEB_OK;
 }

@@ -55,3 +55,36 @@ extern "C" const char* qeb_last_error(void) { return qeb::g_last_error; }
 extern "C" int qeb_version(void) { return QEB_ABI_VERSION; }
 
 extern "C" int64_t qeb_launch_count(void) { return qeb::g_launches.load(); }
+
+// QE randy stream (a 97-entry shuffle table over the LCG
+// seed <- (1366 seed + 150889) mod 714025), drawn in band-outer,
+// plane-wave-inner order as (amplitude, phase) pairs; host code.
+// Same recurrence as qepy_pw/_native_fft.pyx qe_random_pairs (:1411-1444).
+extern "C" int qeb_qe_random_pairs(int64_t plane_waves, int64_t bands, int64_t* table,
+                                   int64_t* current, int64_t* seed, double* first,
+                                   double* second) {
+  if (plane_waves < 0 || bands < 0 || table == nullptr || current == nullptr ||
+      seed == nullptr || (plane_waves * bands > 0 && (first == nullptr || second == nullptr))) {
+    qeb::set_error("qe_random_pairs: invalid arguments");
+    return QEB_EINVAL;
+  }
+  int64_t cur = *current, s = *seed;
+  for (int64_t b = 0; b < bands; ++b) {
+    for (int64_t g = 0; g < plane_waves; ++g) {
+      const int64_t out = g + b * plane_waves;
+      int64_t i = (97 * cur) / 714025;
+      cur = table[i];
+      first[out] = (double)cur / 714025.0;
+      s = (1366 * s + 150889) % 714025;
+      table[i] = s;
+      i = (97 * cur) / 714025;
+      cur = table[i];
+      second[out] = (double)cur / 714025.0;
+      s = (1366 * s + 150889) % 714025;
+      table[i] = s;
+    }
+  }
+  *current = cur;
+  *seed = s;
+  return QEB_OK;
+}

@@ -31,6 +31,19 @@ int cuda_status(cudaError_t err, const char* where);
 // Process-wide count of kernels launched by this library (qeb_launch_count).
 void count_launches(int n);
 
+// Raise (never lower) a kernel's dynamic shared-memory limit on the current
+// device: the attribute is per kernel, while plans of different sizes share
+// the kernel.
+template <typename Kernel>
+cudaError_t raise_smem_limit(Kernel* kernel, size_t bytes) {
+  cudaFuncAttributes attr;
+  cudaError_t err = cudaFuncGetAttributes(&attr, reinterpret_cast<const void*>(kernel));
+  if (err != cudaSuccess) return err;
+  if ((size_t)attr.maxDynamicSharedSizeBytes >= bytes) return cudaSuccess;
+  return cudaFuncSetAttribute(reinterpret_cast<const void*>(kernel),
+                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
 template <typename T>
 struct alignas(2 * sizeof(T)) C2 {
   T re, im;

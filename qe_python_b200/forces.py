@@ -1,0 +1,160 @@
+"""Hellmann-Feynman forces at SCF convergence.
+
+F = F_nonlocal + F_local + F_ewald (symmetrised when the space group is
+non-trivial), minus the mean force, as qepy_pw/pw/scf.py:4143-4227 assembles
+them (no core correction in the supported pseudopotentials).
+  F_nonlocal[atom] = -2 sum_k w_k Re sum_{p in atom, b} f_b
+                     conj(d becp_a[p, b]) (D becp)[p, b],
+                     d becp_a = beta_atom^H (i (k+G)_a psi)     (scf.py:1521-1631)
+  F_local[atom]    = Omega Re sum_G conj(rho(G)) i G V_loc(|G|) e^{-i G tau}
+                                                                 (scf.py:1634-1673)
+  F_ewald          = -dE_ewald/dtau with E_ewald's alpha and G set
+                                                                 (ewald.py:144-260)
+The three d becp products per k point are complex GEMMs on the GPU
+(libqeb200.so); the per-atom reductions are small host sums.  Hartree/bohr.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+from scipy.special import erfc
+
+from . import kernels as K
+from .device import empty_f, to_device_f
+
+
+def ewald_forces(lattice, positions, charges, ecutrho_ry, g_vectors) -> np.ndarray:
+    lattice = np.asarray(lattice, dtype=float)
+    positions = np.asarray(positions, dtype=float)
+    charges = np.asarray(charges, dtype=float)
+    volume = abs(float(np.linalg.det(lattice)))
+    total = float(np.sum(charges))
+    alpha = 2.9
+    while True:
+        alpha -= 0.1
+        if 2.0 * total**2 * np.sqrt(alpha / np.pi) * erfc(np.sqrt(ecutrho_ry / (4.0 * alpha))) <= 1.0e-7:
+            break
+        if alpha <= 0.0:
+            raise RuntimeError("optimal Ewald alpha not found")
+    g = np.asarray(g_vectors, dtype=float)
+    g2 = np.einsum("ij,ij->i", g, g)
+    keep = g2 > 1.0e-14
+    g, g2 = g[keep], g2[keep]
+    forces = np.zeros_like(positions)
+    weight = 2.0 * np.pi / volume * np.exp(-g2 / (4.0 * alpha)) / g2
+    structure = np.zeros(len(g2), dtype=np.complex128)
+    chunk = 64
+    for a0 in range(0, len(positions), chunk):
+        ph = np.exp(-1j * (positions[a0:a0 + chunk] @ g.T))
+        structure += charges[a0:a0 + chunk] @ ph
+    conj_s = np.conj(structure)
+    for a0 in range(0, len(positions), chunk):
+        ph = np.exp(-1j * (positions[a0:a0 + chunk] @ g.T))
+        deriv = 2.0 * np.real(conj_s[None, :] * (-1j * charges[a0:a0 + chunk, None] * ph))
+        forces[a0:a0 + chunk] -= (weight[None, :] * deriv) @ g
+    radius = 4.0 / np.sqrt(alpha)
+    lmin = float(np.linalg.svd(lattice, compute_uv=False)[-1])
+    ra = np.sqrt(alpha)
+    for i, (left, qi) in enumerate(zip(positions, charges)):
+        d0 = left - positions
+        nb = int(np.ceil((radius + np.linalg.norm(d0, axis=1).max()) / lmin)) + 1
+        rng = np.arange(-nb, nb + 1)
+        images = np.stack(np.meshgrid(rng, rng, rng, indexing="ij"), -1).reshape(-1, 3) @ lattice
+        d = d0[:, None, :] + images[None, :, :]
+        dist = np.linalg.norm(d, axis=2)
+        mask = (dist >= 1.0e-14) & (dist <= radius)
+        safe = np.where(mask, dist, 1.0)
+        radial = -erfc(ra * safe) / safe**2 - 2.0 * ra / np.sqrt(np.pi) * np.exp(-alpha * safe**2) / safe
+        grad = 0.25 * qi * charges[:, None, None] * (radial / safe)[:, :, None] * d
+        grad = np.where(mask[:, :, None], grad, 0.0).sum(axis=1)  # (nat, 3), one per right atom
+        forces[i] -= grad.sum(axis=0)
+        forces += grad
+    return forces
+
+
+def local_forces(system, tables, grid, rho) -> np.ndarray:
+    """Omega Re sum_G conj(rho(G)) i G V_loc(|G|) exp(-i G tau), on the GPU."""
+    device = torch.device("cuda", torch.cuda.current_device())
+    rho_g = torch.from_numpy(grid.to_g(rho)).to(device)
+    gvec = torch.from_numpy(grid.vectors).to(device)
+    q = np.sqrt(grid.g2)
+    out = np.zeros((len(system.positions), 3))
+    for label, table in tables.items():
+        vloc = torch.from_numpy(table.vloc(q)).to(device)
+        weight = torch.conj(rho_g) * vloc  # (nG,)
+        idx = [i for i, l in enumerate(system.labels) if l == label]
+        for a0 in range(0, len(idx), 32):
+            atoms = idx[a0:a0 + 32]
+            pos = torch.from_numpy(system.positions[atoms]).to(device)
+            phase = torch.exp(-1j * (pos @ gvec.T))               # (na, nG)
+            term = (1j * weight)[None, :] * phase                   # (na, nG)
+            f = torch.real(term @ gvec.to(torch.complex128))        # (na, 3)
+            out[atoms] = system.volume * f.cpu().numpy()
+    return out
+
+
+def nonlocal_forces(system, states, tables, occupied) -> np.ndarray:
+    out = np.zeros((len(system.positions), 3))
+    f_b = 2.0  # fixed occupations
+    for state, weight in zip(states, system.weights):
+        basis = state.basis
+        device = state.vectors.device
+        psi = state.vectors[:, :occupied]
+        if psi.dtype != torch.complex128:
+            psi = psi.to(torch.complex128)
+        psi = psi.T.contiguous().T
+        vectors = basis.vectors
+        kg = torch.from_numpy(vectors).to(device)
+        for label, table in tables.items():
+            atom_index = [i for i, l in enumerate(system.labels) if l == label]
+            if not atom_index or table.channels == 0:
+                continue
+            species, coupling1 = table.projectors(vectors)
+            angle = vectors @ system.positions[atom_index].T
+            phases = to_device_f(np.cos(angle) - 1j * np.sin(angle), torch.complex128, device)
+            species = to_device_f(species, torch.complex128, device)
+            natoms, c = phases.shape[1], species.shape[1]
+            beta = empty_f(len(basis), natoms * c, torch.complex128, device)
+            for a in range(natoms):
+                beta[:, a * c:(a + 1) * c] = species * phases[:, a:a + 1]
+            coupling = to_device_f(np.kron(np.eye(natoms), coupling1).astype(np.complex128),
+                                   torch.complex128, device)
+            becp = K.gemm(K.OP_C, beta, psi)
+            coupled = K.gemm(K.OP_N, coupling, becp).cpu().numpy()
+            for axis in range(3):
+                scaled = (psi * (1j * kg[:, axis:axis + 1])).T.contiguous().T
+                dbecp = K.gemm(K.OP_C, beta, scaled).cpu().numpy()
+                contrib = np.real(np.conj(dbecp) * coupled).sum(axis=1) * f_b  # per channel
+                out[atom_index, axis] -= 2.0 * float(weight) * contrib.reshape(natoms, c).sum(axis=1)
+    return out
+
+
+def hellmann_feynman_forces(system, states, tables, grid, rho, occupied) -> np.ndarray:
+    charges = np.array([system.pseudos[l].z_valence for l in system.labels])
+    components = [
+        nonlocal_forces(system, states, tables, occupied),
+        ewald_forces(system.lattice, system.positions, charges, system.ecutrho, grid.vectors),
+        local_forces(system, tables, grid, rho),
+    ]
+    total = sum(symmetrize_forces(c, system) for c in components)
+    return total - total.mean(axis=0, keepdims=True)
+
+
+def symmetrize_forces(forces: np.ndarray, system) -> np.ndarray:
+    """Average F over the space group: F'(op(atom)) = F(atom) R (cartesian)."""
+    ops = system.operations
+    if len(ops) <= 1:
+        return forces
+    lattice = system.lattice
+    frac = system.positions @ np.linalg.inv(lattice)
+    out = np.zeros_like(forces)
+    for op in ops:
+        rot = np.linalg.inv(lattice) @ op.matrix @ lattice  # cartesian row convention
+        moved = frac @ op.matrix + op.translation
+        for i, x in enumerate(moved):
+            delta = frac - x
+            delta -= np.round(delta)
+            j = int(np.argmin(np.abs(delta).max(axis=1)))
+            out[j] += forces[i] @ rot
+    return out / len(ops)

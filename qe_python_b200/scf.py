@@ -1,0 +1,531 @@
+"""Self-consistent field driver on the B200 H|psi> / Davidson path.
+
+Restates the reference's SCF loop (qepy_pw/pw/scf.py:_run_scf, :1997-4375)
+for the benchmark cells' feature set: norm-conserving pseudopotentials
+without core correction, LDA (PZ81), no spin, fixed occupations, Davidson,
+linear or plain-Broyden density mixing, symmetry-reduced k points.  Each
+k point's Hamiltonian and Davidson solve run on the GPU (PlaneWaveHamiltonian,
+davidson); the density is accumulated by the GPU FFT kernels; the charge-grid
+steps (Hartree, XC, mixing, energies) stay on the host as in the reference.
+
+Precision schedules:
+  'f64'    plain FP64 everywhere on the GPU;
+  'mixed'  chosen form: FP32 FFT passes and split-TF32 projector GEMMs
+           until the density residual falls below ``switch_ry``, then FP64
+           H|psi> for the remaining iterations (eigenvalues, energies and the
+           density accumulation are always FP64).
+Energies are Hartree internally; SCFResult reports both units.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.fft
+import torch
+
+from . import _lib
+from . import kernels as K
+from .basis import LocalPotentialWorkspace, fft_shape, make_bases
+from .configs import DIAMOND_CUBIC, displacements, supercell
+from .device import empty_f, require_cuda, to_device_f
+from .diagonalization import PlaneWaveHamiltonian, davidson, lowest_generalized_eigh
+from .pseudo import SyntheticPseudo, synthetic_pseudo
+from .pseudo_tables import SpeciesTables, ewald_energy, pz81
+from .symmetry import (
+    DensitySymmetrizer,
+    Operation,
+    fft_factors,
+    mesh_compatible,
+    monkhorst_pack,
+    reduce_kpoints,
+    space_group,
+)
+
+
+@dataclass
+class System:
+    """A periodic cell and the SCF controls (Hartree internally)."""
+
+    lattice: np.ndarray          # rows = lattice vectors (bohr)
+    positions: np.ndarray        # cartesian atom positions (bohr)
+    labels: list[str]
+    pseudos: dict[str, SyntheticPseudo]
+    ecutwfc: float               # Ry
+    ecutrho: float               # Ry
+    nbnd: int
+    kpoints: np.ndarray          # crystal coordinates
+    weights: np.ndarray          # sum to 1
+    operations: list[Operation]
+    conv_thr: float = 1.0e-8     # Ry
+    mixing_mode: str = "plain"
+    mixing_beta: float = 0.7
+    mixing_ndim: int = 8
+    diago_david_ndim: int = 2
+    maxiter: int = 100
+    forces: bool = False
+    name: str = ""
+
+    @property
+    def volume(self) -> float:
+        return abs(float(np.linalg.det(self.lattice)))
+
+    @property
+    def reciprocal(self) -> np.ndarray:
+        return 2.0 * np.pi * np.linalg.inv(self.lattice).T
+
+    @property
+    def nelec(self) -> float:
+        return float(sum(self.pseudos[l].z_valence for l in self.labels))
+
+
+def benchmark_system(name: str) -> System:
+    """The benchmark cells of qe_python_b200.configs as System objects."""
+    pseudo = synthetic_pseudo("X")
+    if name == "scf-fcc2":
+        a = 10.26
+        lattice = a / 2.0 * np.array([[-1.0, 0.0, 1.0], [0.0, 1.0, 1.0], [-1.0, 1.0, 0.0]])
+        positions = np.array([[0.0, 0.0, 0.0], [0.25, 0.25, 0.25]]) * a
+        grid, shift, ecut, ecutrho, nbnd = (4, 4, 4), (1, 1, 1), 20.0, 80.0, 8
+        mixing, forces = "linear", False
+    elif name == "scf-dia64":
+        lattice = np.eye(3) * 20.52
+        positions = supercell(DIAMOND_CUBIC, 2) * 20.52
+        grid, shift, ecut, ecutrho, nbnd = (2, 2, 2), (0, 0, 0), 30.0, 180.0, 160
+        mixing, forces = "plain", False
+    elif name == "scf-dia8-disp":
+        a = 10.26
+        lattice = np.eye(3) * a
+        positions = DIAMOND_CUBIC * a + displacements(8, 0.05)
+        grid, shift, ecut, ecutrho, nbnd = (3, 3, 3), (0, 0, 0), 25.0, 100.0, 24
+        mixing, forces = "plain", True
+    elif name == "scf-dia216":
+        a = 30.78
+        lattice = np.eye(3) * a
+        positions = supercell(DIAMOND_CUBIC, 3) * a + displacements(216, 0.03)
+        grid, shift, ecut, ecutrho, nbnd = None, None, 30.0, 180.0, 480
+        mixing, forces = "plain", True
+    else:
+        raise KeyError(name)
+    labels = ["X"] * len(positions)
+    frac = positions @ np.linalg.inv(lattice)
+    ops = space_group(lattice, frac, labels)
+    if grid is None:  # Gamma only: the space group is used as found
+        kpoints, weights = np.zeros((1, 3)), np.ones(1)
+    else:
+        points, w = monkhorst_pack(grid, shift)
+        ops = mesh_compatible(points, ops)
+        kpoints, weights, _ = reduce_kpoints(points, w, ops)
+    return System(lattice, positions, labels, {"X": pseudo}, ecut, ecutrho, nbnd, kpoints, weights,
+                  ops, mixing_mode=mixing, forces=forces, name=name)
+
+
+# ---------------------------------------------------------------------------
+# host pieces of the loop
+
+class QERandom:
+    """QE randy stream (qepy_pw/pw/scf.py:452-538); pairs drawn by the host
+    routine qeb_qe_random_pairs of libqeb200.so."""
+
+    M, A, C, NT = 714025, 1366, 150889, 97
+
+    def __init__(self, seed: int = 0) -> None:
+        s = min(abs(int(seed)), self.C)
+        s = (self.C - s) % self.M
+        self.table = np.empty(self.NT, dtype=np.int64)
+        for i in range(self.NT):
+            s = (self.A * s + self.C) % self.M
+            self.table[i] = s
+        s = (self.A * s + self.C) % self.M
+        self.seed = s
+        self.current = s
+
+    def pairs(self, plane_waves: int, bands: int) -> tuple[np.ndarray, np.ndarray]:
+        first = np.empty((plane_waves, bands), order="F")
+        second = np.empty((plane_waves, bands), order="F")
+        cur = ctypes.c_int64(self.current)
+        seed = ctypes.c_int64(self.seed)
+        _lib.check("qeb_qe_random_pairs", _lib.load().qeb_qe_random_pairs(
+            plane_waves, bands, self.table.ctypes.data, ctypes.byref(cur), ctypes.byref(seed),
+            first.ctypes.data, second.ctypes.data))
+        self.current, self.seed = int(cur.value), int(seed.value)
+        return first, second
+
+
+class ChargeGrid:
+    """Charge-density sphere on the FFT grid (qepy_pw/pw/scf.py:268-321)."""
+
+    def __init__(self, shape, reciprocal: np.ndarray, cutoff_ry: float) -> None:
+        self.shape = tuple(int(v) for v in shape)
+        axes = [np.rint(np.fft.fftfreq(n) * n).astype(np.int32) for n in self.shape]
+        metric = reciprocal @ reciprocal.T
+        x, y, z = axes[0][:, None, None], axes[1][None, :, None], axes[2][None, None, :]
+        g2 = (metric[0, 0] * x * x + metric[1, 1] * y * y + metric[2, 2] * z * z
+              + 2.0 * metric[0, 1] * x * y + 2.0 * metric[0, 2] * x * z + 2.0 * metric[1, 2] * y * z)
+        self.slots = np.argwhere(g2 <= cutoff_ry + 1.0e-12).astype(np.int32)
+        self.index = tuple(self.slots.T)
+        self.miller = np.column_stack([axes[a][self.slots[:, a]] for a in range(3)]).astype(np.int32)
+        self.vectors = self.miller @ reciprocal
+        self.g2 = g2[self.index]
+        self.size = int(np.prod(self.shape))
+
+    def to_g(self, grid: np.ndarray) -> np.ndarray:
+        """Forward FFT divided by N_r, gathered on the sphere."""
+        return scipy.fft.fftn(grid, workers=-1)[self.index] / self.size
+
+    def to_r(self, coefficients: np.ndarray) -> np.ndarray:
+        """Unnormalised inverse FFT of sphere coefficients (real part)."""
+        full = np.zeros(self.shape, dtype=np.complex128)
+        full[self.index] = coefficients
+        return np.real(scipy.fft.ifftn(full, norm="forward", workers=-1))
+
+
+def hartree(rho_g: np.ndarray, g2: np.ndarray) -> np.ndarray:
+    out = np.zeros_like(rho_g)
+    mask = g2 > 1.0e-14
+    out[mask] = 4.0 * np.pi * rho_g[mask] / g2[mask]
+    return out
+
+
+def neumaier_metric(residual: np.ndarray, g2: np.ndarray) -> float:
+    """sum 4 pi |drho(G)|^2 / G^2 with Neumaier compensation (_native_fft.pyx:1922-1970)."""
+    mask = g2 > 1.0e-14
+    terms = 4.0 * np.pi * (residual[mask].real ** 2 + residual[mask].imag ** 2) / g2[mask]
+    total = 0.0
+    correction = 0.0
+    for t in terms.tolist():
+        u = total + t
+        correction += (total - u) + t if total >= t else (t - u) + total
+        total = u
+    return total + correction
+
+
+class BroydenMixer:
+    """Plain Broyden mixing of rho(G) in the Coulomb metric
+    (qepy_pw/mixing.py:621-759, mode 'plain')."""
+
+    def __init__(self, grid: ChargeGrid, beta: float, ndim: int, cutoff_ry: float) -> None:
+        self.grid = grid
+        self.beta = float(beta)
+        self.ndim = int(ndim)
+        active = grid.g2 > 1.0e-14
+        active &= grid.g2 <= cutoff_ry + 1.0e-12
+        self.active = np.flatnonzero(active)
+        self.g2 = grid.g2[self.active]
+        self.dx: list[np.ndarray] = []
+        self.df: list[np.ndarray] = []
+        self._next = 0
+        self.prev_in = None
+        self.prev_res = None
+
+    def _push(self, store: list, value: np.ndarray) -> None:
+        if len(store) < self.ndim:
+            store.append(value)
+
+    def mix(self, rho_in: np.ndarray, residual_g: np.ndarray) -> np.ndarray:
+        current = self.grid.to_g(rho_in)
+        cur = current[self.active].copy()
+        res = residual_g[self.active].copy()
+        saved_in, saved_res = cur.copy(), res.copy()
+        if self.prev_in is not None:
+            dx, df = self.prev_in - cur, self.prev_res - res
+            if len(self.dx) < self.ndim:
+                self.dx.append(dx)
+                self.df.append(df)
+            else:  # cyclic overwrite of one history slot
+                self.dx[self._next] = dx
+                self.df[self._next] = df
+                self._next = (self._next + 1) % self.ndim
+        if self.dx:
+            dfs = np.array(self.df)
+            dxs = np.array(self.dx)
+            weighted = np.conj(dfs) / self.g2[None, :]
+            projection = np.real(weighted @ res)
+            gram = np.real(weighted @ dfs.T)
+            try:
+                gamma = np.linalg.solve(gram, projection)
+            except np.linalg.LinAlgError:
+                gamma = np.linalg.lstsq(gram, projection, rcond=1.0e-14)[0]
+            cur -= gamma @ dxs
+            res -= gamma @ dfs
+        mixed = current + self.beta * residual_g
+        mixed[self.active] = cur + self.beta * res
+        zero = np.flatnonzero(self.grid.g2 <= 1.0e-14)
+        mixed[zero] = current[zero]
+        self.prev_in, self.prev_res = saved_in, saved_res
+        return self.grid.to_r(mixed)
+
+
+class LinearMixer:
+    def __init__(self, beta: float) -> None:
+        self.beta = float(beta)
+
+    def mix(self, rho_in: np.ndarray, rho_out: np.ndarray) -> np.ndarray:
+        return (1.0 - self.beta) * rho_in + self.beta * rho_out
+
+
+@dataclass
+class SCFResult:
+    converged: bool
+    total_energy_ha: float
+    iterations: int
+    energies_ha: list[float]
+    accuracies_ha: list[float]
+    eigenvalues_ha: list[np.ndarray]
+    energy_terms_ha: dict[str, float]
+    density: np.ndarray
+    forces_ha_per_bohr: np.ndarray | None
+    wall_seconds: float
+    precision_log: list[str] = field(default_factory=list)
+    davidson_iterations: list[float] = field(default_factory=list)
+    timings: dict[str, float] = field(default_factory=dict)
+
+    @property
+    def total_energy_ry(self) -> float:
+        return 2.0 * self.total_energy_ha
+
+
+class KPointState:
+    """Per-k device objects reused across SCF iterations."""
+
+    def __init__(self, basis, shape, device) -> None:
+        self.basis = basis.materialize() if basis.catalog is not None else basis
+        self.workspaces: dict[str, LocalPotentialWorkspace] = {}
+        self.shape = shape
+        self.device = device
+        self.vectors: torch.Tensor | None = None
+        self.eigenvalues: np.ndarray | None = None
+        self.terms = None
+
+    def workspace(self, precision: str) -> LocalPotentialWorkspace:
+        if precision not in self.workspaces:
+            self.workspaces[precision] = LocalPotentialWorkspace(
+                self.basis, self.shape, precision=precision, device=self.device)
+        return self.workspaces[precision]
+
+
+def _as128(t: torch.Tensor) -> torch.Tensor:
+    return t if t.dtype == torch.complex128 else t.to(torch.complex128).T.contiguous().T
+
+
+def random_starting_subspace(ham: PlaneWaveHamiltonian, basis, rng: QERandom, nbnd: int):
+    """Random trial vectors amp e^(2 pi i phase) / (1 + |k+G|^2) rotated by a
+    Rayleigh-Ritz step in their span (qepy_pw/pw/scf.py:853-870, 923-953).
+    Returns (vectors, eigenvalues, H vectors) in the Hamiltonian's dtype."""
+    amp, phase = rng.pairs(len(basis), nbnd)
+    trials = amp * np.exp(2j * np.pi * phase) / (1.0 + 2.0 * basis.kinetic[:, None])
+    trials_dev = to_device_f(trials, ham.dtype, ham.device)
+    applied = ham.apply(trials_dev)
+    t128, a128 = _as128(trials_dev), _as128(applied)
+    proj = K.gemm(K.OP_C, t128, a128)
+    over = K.gemm(K.OP_C, t128, t128)
+    values, rot = lowest_generalized_eigh(0.5 * (proj + proj.conj().T),
+                                          0.5 * (over + over.conj().T), nbnd)
+    vectors = K.gemm(K.OP_N, t128, rot.T.contiguous().T)
+    hvectors = K.gemm(K.OP_N, a128, rot.T.contiguous().T)
+    if ham.dtype != torch.complex128:
+        vectors = vectors.to(ham.dtype).T.contiguous().T
+        hvectors = hvectors.to(ham.dtype).T.contiguous().T
+    return vectors, values.cpu().numpy(), hvectors
+
+
+def projector_terms(system: System, tables: dict, basis) -> tuple:
+    """(beta, coupling) per species with atom phases packed
+    (qepy_pw/pw/scf.py:596-718)."""
+    from .diagonalization import FactorizedProjectorTerm
+
+    vectors = basis.vectors
+    terms = []
+    for label, table in tables.items():
+        pos = np.array([p for p, l in zip(system.positions, system.labels) if l == label])
+        if not len(pos) or table.channels == 0:
+            continue
+        beta, coupling = table.projectors(vectors)
+        angle = vectors @ pos.T
+        phases = np.asfortranarray(np.cos(angle) - 1j * np.sin(angle))
+        terms.append(FactorizedProjectorTerm(beta, phases, coupling))
+    return tuple(terms)
+
+
+def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-6,
+            progress=None) -> SCFResult:
+    """Converge the Kohn-Sham density to ``system.conv_thr`` (Ry) on the GPU."""
+    if precision not in ("f64", "mixed"):
+        raise ValueError("precision must be 'f64' or 'mixed'")
+    device = require_cuda()
+    started = time.perf_counter()
+    timings: dict[str, float] = {}
+
+    def tick(name, t0):
+        timings[name] = timings.get(name, 0.0) + time.perf_counter() - t0
+
+    t0 = time.perf_counter()
+    reciprocal = system.reciprocal
+    volume = system.volume
+    nelec = system.nelec
+    occupied = int(round(nelec / 2.0))
+    bases = make_bases(reciprocal, system.kpoints, system.ecutwfc)
+    if min(len(b) for b in bases) < system.nbnd:
+        raise ValueError("nbnd exceeds the smallest plane-wave basis")
+    shape = fft_shape(bases, reciprocal, system.ecutrho, fft_factors(system.operations))
+    grid = ChargeGrid(shape, reciprocal, system.ecutrho)
+    tables = {label: SpeciesTables(p, volume) for label, p in system.pseudos.items()}
+    q = np.sqrt(grid.g2)
+    v_ion_g = np.zeros(len(grid.g2), dtype=np.complex128)
+    for label, table in tables.items():
+        pos = np.array([p for p, l in zip(system.positions, system.labels) if l == label])
+        structure = np.exp(-1j * (grid.vectors @ pos.T)).sum(axis=1)
+        v_ion_g += table.vloc(q) * structure
+    v_ion = np.ascontiguousarray(grid.to_r(v_ion_g))
+    v_ion_average = float(np.real(np.sum(v_ion_g[grid.g2 < 1.0e-14])))
+    charges = np.array([system.pseudos[l].z_valence for l in system.labels])
+    e_ion = ewald_energy(system.lattice, system.positions, charges, system.ecutrho)
+    # uniform starting density (no PP_RHOATOM): rho(G=0) = nelec / Omega
+    rho = np.full(shape, nelec / volume)
+    symmetrizer = DensitySymmetrizer(system.operations, shape) if len(system.operations) > 1 else None
+    mixer = (LinearMixer(system.mixing_beta) if system.mixing_mode == "linear"
+             else BroydenMixer(grid, system.mixing_beta, system.mixing_ndim, system.ecutrho))
+    states = [KPointState(b, shape, device) for b in bases]
+    rng = QERandom()
+    davidson_tolerance = 0.5 * 1.0e-2  # diago_thr_init 1e-2 Ry -> Ha
+    previous_accuracy = np.inf
+    first_diagonalization = True
+    input_hxc = None
+    energies, accuracies, precision_log, david_its = [], [], [], []
+    energy_terms: dict[str, float] = {}
+    total = 0.0
+    converged = False
+    current_precision = "f32" if precision == "mixed" else "f64"
+    rho_device = torch.zeros(shape, dtype=torch.float64, device=device)
+    tick("setup", t0)
+    iteration = 1
+    while iteration <= system.maxiter:
+        t0 = time.perf_counter()
+        if input_hxc is None:
+            vh = grid.to_r(hartree(grid.to_g(rho), grid.g2))
+            _eps, vxc = pz81(rho)
+            input_hxc = vh + vxc
+        v_eff = v_ion + input_hxc
+        if iteration > 1 and np.isfinite(previous_accuracy):
+            if iteration == 2:
+                davidson_tolerance = 5.0e-3
+            davidson_tolerance = max(5.0e-14, min(davidson_tolerance,
+                                                  0.1 * previous_accuracy / max(1.0, nelec)))
+        if precision == "mixed" and current_precision == "f32" and np.isfinite(previous_accuracy) \
+                and 2.0 * previous_accuracy < switch_ry:
+            current_precision = "f64"
+        # FP32 eigenvalues stall near 1e-7 relative: never ask more of them
+        tol = davidson_tolerance if current_precision == "f64" else max(davidson_tolerance, 2.0e-6)
+        precision_log.append(current_precision)
+        v_dev = torch.from_numpy(v_eff).to(device)
+        tick("v_of_rho", t0)
+        t0 = time.perf_counter()
+        eigenvalues = []
+        its = []
+        for state, weight in zip(states, system.weights):
+            ws = state.workspace(current_precision)
+            if state.terms is None:
+                state.terms = projector_terms(system, tables, state.basis)
+            ham = PlaneWaveHamiltonian(state.basis, None, state.terms, local_workspace=ws,
+                                       real_potential=v_dev, potential_average=v_ion_average)
+            initial_applied = None
+            initial_eigs = None
+            if state.vectors is None:
+                start_vectors, initial_eigs, initial_applied = random_starting_subspace(
+                    ham, state.basis, rng, system.nbnd)
+            else:
+                start_vectors = state.vectors.to(ham.dtype).T.contiguous().T
+            # first SCF iteration: rotate_wfc Ritz vectors (or the first
+            # pass's eigenvectors when the iteration is repeated); later
+            # iterations restart from the converged eigenvectors
+            # (qepy_pw/pw/scf.py:3503-3556)
+            is_ritz = iteration == 1
+            occ_roots = occupied if iteration > 1 else system.nbnd
+            attempt, total_its = 0, 0.0
+            retry_vectors, retry_eigs, retry_applied = start_vectors, initial_eigs, initial_applied
+            while True:
+                sol = davidson(ham.apply, ham.diagonal, system.nbnd, initial_vectors=retry_vectors,
+                               tolerance=tol, max_iterations=20,
+                               subspace_multiplier=system.diago_david_ndim, residual_factor=None,
+                               residual_energy_scale=None, occupied_roots=occ_roots,
+                               initial_is_ritz=is_ritz, initial_is_orthonormal=True,
+                               initial_eigenvalues=retry_eigs, initial_applied=retry_applied,
+                               operator_into=ham.apply_into, dtype=ham.dtype)
+                attempt += 1
+                total_its += sol.iterations
+                if sol.converged or sol.number_unconverged <= 5 or attempt >= 6:
+                    break
+                retry_vectors, retry_eigs, retry_applied = sol.eigenvectors, sol.eigenvalues, None
+            its.append(total_its)
+            state.vectors = sol.eigenvectors.to(torch.complex128).T.contiguous().T
+            state.eigenvalues = np.asarray(sol.eigenvalues)
+            eigenvalues.append(state.eigenvalues)
+        david_its.append(float(np.mean(its)))
+        torch.cuda.synchronize()
+        tick("c_bands", t0)
+        t0 = time.perf_counter()
+        # density from the occupied states (FP64 accumulation on the GPU)
+        rho_device.zero_()
+        for state, weight in zip(states, system.weights):
+            ws = state.workspace("f64")
+            w = torch.full((occupied,), float(weight) * 2.0 / volume, dtype=torch.float64, device=device)
+            ws.accumulate_density(rho_device, state.vectors[:, :occupied], w)
+        rho_out = rho_device.cpu().numpy()
+        rho_out *= nelec * grid.size / (float(np.sum(rho_out)) * volume)
+        if symmetrizer is not None:
+            rho_out = symmetrizer.apply(rho_out)
+            rho_out *= nelec * grid.size / (float(np.sum(rho_out)) * volume)
+        band_energy = sum(w * 2.0 * float(np.sum(e[:occupied])) for w, e in zip(system.weights, eigenvalues))
+        scale = volume / grid.size
+        deband = -scale * float(np.sum(rho_out * input_hxc))
+        residual_g = grid.to_g(rho_out - rho)
+        accuracy = 0.5 * volume * neumaier_metric(residual_g, grid.g2)
+        previous_accuracy = accuracy
+        tick("sum_band", t0)
+        if iteration == 1 and first_diagonalization and accuracy < davidson_tolerance * max(1.0, nelec):
+            davidson_tolerance = max(5.0e-14, 0.1 * accuracy / max(1.0, nelec))
+            first_diagonalization = False
+            continue
+        first_diagonalization = False
+        t0 = time.perf_counter()
+        converged = 2.0 * accuracy < system.conv_thr
+        if converged:
+            rho_energy = rho_out
+        elif isinstance(mixer, BroydenMixer):
+            rho_energy = mixer.mix(rho, residual_g)
+        else:
+            rho_energy = mixer.mix(rho, rho_out)
+        rho_energy_g = grid.to_g(rho_energy)
+        vh_g = hartree(rho_energy_g, grid.g2)
+        e_h = volume * 0.5 * float(np.real(np.vdot(rho_energy_g, vh_g)))
+        eps_xc, vxc = pz81(rho_energy)
+        e_xc = scale * float(np.sum(rho_energy * eps_xc))
+        vh = grid.to_r(vh_g)
+        hxc = vh + vxc
+        descf = -scale * float(np.sum(rho_energy * hxc) - np.sum(rho_out * hxc))
+        input_hxc = hxc
+        energy_terms = {"one_electron": band_energy + deband, "hartree": e_h, "xc": e_xc,
+                        "ewald": e_ion, "descf": descf}
+        total = sum(energy_terms.values())
+        energies.append(total)
+        accuracies.append(accuracy)
+        tick("mix_energy", t0)
+        if progress is not None:
+            progress(iteration, total, accuracy, current_precision)
+        rho = rho_energy
+        if converged:
+            break
+        iteration += 1
+    forces = None
+    if system.forces and converged:
+        from .forces import hellmann_feynman_forces
+
+        t0 = time.perf_counter()
+        forces = hellmann_feynman_forces(system, states, tables, grid, rho, occupied)
+        tick("forces", t0)
+    return SCFResult(converged, total, iteration, energies, accuracies,
+                     [s.eigenvalues for s in states], energy_terms, rho, forces,
+                     time.perf_counter() - started, precision_log, david_its, timings)

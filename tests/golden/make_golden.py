@@ -202,6 +202,36 @@ def scf(name: str, workdir: Path, filename: str) -> None:
           f"{record['iterations']} iterations")
 
 
+def setup_tables(workdir: Path) -> None:
+    """Reference V_loc(q), projector columns, Ewald energies/forces and PZ81
+    values for the synthetic pseudopotential (setup_tables.npz)."""
+    from qepy_pw.ewald import ewald_energy, ewald_forces
+    from qepy_pw.upf import read_upf
+    from qepy_pw.xc import pz81_unpolarized
+
+    from qe_python_b200.configs import DIAMOND_CUBIC, displacements
+    from qe_python_b200.pseudo import write_synthetic_upf
+
+    write_synthetic_upf(workdir / "X.upf")
+    pseudo = read_upf(workdir / "X.upf")
+    volume = 270.0
+    q = np.linspace(0.0, 13.0, 1500)
+    rng = np.random.default_rng(11)
+    kg = rng.normal(size=(400, 3)) * 3.0
+    beta, coupling = pseudo.projector_basis(kg, volume)
+    rho = 10.0 ** rng.uniform(-12.0, 1.0, 4000)
+    eps, vxc = pz81_unpolarized(rho)
+    a = 10.26
+    lattice = np.eye(3) * a
+    positions = DIAMOND_CUBIC * a + displacements(8, 0.05)
+    charges = np.full(8, 4.0)
+    np.savez_compressed(
+        HERE / "setup_tables.npz", volume=volume, q=q, vloc=pseudo.fourier(q, volume), kg=kg,
+        beta=beta, coupling=coupling, rho=rho, eps=eps, vxc=vxc, lattice=lattice,
+        positions=positions, ewald_energy=ewald_energy(lattice, positions, charges, 100.0),
+        ewald_forces=ewald_forces(lattice, positions, charges, 100.0))
+
+
 def si_regression() -> None:
     path = REFERENCE_ROOT / "tests/qe_reference/reference/pw_scf/scf.in.out"
     text = path.read_text()
@@ -225,6 +255,7 @@ def main() -> None:
         workdir = Path(tmp)
         index_maps(workdir)
         hamiltonian_and_davidson()
+        setup_tables(workdir)
         si_regression()
         if not args.skip_scf:
             scf("scf-fcc2", workdir, "scf_fcc2.json")

@@ -1,0 +1,34 @@
+"""GPU SCF against the reference's own SCF results (golden fixtures).
+
+tests/golden/scf_fcc2.json is the reference qepy-pw SCF of the 2-atom fcc
+cell (synthetic pseudopotential, 10 k points, linear mixing 0.7, conv_thr
+1e-8 Ry), generated by tests/golden/make_golden.py.  Bars: plain FP64 total
+energy within 1e-8 Ry and eigenvalues within 1e-7 Ry; the mixed form
+(FP32/split-TF32 then FP64 polish) total energy within 1e-8 Ry and
+eigenvalues within 1e-6 Ry.
+"""
+
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.mark.parametrize("precision,e_tol,eig_tol", [("f64", 1e-8, 1e-7), ("mixed", 1e-8, 1e-6)])
+def test_scf_fcc2_matches_reference(cuda_device, precision, e_tol, eig_tol):
+    from qe_python_b200.scf import benchmark_system, run_scf
+
+    ref = json.loads((GOLDEN / "scf_fcc2.json").read_text())
+    system = benchmark_system("scf-fcc2")
+    result = run_scf(system, precision=precision)
+    assert result.converged
+    assert abs(result.total_energy_ry - ref["total_energy_ry"]) < e_tol
+    for mine, theirs in zip(result.eigenvalues_ha, ref["eigenvalues_ry"]):
+        np.testing.assert_allclose(2.0 * np.asarray(mine), theirs, atol=eig_tol)
