@@ -267,12 +267,29 @@ def lowest_generalized_eigh(h: torch.Tensor, s: torch.Tensor, roots: int):
     s = s.to(torch.complex128)
     lower, info = torch.linalg.cholesky_ex(s)
     if int(info) != 0:
-        raise np.linalg.LinAlgError("overlap matrix is not positive definite")
+        # A subspace built from FP32 vectors can make S numerically
+        # indefinite; solve in the well-conditioned part of its range
+        # (canonical orthogonalisation) instead of failing.
+        return _canonical_generalized_eigh(h, s, roots)
     left = torch.linalg.solve_triangular(lower, h, upper=False)
     reduced = torch.linalg.solve_triangular(lower, left.conj().T, upper=False).conj().T
     values, vectors = torch.linalg.eigh(_hermitize(reduced))
     vectors = torch.linalg.solve_triangular(lower.conj().T, vectors, upper=True)
     return values[:roots], vectors[:, :roots]
+
+
+def _canonical_generalized_eigh(h: torch.Tensor, s: torch.Tensor, roots: int,
+                                threshold: float = 1.0e-10):
+    """H x = e S x restricted to eigenvectors of S above threshold * max(s):
+    X = U s^-1/2, eigh(X^H H X) = Z, x = X Z."""
+    values, vectors = torch.linalg.eigh(_hermitize(s))
+    keep = values > threshold * values.max()
+    if int(keep.sum()) < roots:
+        raise np.linalg.LinAlgError("overlap matrix has fewer independent directions than roots")
+    x = vectors[:, keep] / torch.sqrt(values[keep])[None, :]
+    reduced = _hermitize(x.conj().T @ h @ x)
+    e, z = torch.linalg.eigh(reduced)
+    return e[:roots], (x @ z)[:, :roots]
 
 
 def _orthonormalize(block: torch.Tensor, threshold: float = 1.0e-12) -> torch.Tensor:

@@ -198,9 +198,20 @@ class SpeciesTables:
         return beta, coupling
 
 
+def structure_factor(vectors: np.ndarray, positions: np.ndarray, weights: np.ndarray) -> np.ndarray:
+    """S(G) = sum_a w_a exp(-i G.tau_a), chunked over atoms (host)."""
+    out = np.zeros(len(vectors), dtype=np.complex128)
+    for a0 in range(0, len(positions), 16):
+        out += np.exp(-1j * (vectors @ positions[a0:a0 + 16].T)) @ weights[a0:a0 + 16]
+    return out
+
+
 def ewald_energy(lattice: np.ndarray, positions: np.ndarray, charges: np.ndarray,
-                 ecutrho_ry: float) -> float:
-    """Ion-ion Ewald energy in Hartree (qepy_pw/ewald.py:49-143)."""
+                 ecutrho_ry: float, structure=structure_factor) -> float:
+    """Ion-ion Ewald energy in Hartree (qepy_pw/ewald.py:49-143).
+
+    ``structure(vectors, positions, charges)`` evaluates the structure factor
+    (host by default; the SCF passes a GPU evaluation for large cells)."""
     lattice = np.asarray(lattice, dtype=float)
     positions = np.asarray(positions, dtype=float)
     charges = np.asarray(charges, dtype=float)
@@ -221,17 +232,19 @@ def ewald_energy(lattice: np.ndarray, positions: np.ndarray, charges: np.ndarray
     axis = np.arange(-nmax, nmax + 1)
     recip_sum = -total**2 / (4.0 * alpha)
     acc = 0.0
+    yz = np.stack(np.meshgrid(axis, axis, indexing="ij"), -1).reshape(-1, 2)
+    gs, g2s = [], []
     for i in axis:
-        yz = np.stack(np.meshgrid(axis, axis, indexing="ij"), -1).reshape(-1, 2)
         miller = np.column_stack((np.full(len(yz), i), yz))
         g = miller @ reciprocal
         g2 = np.einsum("ij,ij->i", g, g)
         keep = (g2 <= ecutrho_ry) & (g2 > 1.0e-14)
-        g, g2 = g[keep], g2[keep]
-        if not g2.size:
-            continue
-        structure = np.exp(-1j * (positions @ g.T)).T @ charges
-        acc += float(np.sum(np.abs(structure) ** 2 * np.exp(-g2 / (4.0 * alpha)) / g2))
+        gs.append(g[keep])
+        g2s.append(g2[keep])
+    g, g2 = np.concatenate(gs), np.concatenate(g2s)
+    if g2.size:
+        s = structure(g, positions, charges)
+        acc = float(np.sum(np.abs(s) ** 2 * np.exp(-g2 / (4.0 * alpha)) / g2))
     recip_sum = (recip_sum + acc) * 4.0 * np.pi / volume
     recip_sum -= float(np.sum(charges**2) * 2.0 * np.sqrt(alpha / np.pi))
     # real-space sum within 4/sqrt(alpha)

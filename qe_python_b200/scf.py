@@ -307,6 +307,20 @@ class KPointState:
         return self.workspaces[precision]
 
 
+def gpu_structure_factor(vectors: np.ndarray, positions: np.ndarray,
+                         weights: np.ndarray) -> np.ndarray:
+    """S(G) = sum_a w_a exp(-i G.tau_a) in FP64 on the device (set-up of large
+    cells: one complex exponential per G vector and atom)."""
+    device = torch.device("cuda", torch.cuda.current_device())
+    g = torch.from_numpy(np.ascontiguousarray(vectors)).to(device)
+    pos = torch.from_numpy(np.ascontiguousarray(positions)).to(device)
+    w = torch.from_numpy(np.asarray(weights, dtype=np.float64)).to(device).to(torch.complex128)
+    out = torch.zeros(len(vectors), dtype=torch.complex128, device=device)
+    for a0 in range(0, len(positions), 32):
+        out += torch.exp(-1j * (g @ pos[a0:a0 + 32].T)) @ w[a0:a0 + 32]
+    return out.cpu().numpy()
+
+
 def _as128(t: torch.Tensor) -> torch.Tensor:
     return t if t.dtype == torch.complex128 else t.to(torch.complex128).T.contiguous().T
 
@@ -350,7 +364,7 @@ def projector_terms(system: System, tables: dict, basis) -> tuple:
     return tuple(terms)
 
 
-def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-6,
+def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             progress=None) -> SCFResult:
     """Converge the Kohn-Sham density to ``system.conv_thr`` (Ry) on the GPU."""
     if precision not in ("f64", "mixed"):
@@ -377,12 +391,13 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-6,
     v_ion_g = np.zeros(len(grid.g2), dtype=np.complex128)
     for label, table in tables.items():
         pos = np.array([p for p, l in zip(system.positions, system.labels) if l == label])
-        structure = np.exp(-1j * (grid.vectors @ pos.T)).sum(axis=1)
+        structure = gpu_structure_factor(grid.vectors, pos, np.ones(len(pos)))
         v_ion_g += table.vloc(q) * structure
     v_ion = np.ascontiguousarray(grid.to_r(v_ion_g))
     v_ion_average = float(np.real(np.sum(v_ion_g[grid.g2 < 1.0e-14])))
     charges = np.array([system.pseudos[l].z_valence for l in system.labels])
-    e_ion = ewald_energy(system.lattice, system.positions, charges, system.ecutrho)
+    e_ion = ewald_energy(system.lattice, system.positions, charges, system.ecutrho,
+                         structure=gpu_structure_factor)
     # uniform starting density (no PP_RHOATOM): rho(G=0) = nelec / Omega
     rho = np.full(shape, nelec / volume)
     symmetrizer = DensitySymmetrizer(system.operations, shape) if len(system.operations) > 1 else None
