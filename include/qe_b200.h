@@ -138,6 +138,16 @@ int qeb_zgemm_static_scratch(int M, int N, int K, const double* alpha, const voi
                              int64_t lda, const void* B, int64_t ldb, const double* beta,
                              void* C, int64_t ldc, void* stream);
 
+/* out = D becp for a block-diagonal D (P x P): block k covers rows/columns
+ * [start[k], start[k] + size[k]) with its size x size entries row-major at
+ * values + offset[k]; row_block[p] is the block of row p.  All arrays are
+ * device arrays; becp/out are column-major (P, nb).  Replaces the dense
+ * coupling @ overlaps product (qepy_pw/diagonalization.py:348). */
+int qeb_block_coupling(int precision, int P, int nb, int nblocks, const int32_t* row_block,
+                       const int32_t* start, const int32_t* size, const int64_t* offset,
+                       const void* values, const void* becp, int64_t ldb, void* out,
+                       int64_t ldo, void* stream);
+
 /* ------------------------------------------------------------------------
  * Split-TF32 complex GEMM on tcgen05 tensor cores (the chosen form of the
  * projector and subspace contractions; replaces the same ZGEMM calls as
@@ -173,6 +183,24 @@ int qeb_tf32_gemm(int M, int N, int kp, const void* a_hi, const void* a_lo, int6
                   int64_t ldb, const double* alpha, const double* beta, void* C, int64_t ldc,
                   void* scratch, int64_t scratch_bytes, void* stream);
 int qeb_tf32_gemm_error(int* out);
+
+/* ------------------------------------------------------------------------
+ * Split-TF32 complex GEMM on unpacked complex64 operands (the chosen form of
+ * projector_overlaps / add_projector_product, _native_fft.pyx:694-731 and
+ * :782-836, and of the Davidson subspace GEMMs, diagonalization.py:658-726).
+ *   C = alpha op(A) B + beta C,  op = QEB_OP_C (A^H, A is K x M) or QEB_OP_N
+ * A, B, C column-major complex64.  hi/lo splitting happens in shared memory
+ * inside the kernel; no packed copies.  A and B must be 16-byte aligned with
+ * even leading dimensions, else QEB_STATUS_EUNSUPPORTED (the caller then uses
+ * the packed path).  K = 0 is QEB_STATUS_EUNSUPPORTED (scale C instead).
+ * scratch: qeb_cgemm_tf32x3_scratch_bytes() for a split K range (less or
+ * none lowers the split).  Bounded waits report through
+ * qeb_tf32_gemm_error().
+ * ---------------------------------------------------------------------- */
+int64_t qeb_cgemm_tf32x3_scratch_bytes(int op_a, int M, int N, int K);
+int qeb_cgemm_tf32x3(int op_a, int M, int N, int K, const double* alpha, const void* A,
+                     int64_t lda, const void* B, int64_t ldb, const double* beta, void* C,
+                     int64_t ldc, void* scratch, int64_t scratch_bytes, void* stream);
 
 /* ------------------------------------------------------------------------
  * Davidson column kernels (precision QEB_F64 / QEB_F32 selects the vector

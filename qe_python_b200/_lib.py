@@ -46,11 +46,14 @@ SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_cgemm", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
     ("qeb_zgemm_static_scratch_capacity", _L, []),
     ("qeb_zgemm_static_scratch", _I, [_I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P]),
+    ("qeb_block_coupling", _I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _L, _P, _L, _P]),
     ("qeb_tf32_pack", _I, [_I, _I, _I, _I, _I, _P, _L, _P, _P, _L, _P]),
     ("qeb_tf32_gemm_scratch_bytes", _L, [_I, _I, _I]),
     ("qeb_tf32_gemm", _I, [_I, _I, _I, _P, _P, _L, _P, _P, _P, _P, _L, _P, _P, _P, _L, _P, _L,
                            _P]),
     ("qeb_tf32_gemm_error", _I, [_P]),
+    ("qeb_cgemm_tf32x3_scratch_bytes", _L, [_I, _I, _I, _I]),
+    ("qeb_cgemm_tf32x3", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
     ("qeb_column_squared_norms", _I, [_I, _L, _L, _P, _L, _P, _P]),
     ("qeb_column_diagonal_expectations", _I, [_I, _L, _L, _P, _L, _P, _P, _P]),
     ("qeb_column_inner_products", _I, [_I, _L, _L, _P, _L, _P, _L, _P, _P]),

@@ -28,10 +28,19 @@ class BandProblem:
     """Fixed cell, bases and tables; positions and V_Hxc vary."""
 
     def __init__(self, system, precision: str = "f64", tolerance: float = 1.0e-11) -> None:
+        """precision: 'f64' (plain), or 'mixed' (chosen form: an FP32/split-TF32
+        Davidson to 1e-6 Ha, then FP64 Davidson iterations from its vectors).
+
+        Hellmann-Feynman gradients are first order in the eigenvector error,
+        while the Davidson stopping rule on eigenvalue changes only bounds a
+        second-order quantity, so the final solve also requires residual norms
+        below ``tolerance``."""
         from .basis import fft_shape, make_bases
         from .pseudo_tables import SpeciesTables
         from .symmetry import fft_factors
 
+        if precision not in ("f64", "mixed"):
+            raise ValueError("precision must be 'f64' or 'mixed'")
         self.system = system
         self.precision = precision
         self.tolerance = tolerance
@@ -64,15 +73,26 @@ class BandProblem:
         for basis, weight in zip(self.bases, system.weights):
             state = KPointState(basis, self.shape, self.device)
             state.terms = projector_terms(system, self.tables, state.basis)
-            ws = state.workspace(self.precision)
-            ham = PlaneWaveHamiltonian(state.basis, None, state.terms, local_workspace=ws,
-                                       real_potential=v_dev, potential_average=v0)
-            start, eigs, applied = random_starting_subspace(ham, state.basis, rng, system.nbnd)
-            sol = davidson(ham.apply, ham.diagonal, system.nbnd, initial_vectors=start,
-                           tolerance=self.tolerance, max_iterations=200, subspace_multiplier=4,
-                           residual_factor=None, initial_is_ritz=True, initial_is_orthonormal=True,
-                           initial_eigenvalues=eigs, initial_applied=applied,
-                           operator_into=ham.apply_into, dtype=ham.dtype)
+            stages = [("f64", self.tolerance)] if self.precision == "f64" else \
+                [("f32", max(self.tolerance, 1.0e-6)), ("f64", self.tolerance)]
+            sol = None
+            for stage, (precision, tolerance) in enumerate(stages):
+                ws = state.workspace(precision)
+                ham = PlaneWaveHamiltonian(state.basis, None, state.terms, local_workspace=ws,
+                                           real_potential=v_dev, potential_average=v0)
+                final = stage == len(stages) - 1
+                if sol is None:
+                    start, eigs, applied = random_starting_subspace(ham, state.basis, rng,
+                                                                    system.nbnd)
+                else:
+                    start, eigs, applied = sol.eigenvectors.to(ham.dtype), None, None
+                sol = davidson(ham.apply, ham.diagonal, system.nbnd, initial_vectors=start,
+                               tolerance=tolerance, max_iterations=300, subspace_multiplier=4,
+                               residual_factor=1.0 if final else None,
+                               initial_is_ritz=eigs is not None,
+                               initial_is_orthonormal=eigs is not None, initial_eigenvalues=eigs,
+                               initial_applied=applied, operator_into=ham.apply_into,
+                               dtype=ham.dtype)
             state.vectors = sol.eigenvectors.to(torch.complex128).T.contiguous().T
             state.eigenvalues = np.asarray(sol.eigenvalues)
             energy += float(weight) * 2.0 * float(np.sum(state.eigenvalues[:self.occupied]))

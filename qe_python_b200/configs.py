@@ -2,13 +2,17 @@
 
   scf-fcc2      2-atom diamond-structure fcc, a = 10.26 bohr, ecutwfc 20 / ecutrho
                 80 Ry, 4x4x4 shifted Monkhorst-Pack mesh, 8 bands, linear mixing 0.7
+  scf-fcc2-smear the same cell with Broyden mixing and Marzari-Vanderbilt
+                smearing (degauss 0.02 Ry): the small pin of broadened filling
   scf-dia64     2x2x2 supercell of the 8-atom cubic diamond cell (a = 20.52),
-                ecutwfc 30 / ecutrho 180 Ry, unshifted 2x2x2 mesh (4 k), 160 bands
+                ecutwfc 30 / ecutrho 180 Ry, unshifted 2x2x2 mesh (4 k), 160 bands,
+                Gaussian smearing 0.02 Ry, Thomas-Fermi mixing
   scf-dia8-disp 8-atom cubic diamond (a = 10.26), each atom displaced by a seeded
                 uniform vector of length <= 0.05 bohr, ecutwfc 25 Ry, 3x3x3 mesh,
                 24 bands, forces
   scf-dia216    3x3x3 supercell (a = 30.78), seeded 0.03-bohr displacements,
-                ecutwfc 30 / ecutrho 180 Ry, Gamma only, 480 bands, forces
+                ecutwfc 30 / ecutrho 180 Ry, Gamma only, 480 bands, forces,
+                Gaussian smearing 0.02 Ry, Thomas-Fermi mixing
 All converge to conv_thr = 1e-8 Ry.  The text is readable by the reference's
 read_pw_input (qepy_pw/pw/input.py:1063).
 """
@@ -38,6 +42,20 @@ def displacements(count: int, maximum: float, seed: int = SEED) -> np.ndarray:
     return direction * rng.uniform(0.0, maximum, count)[:, None]
 
 
+# The synthetic pseudopotential makes the diamond lattice a semimetal (the
+# highest occupied band of the displaced 8-atom cell reaches 1.90 eV, the
+# lowest empty one starts at 1.24 eV).  A supercell folds those k-points onto
+# one another, and fixed filling of the lowest bands then swaps states at the
+# Fermi level between iterations and never converges (the 216-atom Gamma cell
+# was measured oscillating for 100 iterations).  The supercells therefore use
+# Gaussian broadening, which the reference supports (qepy_pw/pw/scf.py:2146),
+# and Thomas-Fermi-preconditioned Broyden mixing (mixing_mode 'TF',
+# qepy_pw/mixing.py:51-59, 398-399) against long-wavelength charge sloshing,
+# which plain Broyden from a uniform start does not damp in these cells.
+SUPERCELL_SMEARING = {"occupations": "smearing", "smearing": "gaussian", "degauss": 0.02}
+SUPERCELL_MIXING = {"mixing_mode": "TF"}
+
+
 def _positions_block(unit: str, labels, positions) -> str:
     rows = "\n".join(f"  {lab} {p[0]:.12f} {p[1]:.12f} {p[2]:.12f}" for lab, p in zip(labels, positions))
     return f"ATOMIC_POSITIONS ({unit})\n{rows}\n"
@@ -61,7 +79,13 @@ def _value(v):
 def config_input(name: str, pseudo_dir: str, pseudo_file: str = "X.upf") -> str:
     control = {"calculation": "scf", "pseudo_dir": pseudo_dir, "disk_io": "none"}
     electrons = {"conv_thr": 1.0e-8, "diagonalization": "david"}
-    if name == "scf-fcc2":
+    if name == "scf-fcc2-smear":
+        system = {"ibrav": 2, "celldm(1)": 10.26, "nat": 2, "ntyp": 1, "ecutwfc": 20.0,
+                  "ecutrho": 80.0, "nbnd": 8, "occupations": "smearing",
+                  "smearing": "marzari-vanderbilt", "degauss": 0.02}
+        positions = _positions_block("alat", ["X", "X"], [[0, 0, 0], [0.25, 0.25, 0.25]])
+        kpoints = "K_POINTS automatic\n 4 4 4 1 1 1\n"
+    elif name == "scf-fcc2":
         system = {"ibrav": 2, "celldm(1)": 10.26, "nat": 2, "ntyp": 1, "ecutwfc": 20.0,
                   "ecutrho": 80.0, "nbnd": 8}
         # linear mixing is set programmatically (ELECTRON_OVERRIDES): the
@@ -75,7 +99,8 @@ def config_input(name: str, pseudo_dir: str, pseudo_file: str = "X.upf") -> str:
         # points Gamma, X, M, R (weights 1:3:3:1) whose plane-wave counts
         # differ slightly; the shifted mesh would collapse to one point.
         system = {"ibrav": 1, "celldm(1)": 20.52, "nat": len(frac), "ntyp": 1, "ecutwfc": 30.0,
-                  "ecutrho": 180.0, "nbnd": 160}
+                  "ecutrho": 180.0, "nbnd": 160, **SUPERCELL_SMEARING}
+        electrons.update(SUPERCELL_MIXING)
         positions = _positions_block("crystal", ["X"] * len(frac), frac)
         kpoints = "K_POINTS automatic\n 2 2 2 0 0 0\n"
     elif name == "scf-dia8-disp":
@@ -90,7 +115,8 @@ def config_input(name: str, pseudo_dir: str, pseudo_file: str = "X.upf") -> str:
         frac = supercell(DIAMOND_CUBIC, 3)
         cart = frac * a + displacements(len(frac), 0.03)
         system = {"ibrav": 1, "celldm(1)": a, "nat": len(frac), "ntyp": 1, "ecutwfc": 30.0,
-                  "ecutrho": 180.0, "nbnd": 480}
+                  "ecutrho": 180.0, "nbnd": 480, **SUPERCELL_SMEARING}
+        electrons.update(SUPERCELL_MIXING)
         control["tprnfor"] = True
         positions = _positions_block("bohr", ["X"] * len(frac), cart)
         kpoints = "K_POINTS gamma\n"
@@ -103,7 +129,7 @@ def config_input(name: str, pseudo_dir: str, pseudo_file: str = "X.upf") -> str:
     return text
 
 
-CONFIGS = ("scf-fcc2", "scf-dia64", "scf-dia8-disp", "scf-dia216")
+CONFIGS = ("scf-fcc2", "scf-fcc2-smear", "scf-dia64", "scf-dia8-disp", "scf-dia216")
 
 # ELECTRONS entries applied after parsing (qepy_pw/pw/scf.py:3042 'linear').
 ELECTRON_OVERRIDES = {"scf-fcc2": {"mixing_mode": "linear"}}

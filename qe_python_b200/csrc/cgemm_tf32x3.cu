@@ -1,0 +1,439 @@
+// Split-TF32 complex GEMM that reads complex64 operands directly.
+//
+//   C = alpha * op(A) B + beta * C,  op(A) = A^H (QEB_OP_C) or A (QEB_OP_N)
+//
+// A, B and C are column-major complex64 matrices.  Unlike qeb_tf32_gemm,
+// nothing is packed beforehand: each pipeline stage TMA-loads the raw FP32
+// words of one 128-row by 16-complex slab of A and of B into shared memory,
+// and four converter warps split every value x into hi = tf32(x) and
+// lo = tf32(x - hi) in place, in the 128-byte-swizzled K-major layout that
+// tcgen05.mma reads.  The complex product is carried by real products over
+// (re, im) pairs interleaved along K:
+//   OP_C  Re(conj(a) b) = [a_re, a_im].[b_re, b_im]
+//         Im(conj(a) b) = [a_re, a_im].[b_im, -b_re]       (B1 = swap-negated B)
+//   OP_N  Re(a b)       = [a_re, -a_im].[b_re, b_im]      (A0, A transposed by
+//         Im(a b)       = [a_im, a_re].[b_re, b_im]        the converters)
+// and each real product is hi*hi + hi*lo + lo*hi, three tcgen05.mma.kind::tf32
+// accumulating in FP32 in tensor memory (Re in columns [0, 128), Im in
+// [128, 256)).
+//
+// One CTA = 192 threads computes a 128 x 128 output tile over a K range:
+//   warp 0 lane 0 : TMA producer, two stages
+//   warp 1 lane 0 : MMA issuer; warp 1 owns the tensor-memory allocation
+//   warps 2-5     : converters, then the epilogue (tcgen05.ld, complex store)
+// K is split across CTAs (grid.z) into caller scratch when the output has
+// few tiles; a second kernel sums the slices in a fixed order.  Every wait
+// is bounded; on timeout the CTA records an error code in the device word
+// read by qeb_tf32_gemm_error and unwinds.
+//
+// Requirements (else QEB_STATUS_EUNSUPPORTED, and the caller uses the packed
+// path): A and B 16-byte aligned with even leading dimensions (TMA rows must
+// start on 16-byte boundaries).
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include "qeb_common.cuh"
+#include "tcgen05.cuh"
+#include "../../include/qe_b200.h"
+
+namespace {
+
+using namespace qeb::tc;
+
+constexpr int BM = 128, BN = 128;
+constexpr int BKF = 32;      // FP32 words along K per stage (16 complex values)
+constexpr int TILE = 16384;  // bytes of one 128-row x 32-word tile
+constexpr int STAGES = 2;
+constexpr int THREADS = 192;
+constexpr int TMEM_COLS = 2 * BN;
+constexpr uint32_t kIdesc = idesc_tf32(BM, BN);
+
+// Tile slots of one stage.  OP_C: 0 A (raw, then hi), 1 A lo, 2 B (raw, then
+// hi), 3 B lo, 4 B1 hi, 5 B1 lo.  OP_N: 0 A raw (16 x 256 words, row-major,
+// unswizzled), 1 B (raw, then hi), 2 B lo, 3 A0 hi, 4 A0 lo, 5 A1 hi, 6 A1 lo.
+template <int OP>
+struct Slots {
+  static constexpr bool kC = OP == QEB_OP_C;
+  static constexpr int tiles = kC ? 6 : 7;
+  static constexpr int stage_bytes = tiles * TILE;
+  static constexpr int raw_a = 0, raw_b = kC ? 2 : 1;
+  static constexpr int a_re_hi = kC ? 0 : 3, a_re_lo = kC ? 1 : 4;
+  static constexpr int a_im_hi = kC ? 0 : 5, a_im_lo = kC ? 1 : 6;
+  static constexpr int b_re_hi = kC ? 2 : 1, b_re_lo = kC ? 3 : 2;
+  static constexpr int b_im_hi = kC ? 4 : 1, b_im_lo = kC ? 5 : 2;
+};
+
+template <int OP>
+constexpr size_t smem_bytes() {
+  return (size_t)STAGES * Slots<OP>::stage_bytes + 1024 /*alignment*/ + 256 /*barriers*/;
+}
+
+struct Maps {
+  CUtensorMap a, b;
+};
+
+__device__ __forceinline__ float4 hi4(float4 v) {
+  return make_float4(tf32_round(v.x), tf32_round(v.y), tf32_round(v.z), tf32_round(v.w));
+}
+__device__ __forceinline__ float4 lo4(float4 v, float4 h) {
+  return make_float4(tf32_round(v.x - h.x), tf32_round(v.y - h.y), tf32_round(v.z - h.z),
+                     tf32_round(v.w - h.w));
+}
+
+// Split one K-major tile in place (hi) with its lo part into another slot.
+// The split is elementwise, so the 128-byte swizzle needs no attention.
+__device__ __forceinline__ void split_tile(unsigned char* tile, unsigned char* lo, int ct,
+                                           unsigned char* swap_hi, unsigned char* swap_lo) {
+  float4* t = reinterpret_cast<float4*>(tile);
+  float4* l = reinterpret_cast<float4*>(lo);
+#pragma unroll 4
+  for (int c = ct; c < TILE / 16; c += 128) {
+    const float4 v = t[c];
+    const float4 h = hi4(v), w = lo4(v, h);
+    t[c] = h;
+    l[c] = w;
+    if (swap_hi != nullptr) {  // (re, im) -> (im, -re)
+      reinterpret_cast<float4*>(swap_hi)[c] = make_float4(h.y, -h.x, h.w, -h.z);
+      reinterpret_cast<float4*>(swap_lo)[c] = make_float4(w.y, -w.x, w.w, -w.z);
+    }
+  }
+}
+
+// OP_N: transpose the raw M-major slab of A (16 K rows x 128 complex) into
+// the K-major swizzled tiles A0 = [re, -im] and A1 = [im, re], hi and lo.
+__device__ __forceinline__ void transpose_a(const unsigned char* raw, unsigned char* a0h,
+                                            unsigned char* a0l, unsigned char* a1h,
+                                            unsigned char* a1l, int ct) {
+  const float2* x = reinterpret_cast<const float2*>(raw);
+#pragma unroll 2
+  for (int it = ct; it < BM * 8; it += 128) {
+    const int m = it & (BM - 1), kp = it >> 7;  // kp: pair of K values 2kp, 2kp+1
+    const float2 x0 = x[(2 * kp) * BM + m];
+    const float2 x1 = x[(2 * kp + 1) * BM + m];
+    const float4 r0 = make_float4(x0.x, -x0.y, x1.x, -x1.y);
+    const float4 r1 = make_float4(x0.y, x0.x, x1.y, x1.x);
+    const float4 h0 = hi4(r0), h1 = hi4(r1);
+    const int off = m * 128 + ((kp ^ (m & 7)) << 4);
+    *reinterpret_cast<float4*>(a0h + off) = h0;
+    *reinterpret_cast<float4*>(a0l + off) = lo4(r0, h0);
+    *reinterpret_cast<float4*>(a1h + off) = h1;
+    *reinterpret_cast<float4*>(a1l + off) = lo4(r1, h1);
+  }
+}
+
+template <int OP>
+__global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
+    const __grid_constant__ Maps maps, int M, int N, int kb_per_split, int kb_total, float2 alpha,
+    float2 beta, float2* C, int64_t ldc, float2* split, int* error) {
+  using S = Slots<OP>;
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>(
+      (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * S::stage_bytes);
+  uint64_t* conv = full + STAGES;
+  uint64_t* empty = conv + STAGES;
+  uint64_t* done = empty + STAGES;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
+  int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
+  volatile int* abort_v = abort_flag;
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int kb0 = blockIdx.z * kb_per_split;
+  const int nk = max(0, min(kb_total, kb0 + kb_per_split) - kb0);
+
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < STAGES; ++s) {
+      mbar_init(&full[s], 1);
+      mbar_init(&conv[s], 4);  // one arrival per converter warp
+      mbar_init(&empty[s], 1);
+    }
+    mbar_init(done, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tmem_slot)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t tmem = *tmem_slot;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int i = 0; i < nk; ++i) {
+        const int s = i % STAGES;
+        if (i >= STAGES && !mbar_wait(&empty[s], ((i / STAGES) - 1) & 1)) {
+          atomicExch(error, 11);
+          *abort_v = 1;
+          break;
+        }
+        if (*abort_v) break;
+        unsigned char* st = base + s * S::stage_bytes;
+        mbar_expect_tx(&full[s], 2 * TILE);
+        const int kb = kb0 + i;
+        if (OP == QEB_OP_C) {
+          tma_load_2d(st + S::raw_a * TILE, &maps.a, &full[s], kb * BKF, m0);
+        } else {
+          tma_load_2d(st + S::raw_a * TILE, &maps.a, &full[s], 2 * m0, kb * (BKF / 2));
+        }
+        tma_load_2d(st + S::raw_b * TILE, &maps.b, &full[s], kb * BKF, n0);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      const uint32_t t_re = tmem, t_im = tmem + BN;
+      for (int i = 0; i < nk; ++i) {
+        const int s = i % STAGES;
+        if (!mbar_wait(&conv[s], (i / STAGES) & 1)) {
+          atomicExch(error, 12);
+          *abort_v = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const uint32_t st = smem_u32(base + s * S::stage_bytes);
+#pragma unroll
+        for (int kk = 0; kk < BKF / 8; ++kk) {
+          const uint32_t off = kk * 32;  // 8 tf32 words along K
+          const uint32_t acc = (i > 0 || kk > 0) ? 1u : 0u;
+          const uint64_t arh = smem_desc_sw128(st + S::a_re_hi * TILE + off);
+          const uint64_t arl = smem_desc_sw128(st + S::a_re_lo * TILE + off);
+          const uint64_t aih = smem_desc_sw128(st + S::a_im_hi * TILE + off);
+          const uint64_t ail = smem_desc_sw128(st + S::a_im_lo * TILE + off);
+          const uint64_t brh = smem_desc_sw128(st + S::b_re_hi * TILE + off);
+          const uint64_t brl = smem_desc_sw128(st + S::b_re_lo * TILE + off);
+          const uint64_t bih = smem_desc_sw128(st + S::b_im_hi * TILE + off);
+          const uint64_t bil = smem_desc_sw128(st + S::b_im_lo * TILE + off);
+          mma_tf32(t_re, arh, brh, kIdesc, acc);
+          mma_tf32(t_re, arh, brl, kIdesc, 1u);
+          mma_tf32(t_re, arl, brh, kIdesc, 1u);
+          mma_tf32(t_im, aih, bih, kIdesc, acc);
+          mma_tf32(t_im, aih, bil, kIdesc, 1u);
+          mma_tf32(t_im, ail, bih, kIdesc, 1u);
+        }
+        mma_commit(&empty[s]);
+      }
+      mma_commit(done);  // arrives once every MMA issued above has completed
+    }
+  } else {
+    const int ct = threadIdx.x - 64;  // 0..127
+    for (int i = 0; i < nk; ++i) {
+      const int s = i % STAGES;
+      const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], (i / STAGES) & 1));
+      if (!ok || *abort_v) {
+        if (!ok && lane == 0) {
+          atomicExch(error, 13);
+          *abort_v = 1;
+        }
+        break;
+      }
+      unsigned char* st = base + s * S::stage_bytes;
+      if (OP == QEB_OP_C) {
+        split_tile(st + S::raw_a * TILE, st + S::a_re_lo * TILE, ct, nullptr, nullptr);
+        split_tile(st + S::raw_b * TILE, st + S::b_re_lo * TILE, ct, st + S::b_im_hi * TILE,
+                   st + S::b_im_lo * TILE);
+      } else {
+        transpose_a(st + S::raw_a * TILE, st + S::a_re_hi * TILE, st + S::a_re_lo * TILE,
+                    st + S::a_im_hi * TILE, st + S::a_im_lo * TILE, ct);
+        split_tile(st + S::raw_b * TILE, st + S::b_re_lo * TILE, ct, nullptr, nullptr);
+      }
+      fence_proxy_async_smem();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&conv[s]);
+    }
+  }
+  __syncwarp();
+
+  if (warp >= 2) {
+    const bool ok = mbar_wait(done, 0);
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    if (!ok && lane == 0) atomicExch(error, 14);
+    const bool aborted = !__all_sync(0xffffffffu, ok) || *abort_v;
+    const int quarter = warp & 3;  // tcgen05.ld lane window of this warp
+    const int row = m0 + quarter * 32 + lane;
+    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
+    for (int c0 = 0; c0 < BN; c0 += 32) {
+      float re[32], im[32];
+      tmem_ld32(lane_base + c0, re);
+      tmem_ld32(lane_base + BN + c0, im);
+      tmem_wait_ld();
+      if (nk == 0) {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) re[j] = im[j] = 0.0f;
+      }
+      if (aborted || row >= M) continue;
+#pragma unroll
+      for (int j = 0; j < 32; ++j) {
+        const int col = n0 + c0 + j;
+        if (col >= N) break;
+        if (split != nullptr) {
+          split[(int64_t)blockIdx.z * M * N + row + (int64_t)col * M] = make_float2(re[j], im[j]);
+        } else {
+          float2* c = C + row + (int64_t)col * ldc;
+          float2 v = make_float2(alpha.x * re[j] - alpha.y * im[j], alpha.x * im[j] + alpha.y * re[j]);
+          if (beta.x != 0.0f || beta.y != 0.0f) {
+            const float2 o = *c;
+            v.x += beta.x * o.x - beta.y * o.y;
+            v.y += beta.x * o.y + beta.y * o.x;
+          }
+          *c = v;
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncthreads();
+  if (warp == 1) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "r"(TMEM_COLS));
+  }
+}
+
+// C = alpha * sum_k P_k + beta * C over the split slices, in slice order.
+__global__ void reduce_slices(int M, int N, int splits, const float2* __restrict__ P, float2 alpha,
+                              float2 beta, float2* C, int64_t ldc) {
+  const int64_t total = (int64_t)M * N;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    float2 s = make_float2(0.0f, 0.0f);
+    for (int k = 0; k < splits; ++k) {
+      const float2 p = P[(int64_t)k * total + i];
+      s.x += p.x;
+      s.y += p.y;
+    }
+    const int64_t m = i % M, n = i / M;
+    float2* c = C + m + n * ldc;
+    float2 v = make_float2(alpha.x * s.x - alpha.y * s.y, alpha.x * s.y + alpha.y * s.x);
+    if (beta.x != 0.0f || beta.y != 0.0f) {
+      const float2 o = *c;
+      v.x += beta.x * o.x - beta.y * o.y;
+      v.y += beta.x * o.y + beta.y * o.x;
+    }
+    *c = v;
+  }
+}
+
+int encode_map(qeb::EncodeTiled enc, CUtensorMap* map, const void* ptr, uint64_t inner,
+               uint64_t outer, int64_t ld_bytes, uint32_t box_inner, uint32_t box_outer,
+               bool swizzle) {
+  const cuuint64_t dims[2] = {(cuuint64_t)inner, (cuuint64_t)outer};
+  const cuuint64_t strides[1] = {(cuuint64_t)ld_bytes};
+  const cuuint32_t box[2] = {box_inner, box_outer};
+  const cuuint32_t estr[2] = {1, 1};
+  CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(ptr), dims, strides,
+                   box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                   swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                   CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    qeb::set_error("cgemm_tf32x3: cuTensorMapEncodeTiled failed (%d) for %llu x %llu words",
+                   (int)r, (unsigned long long)inner, (unsigned long long)outer);
+    return QEB_ECUDA;
+  }
+  return QEB_OK;
+}
+
+int sm_count() {
+  static int count = 0;
+  if (count == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&count, cudaDevAttrMultiProcessorCount, dev);
+    if (count <= 0) count = 148;
+  }
+  return count;
+}
+
+int choose_splits(int M, int N, int K) {
+  const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
+  const int kblocks = (2 * K + BKF - 1) / BKF;
+  int s = (sm_count() + tiles - 1) / tiles;  // about one wave of CTAs
+  if (s > kblocks / 4) s = kblocks / 4;      // at least four stages per slice
+  if (s > 32) s = 32;
+  return s < 1 ? 1 : s;
+}
+
+template <int OP>
+int launch(const Maps& maps, int M, int N, int K, float2 al, float2 be, float2* C, int64_t ldc,
+           void* scratch, int64_t scratch_bytes, int* err, cudaStream_t s) {
+  cudaError_t e = qeb::raise_smem_limit(cgemm_tf32x3_kernel<OP>, smem_bytes<OP>());
+  if (e != cudaSuccess) return qeb::cuda_status(e, "cgemm_tf32x3 shared-memory limit");
+  const int kblocks = (2 * K + BKF - 1) / BKF;
+  int splits = choose_splits(M, N, K);
+  const int64_t slice = (int64_t)M * N * 8;
+  if (splits > 1 && (scratch == nullptr || scratch_bytes < splits * slice)) {
+    const int64_t fit = scratch == nullptr ? 0 : scratch_bytes / slice;
+    splits = fit > 1 ? (int)(fit < splits ? fit : splits) : 1;
+  }
+  const int per = (kblocks + splits - 1) / splits;
+  splits = (kblocks + per - 1) / per;
+  float2* part = splits > 1 ? static_cast<float2*>(scratch) : nullptr;
+  const dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, splits);
+  cgemm_tf32x3_kernel<OP><<<grid, THREADS, smem_bytes<OP>(), s>>>(maps, M, N, per, kblocks, al,
+                                                                  be, C, ldc, part, err);
+  qeb::count_launches(1);
+  if (splits > 1) {
+    int blocks = (int)(((int64_t)M * N + 255) / 256);
+    if (blocks > 4 * sm_count()) blocks = 4 * sm_count();
+    reduce_slices<<<blocks, 256, 0, s>>>(M, N, splits, part, al, be, C, ldc);
+    qeb::count_launches(1);
+  }
+  return qeb::cuda_status(cudaGetLastError(), "cgemm_tf32x3 launch");
+}
+
+}  // namespace
+
+extern "C" int64_t qeb_cgemm_tf32x3_scratch_bytes(int op_a, int M, int N, int K) {
+  (void)op_a;
+  if (M <= 0 || N <= 0 || K <= 0) return 0;
+  const int s = choose_splits(M, N, K);
+  return s > 1 ? (int64_t)s * M * N * 8 : 0;
+}
+
+extern "C" int qeb_cgemm_tf32x3(int op_a, int M, int N, int K, const double* alpha, const void* A,
+                                int64_t lda, const void* B, int64_t ldb, const double* beta,
+                                void* C, int64_t ldc, void* scratch, int64_t scratch_bytes,
+                                void* stream) {
+  if ((op_a != QEB_OP_N && op_a != QEB_OP_C) || M < 0 || N < 0 || K < 0 || alpha == nullptr ||
+      beta == nullptr || ldc < (M > 0 ? M : 1) || ldb < (K > 0 ? K : 1) ||
+      lda < (op_a == QEB_OP_N ? (M > 0 ? M : 1) : (K > 0 ? K : 1))) {
+    qeb::set_error("cgemm_tf32x3: invalid arguments (op=%d M=%d N=%d K=%d)", op_a, M, N, K);
+    return QEB_EINVAL;
+  }
+  if (M == 0 || N == 0) return QEB_OK;
+  if (K == 0) {
+    qeb::set_error("cgemm_tf32x3: K = 0 (scale C by beta instead)");
+    return QEB_EUNSUPPORTED;
+  }
+  if ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) % 16 != 0 || lda % 2 != 0 ||
+      ldb % 2 != 0) {
+    qeb::set_error("cgemm_tf32x3: A and B need 16-byte aligned columns (even leading dimension)");
+    return QEB_EUNSUPPORTED;
+  }
+  if ((int64_t)2 * K > 0x7fffffff || (int64_t)2 * M > 0x7fffffff || (N + BN - 1) / BN > 65535) {
+    qeb::set_error("cgemm_tf32x3: matrix too large for one launch");
+    return QEB_EUNSUPPORTED;
+  }
+  qeb::EncodeTiled enc;
+  int rc = qeb::tensor_map_encoder(&enc);
+  if (rc) return rc;
+  int* err = nullptr;
+  if ((rc = qeb::tensor_error_word(&err))) return rc;
+  Maps maps;
+  if (op_a == QEB_OP_C) {
+    rc = encode_map(enc, &maps.a, A, 2 * (uint64_t)K, M, lda * 8, BKF, BM, true);
+  } else {
+    rc = encode_map(enc, &maps.a, A, 2 * (uint64_t)M, K, lda * 8, 2 * BM, BKF / 2, false);
+  }
+  if (rc == QEB_OK) rc = encode_map(enc, &maps.b, B, 2 * (uint64_t)K, N, ldb * 8, BKF, BN, true);
+  if (rc) return rc;
+  const float2 al = make_float2((float)alpha[0], (float)alpha[1]);
+  const float2 be = make_float2((float)beta[0], (float)beta[1]);
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  float2* c = static_cast<float2*>(C);
+  return op_a == QEB_OP_C ? launch<QEB_OP_C>(maps, M, N, K, al, be, c, ldc, scratch, scratch_bytes, err, s)
+                          : launch<QEB_OP_N>(maps, M, N, K, al, be, c, ldc, scratch, scratch_bytes, err, s);
+}

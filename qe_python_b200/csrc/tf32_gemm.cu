@@ -28,11 +28,14 @@
 #include <mutex>
 
 #include "qeb_common.cuh"
+#include "tcgen05.cuh"
 #include "../../include/qe_b200.h"
 
 using qeb::C2;
 
 namespace {
+
+using namespace qeb::tc;
 
 constexpr int BM = 128, BN = 64, BK = 32;  // BK: fp32 elements = 128 bytes
 constexpr int STAGES = 3;
@@ -42,90 +45,9 @@ constexpr int STAGE_BYTES = 2 * A_TILE_BYTES + 4 * B_TILE_BYTES;  // 64 KiB
 constexpr int TMEM_COLS = 2 * BN;  // Re and Im accumulators
 constexpr int THREADS = 128;
 constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_BYTES + 1024 /*align*/ + 256 /*barriers*/;
-constexpr long long kWaitLimit = 1ll << 22;  // bounded spin on every mbarrier (~1 s)
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-// Bounded wait on the phase with the given parity; false on timeout.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  const uint32_t addr = smem_u32(bar);
-  for (long long i = 0; i < kWaitLimit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (done) return true;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar,
-                                            int c0, int c1) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
-      " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
-      : "memory");
-}
-
-// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
-// 1024 bytes apart (SBO), version 1 (sm_100), tile base 1024-byte aligned.
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
 
 // Instruction descriptor: D = F32, A = B = TF32, both K-major, M = 128, N = BN.
-constexpr uint32_t kIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(BN >> 3) << 17) |
-                            ((uint32_t)(BM >> 4) << 24);
-
-__device__ __forceinline__ void mma_tf32(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
-                                         uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(adesc), "l"(bdesc), "r"(kIdesc), "r"(accumulate));
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t* bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                   smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
-  uint32_t r[32];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
-        "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
-        "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
-        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
-        "=r"(r[31])
-      : "r"(taddr));
-#pragma unroll
-  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
-}
+constexpr uint32_t kIdesc = idesc_tf32(BM, BN);
 
 struct Maps {
   CUtensorMap a_hi, a_lo, b0_hi, b0_lo, b1_hi, b1_lo;
@@ -212,12 +134,12 @@ __global__ void __launch_bounds__(THREADS, 1) tf32x3_gemm_kernel(
       for (int kk = 0; kk < BK / 8; ++kk) {
         const uint32_t off = kk * 32;  // 8 tf32 = 32 bytes along K
         const uint32_t acc = (i > 0 || kk > 0) ? 1u : 0u;
-        mma_tf32(t_re, smem_desc(a_hi + off), smem_desc(b0_hi + off), acc);
-        mma_tf32(t_re, smem_desc(a_hi + off), smem_desc(b0_lo + off), 1u);
-        mma_tf32(t_re, smem_desc(a_lo + off), smem_desc(b0_hi + off), 1u);
-        mma_tf32(t_im, smem_desc(a_hi + off), smem_desc(b1_hi + off), acc);
-        mma_tf32(t_im, smem_desc(a_hi + off), smem_desc(b1_lo + off), 1u);
-        mma_tf32(t_im, smem_desc(a_lo + off), smem_desc(b1_hi + off), 1u);
+        mma_tf32(t_re, smem_desc_sw128(a_hi + off), smem_desc_sw128(b0_hi + off), kIdesc, acc);
+        mma_tf32(t_re, smem_desc_sw128(a_hi + off), smem_desc_sw128(b0_lo + off), kIdesc, 1u);
+        mma_tf32(t_re, smem_desc_sw128(a_lo + off), smem_desc_sw128(b0_hi + off), kIdesc, 1u);
+        mma_tf32(t_im, smem_desc_sw128(a_hi + off), smem_desc_sw128(b1_hi + off), kIdesc, acc);
+        mma_tf32(t_im, smem_desc_sw128(a_hi + off), smem_desc_sw128(b1_lo + off), kIdesc, 1u);
+        mma_tf32(t_im, smem_desc_sw128(a_lo + off), smem_desc_sw128(b1_hi + off), kIdesc, 1u);
       }
       mma_commit(&empty[s]);
       ++issued;
@@ -238,7 +160,7 @@ __global__ void __launch_bounds__(THREADS, 1) tf32x3_gemm_kernel(
     if (nk > 0) {
       tmem_ld32(lane_base + c0, re);
       tmem_ld32(lane_base + BN + c0, im);
-      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      tmem_wait_ld();
     } else {
 #pragma unroll
       for (int j = 0; j < 32; ++j) re[j] = im[j] = 0.0f;
@@ -297,12 +219,6 @@ __global__ void reduce_split(int M, int N, int splits, const float2* __restrict_
 // Packing: complex source -> K-major hi/lo FP32 planes with interleaved
 // (re, im) along K, rows padded to kp (multiple of 32) with zeros.
 
-__device__ __forceinline__ float tf32_round(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
-
 // layout: QEB_PACK_RAW [re, im]; QEB_PACK_SWAPNEG [im, -re];
 // QEB_PACK_NEGIM [re, -im]; QEB_PACK_SWAP [im, re].
 // transposed == 0: src column r (K contiguous complex values) -> dst row r.
@@ -342,29 +258,7 @@ __global__ void pack_kernel(int rows, int K, int kp, const S* __restrict__ src, 
 // ---------------------------------------------------------------------------
 // Host
 
-using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                 const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                 const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                 CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-std::mutex g_encode_mutex;
-EncodeTiled g_encode = nullptr;
-
-int get_encoder(EncodeTiled* out) {
-  std::lock_guard<std::mutex> lock(g_encode_mutex);
-  if (g_encode == nullptr) {
-    void* fn = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    cudaError_t err = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
-    if (err != cudaSuccess || fn == nullptr || q != cudaDriverEntryPointSuccess) {
-      qeb::set_error("cuTensorMapEncodeTiled is unavailable from the driver");
-      return QEB_ECUDA;
-    }
-    g_encode = reinterpret_cast<EncodeTiled>(fn);
-  }
-  *out = g_encode;
-  return QEB_OK;
-}
+using qeb::EncodeTiled;
 
 int encode(EncodeTiled enc, CUtensorMap* map, const float* ptr, int rows, int kp, int64_t ldp,
            int box_rows) {
@@ -408,11 +302,34 @@ int tf32_splits(int M, int N, int kp) {
   return s < 1 ? 1 : s;
 }
 
-// Device error word for the bounded waits (one per device).
+}  // namespace
+
+namespace qeb {
+
+namespace {
+std::mutex g_encode_mutex;
+EncodeTiled g_encode = nullptr;
 std::mutex g_err_mutex;
 int* g_err[64] = {nullptr};
+}  // namespace
 
-int error_word(int** out) {
+int tensor_map_encoder(EncodeTiled* out) {
+  std::lock_guard<std::mutex> lock(g_encode_mutex);
+  if (g_encode == nullptr) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    cudaError_t err = cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q);
+    if (err != cudaSuccess || fn == nullptr || q != cudaDriverEntryPointSuccess) {
+      set_error("cuTensorMapEncodeTiled is unavailable from the driver");
+      return QEB_ECUDA;
+    }
+    g_encode = reinterpret_cast<EncodeTiled>(fn);
+  }
+  *out = g_encode;
+  return QEB_OK;
+}
+
+int tensor_error_word(int** out) {
   int dev = 0;
   cudaGetDevice(&dev);
   if (dev < 0 || dev >= 64) return QEB_EUNSUPPORTED;
@@ -420,13 +337,13 @@ int error_word(int** out) {
   if (g_err[dev] == nullptr) {
     cudaError_t e = cudaMalloc(&g_err[dev], sizeof(int));
     if (e == cudaSuccess) e = cudaMemset(g_err[dev], 0, sizeof(int));
-    if (e != cudaSuccess) return qeb::cuda_status(e, "tf32 gemm error word");
+    if (e != cudaSuccess) return cuda_status(e, "tensor-core GEMM error word");
   }
   *out = g_err[dev];
   return QEB_OK;
 }
 
-}  // namespace
+}  // namespace qeb
 
 extern "C" int qeb_tf32_pack(int precision, int layout, int transposed, int rows, int K,
                              const void* src, int64_t ld, void* hi, void* lo, int64_t ldp,
@@ -482,10 +399,10 @@ extern "C" int qeb_tf32_gemm(int M, int N, int kp, const void* a_hi, const void*
     return QEB_EUNSUPPORTED;
   }
   EncodeTiled enc;
-  int rc = get_encoder(&enc);
+  int rc = qeb::tensor_map_encoder(&enc);
   if (rc) return rc;
   int* err = nullptr;
-  if ((rc = error_word(&err))) return rc;
+  if ((rc = qeb::tensor_error_word(&err))) return rc;
   Maps maps;
   if ((rc = encode(enc, &maps.a_hi, (const float*)a_hi, M, kp, lda, BM)) ||
       (rc = encode(enc, &maps.a_lo, (const float*)a_lo, M, kp, lda, BM)) ||
@@ -527,11 +444,11 @@ extern "C" int qeb_tf32_gemm(int M, int N, int kp, const void* a_hi, const void*
   return qeb::cuda_status(cudaGetLastError(), "tf32_gemm launch");
 }
 
-// Reads and clears the device error word of the tf32 GEMM bounded waits
+// Reads and clears the device error word of the tensor-core GEMMs' bounded waits
 // (0 = no timeout since the last call).  Synchronises the device.
 extern "C" int qeb_tf32_gemm_error(int* out) {
   int* err = nullptr;
-  int rc = error_word(&err);
+  int rc = qeb::tensor_error_word(&err);
   if (rc) return rc;
   int value = 0;
   cudaError_t e = cudaMemcpy(&value, err, sizeof(int), cudaMemcpyDeviceToHost);

@@ -45,17 +45,25 @@ def leading_dimension(t: torch.Tensor) -> int:
     return t.stride(1)
 
 
+def aligned_ld(rows: int) -> int:
+    """Leading dimension of the matrices this package allocates: rows rounded
+    up to even, so every complex64 column starts on a 16-byte boundary (the
+    TMA loads of the tensor-core GEMMs need that)."""
+    return max(2, rows + (rows & 1))
+
+
 def empty_f(rows: int, cols: int, dtype, device=None, ld: int | None = None) -> torch.Tensor:
     """Uninitialised column-major (rows, cols) tensor."""
     device = device if device is not None else require_cuda()
-    ld = rows if ld is None else ld
+    ld = aligned_ld(rows) if ld is None else ld
     storage = torch.empty((cols, ld), dtype=dtype, device=device)
     return storage.T[:rows]
 
 
 def zeros_f(rows: int, cols: int, dtype, device=None) -> torch.Tensor:
     device = device if device is not None else require_cuda()
-    return torch.zeros((cols, rows), dtype=dtype, device=device).T
+    storage = torch.zeros((cols, aligned_ld(rows)), dtype=dtype, device=device)
+    return storage.T[:rows]
 
 
 def to_device_f(values, dtype, device=None) -> torch.Tensor:
@@ -63,11 +71,13 @@ def to_device_f(values, dtype, device=None) -> torch.Tensor:
     device = device if device is not None else require_cuda()
     if isinstance(values, torch.Tensor):
         t = values
+        if t.dim() == 2 and (t.device != device or t.dtype != dtype or not is_column_major(t)):
+            out = empty_f(t.shape[0], t.shape[1], dtype, device)
+            out.copy_(t)
+            return out
         if t.device != device or t.dtype != dtype:
             t = t.to(device=device, dtype=dtype)
-        if t.dim() == 2 and not is_column_major(t):
-            t = t.T.contiguous().T
-        elif t.dim() == 1 and t.stride(0) != 1:
+        if t.dim() == 1 and t.stride(0) != 1:
             t = t.contiguous()
         return t
     array = np.asarray(values)

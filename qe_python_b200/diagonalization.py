@@ -119,17 +119,28 @@ class _DeviceProjectors:
                 beta[:, offset:offset + n] = b
                 coupling[offset:offset + n, offset:offset + n] = c
                 offset += n
-            self.beta = beta.to(dtype) if dtype != torch.complex128 else beta
-            if dtype != torch.complex128:
-                self.beta = self.beta.T.contiguous().T
+            self.beta = to_device_f(beta, dtype, device) if dtype != torch.complex128 else beta
             self.coupling = to_device_f(coupling, dtype, device)
-        # Split-TF32 operands of the chosen form, packed once per Hamiltonian:
-        # beta^H (calbec) and beta (the H psi update, rows = plane waves).
-        self.packed_conj = None
-        self.packed_plain = None
-        if self.beta is not None and dtype == torch.complex64:
-            self.packed_conj = K.tf32_pack(self.beta, K.PACK_RAW)
-            self.packed_plain = K.tf32_pack(self.beta, K.PACK_RAW, transposed=True)
+            self.block_coupling = K.BlockCoupling(coupling, dtype, device)
+        self._packed_conj = None
+        self._packed_plain = None
+        self._diagonal_terms(diagonals, npw, device)
+
+    # Packed split-TF32 copies of beta for qeb_tf32_gemm, made on first use:
+    # only needed when the operands cannot go to cgemm_tf32x3 directly.
+    @property
+    def packed_conj(self):
+        if self._packed_conj is None and self.beta is not None and self.beta.dtype == torch.complex64:
+            self._packed_conj = K.tf32_pack(self.beta, K.PACK_RAW)
+        return self._packed_conj
+
+    @property
+    def packed_plain(self):
+        if self._packed_plain is None and self.beta is not None and self.beta.dtype == torch.complex64:
+            self._packed_plain = K.tf32_pack(self.beta, K.PACK_RAW, transposed=True)
+        return self._packed_plain
+
+    def _diagonal_terms(self, diagonals, npw, device):
         # Preconditioner diagonal (diagonalization.py:205-229).
         for entry in diagonals:
             if entry[0] == "packed":
@@ -199,7 +210,7 @@ class PlaneWaveHamiltonian:
 
     def couple(self, becp: torch.Tensor) -> torch.Tensor:
         """coupled = D becp with the block-diagonal 0.5 D_Ry (diagonalization.py:348)."""
-        return K.gemm(K.OP_N, self.projectors.coupling, becp)
+        return self.projectors.block_coupling.apply(becp)
 
     def add_projectors(self, coupled: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
         """target += beta coupled (add_projector_product, _native_fft.pyx:782-836)."""
@@ -246,6 +257,50 @@ class PlaneWaveHamiltonian:
                 result = out
             return result[:, 0] if was_vector and result.ndim == 2 else result
         return target[:, 0] if was_vector else target
+
+
+class HpsiGraph:
+    """H|psi> of a fixed band count captured once as a CUDA graph.
+
+    Every kernel of the application (FFT passes, operand packing, projector
+    GEMMs, coupling) is recorded on the capture stream; ``__call__`` copies
+    the input into the captured buffer, replays the graph and copies the
+    result out, so one host call issues the whole H|psi> with no per-kernel
+    launch overhead.
+    """
+
+    def __init__(self, ham: PlaneWaveHamiltonian, nbands: int) -> None:
+        npw = len(ham.basis)
+        self.ham = ham
+        self.nbands = int(nbands)
+        self.input = zeros_f(npw, self.nbands, ham.dtype, ham.device)
+        self.output = zeros_f(npw, self.nbands, ham.dtype, ham.device)
+        stream = torch.cuda.Stream(device=ham.device)
+        stream.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(stream):
+            # warm-up outside the capture: workspaces, attributes, scratch
+            for _ in range(2):
+                ham.apply_into(self.input, self.output)
+        torch.cuda.current_stream().wait_stream(stream)
+        torch.cuda.synchronize()
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            ham.apply_into(self.input, self.output)
+        torch.cuda.synchronize()
+
+    def replay(self) -> torch.Tensor:
+        self.graph.replay()
+        return self.output
+
+    def __call__(self, vectors: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        if tuple(vectors.shape) != tuple(self.input.shape):
+            raise ValueError("the captured graph has a fixed band count")
+        self.input.copy_(vectors)
+        self.graph.replay()
+        if out is None:
+            return self.output.clone()
+        out.copy_(self.output)
+        return out
 
 
 # ---------------------------------------------------------------------------

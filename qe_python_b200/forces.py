@@ -94,13 +94,28 @@ def local_forces(system, tables, grid, rho) -> np.ndarray:
     return out
 
 
-def nonlocal_forces(system, states, tables, occupied) -> np.ndarray:
+def _band_occupations(occupations, nk: int) -> list[np.ndarray]:
+    """Per-k occupation arrays; an int means two electrons in that many bands."""
+    if isinstance(occupations, (int, np.integer)):
+        return [np.full(int(occupations), 2.0) for _ in range(nk)]
+    return [np.asarray(f, dtype=float) for f in occupations]
+
+
+def nonlocal_forces(system, states, tables, occupations) -> np.ndarray:
+    """F_nl = -2 sum_k w_k sum_b f_b Re[conj(d becp/d tau) D becp]
+    (qepy_pw/pw/scf.py:1521-1631); ``occupations`` is a band count (two
+    electrons each) or one occupation array per k point."""
     out = np.zeros((len(system.positions), 3))
-    f_b = 2.0  # fixed occupations
-    for state, weight in zip(states, system.weights):
+    band_occ = _band_occupations(occupations, len(states))
+    for state, weight, occ in zip(states, system.weights, band_occ):
+        active = np.flatnonzero(np.abs(occ) > 1.0e-15)
+        if active.size == 0:
+            continue
+        count = int(active[-1]) + 1
+        f_b = occ[:count][None, :]
         basis = state.basis
         device = state.vectors.device
-        psi = state.vectors[:, :occupied]
+        psi = state.vectors[:, :count]
         if psi.dtype != torch.complex128:
             psi = psi.to(torch.complex128)
         psi = psi.T.contiguous().T
@@ -125,15 +140,15 @@ def nonlocal_forces(system, states, tables, occupied) -> np.ndarray:
             for axis in range(3):
                 scaled = (psi * (1j * kg[:, axis:axis + 1])).T.contiguous().T
                 dbecp = K.gemm(K.OP_C, beta, scaled).cpu().numpy()
-                contrib = np.real(np.conj(dbecp) * coupled).sum(axis=1) * f_b  # per channel
+                contrib = (np.real(np.conj(dbecp) * coupled) * f_b).sum(axis=1)  # per channel
                 out[atom_index, axis] -= 2.0 * float(weight) * contrib.reshape(natoms, c).sum(axis=1)
     return out
 
 
-def hellmann_feynman_forces(system, states, tables, grid, rho, occupied) -> np.ndarray:
+def hellmann_feynman_forces(system, states, tables, grid, rho, occupations) -> np.ndarray:
     charges = np.array([system.pseudos[l].z_valence for l in system.labels])
     components = [
-        nonlocal_forces(system, states, tables, occupied),
+        nonlocal_forces(system, states, tables, occupations),
         ewald_forces(system.lattice, system.positions, charges, system.ecutrho, grid.vectors),
         local_forces(system, tables, grid, rho),
     ]

@@ -50,9 +50,27 @@ def _check_matrix(name: str, t: torch.Tensor) -> None:
         raise ValueError(f"{name} must be a column-major 2-D CUDA tensor")
 
 
+# complex64 products with at least this many complex multiply-adds run as
+# split-TF32 on the tensor cores (cgemm_tf32x3); smaller ones on the FP32 pipes
+TENSOR_MIN_MACS = 1 << 21
+
+
 def gemm(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None,
-         alpha: complex = 1.0, beta: complex = 0.0) -> torch.Tensor:
-    """c = alpha op(a) b + beta c with op(a) = a (OP_N) or a^H (OP_C)."""
+         alpha: complex = 1.0, beta: complex = 0.0, tensor: bool | None = None) -> torch.Tensor:
+    """c = alpha op(a) b + beta c with op(a) = a (OP_N) or a^H (OP_C).
+
+    complex128: FP64 (qeb_zgemm).  complex64: split-TF32 tensor-core products
+    (qeb_cgemm_tf32x3) when ``tensor`` is True, or when it is None and the
+    product is large; else FP32 FMA (qeb_cgemm).
+    """
+    if tensor is not False and a.dtype == torch.complex64 and b.dtype == torch.complex64:
+        m = a.shape[1] if op_a == OP_C else a.shape[0]
+        k = a.shape[0] if op_a == OP_C else a.shape[1]
+        n = b.shape[1] if b.dim() == 2 else 1
+        if tensor or m * n * k >= TENSOR_MIN_MACS:
+            out = cgemm_tf32x3(op_a, a, b, c, alpha, beta)
+            if out is not None:
+                return out
     _check_matrix("a", a)
     _check_matrix("b", b)
     if a.dtype != b.dtype:
@@ -87,6 +105,62 @@ def gemm(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = N
                 0 if scratch is None else scratch.data_ptr(), need, stream_handle())
     _lib.check("qeb_zgemm" if prec == _lib.QEB_F64 else "qeb_cgemm", status)
     return c
+
+
+def diagonal_blocks(coupling: np.ndarray) -> list[tuple[int, int]]:
+    """Smallest contiguous diagonal blocks (start, size) covering every
+    nonzero entry of a square matrix."""
+    nz = np.asarray(coupling) != 0
+    n = nz.shape[0]
+    blocks, s = [], 0
+    while s < n:
+        e = s + 1
+        while True:
+            rows = np.flatnonzero(nz[s:e].any(axis=0))
+            cols = np.flatnonzero(nz[:, s:e].any(axis=1))
+            reach = max(rows.max(initial=s), cols.max(initial=s)) + 1
+            if reach <= e:
+                break
+            e = reach
+        blocks.append((s, e - s))
+        s = e
+    return blocks
+
+
+class BlockCoupling:
+    """coupled = D becp with D block diagonal (qeb_block_coupling)."""
+
+    def __init__(self, coupling: np.ndarray, dtype: torch.dtype, device) -> None:
+        coupling = np.asarray(coupling)
+        self.channels = coupling.shape[0]
+        self.dtype = dtype
+        blocks = diagonal_blocks(coupling)
+        starts = np.array([s for s, _ in blocks], dtype=np.int32)
+        sizes = np.array([n for _, n in blocks], dtype=np.int32)
+        offsets = np.concatenate(([0], np.cumsum(sizes.astype(np.int64) ** 2)[:-1])).astype(np.int64)
+        values = np.concatenate([coupling[s:s + n, s:s + n].reshape(-1) for s, n in blocks]) \
+            if blocks else np.zeros(1)
+        row_block = np.repeat(np.arange(len(blocks), dtype=np.int32), sizes)
+        self.nblocks = len(blocks)
+        self.max_block = int(sizes.max(initial=0))
+        self._row_block = torch.from_numpy(row_block).to(device)
+        self._start = torch.from_numpy(starts).to(device)
+        self._size = torch.from_numpy(sizes).to(device)
+        self._offset = torch.from_numpy(offsets).to(device)
+        self._values = torch.from_numpy(values.astype(np.complex128)).to(device).to(dtype)
+
+    def apply(self, becp: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        _check_matrix("becp", becp)
+        if becp.shape[0] != self.channels or becp.dtype != self.dtype:
+            raise ValueError("becp does not match the coupling")
+        if out is None:
+            out = empty_f(becp.shape[0], becp.shape[1], becp.dtype, becp.device)
+        _lib.check("qeb_block_coupling", _lib.load().qeb_block_coupling(
+            _precision(becp), self.channels, becp.shape[1], self.nblocks,
+            self._row_block.data_ptr(), self._start.data_ptr(), self._size.data_ptr(),
+            self._offset.data_ptr(), self._values.data_ptr(), becp.data_ptr(),
+            leading_dimension(becp), out.data_ptr(), leading_dimension(out), stream_handle()))
+        return out
 
 
 PACK_RAW, PACK_SWAPNEG, PACK_NEGIM, PACK_SWAP = 0, 1, 2, 3
@@ -151,14 +225,65 @@ def tf32_error() -> int:
     return int(value.value)
 
 
+def cgemm_tf32x3(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None,
+                 alpha: complex = 1.0, beta: complex = 0.0) -> torch.Tensor | None:
+    """Split-TF32 c = alpha op(a) b + beta c reading complex64 a and b directly
+    (qeb_cgemm_tf32x3).  Returns None, touching nothing, when a or b lacks
+    16-byte aligned columns (odd leading dimension); callers then use the
+    packed path."""
+    _check_matrix("a", a)
+    _check_matrix("b", b)
+    if a.dtype != torch.complex64 or b.dtype != torch.complex64:
+        raise TypeError("cgemm_tf32x3 takes complex64 operands")
+    if op_a == OP_C:
+        k, m = a.shape
+    elif op_a == OP_N:
+        m, k = a.shape
+    else:
+        raise ValueError("op_a must be OP_N or OP_C")
+    if b.shape[0] != k:
+        raise ValueError(f"inner dimensions disagree: op(a) is {m}x{k}, b is {tuple(b.shape)}")
+    n = b.shape[1]
+    lda, ldb = leading_dimension(a), leading_dimension(b)
+    if (a.data_ptr() % 16 or b.data_ptr() % 16 or lda % 2 or ldb % 2) and m * n * k > 0:
+        return None
+    if c is None:
+        c = empty_f(m, n, torch.complex64, b.device)
+        beta = 0.0
+    else:
+        _check_matrix("c", c)
+        if tuple(c.shape) != (m, n) or c.dtype != torch.complex64:
+            raise ValueError("c has the wrong shape or dtype")
+    if m == 0 or n == 0:
+        return c
+    if k == 0:  # empty contraction: c = beta c
+        return c.zero_() if complex(beta) == 0 else c.mul_(beta)
+    lib = _lib.load()
+    al = (ctypes.c_double * 2)(complex(alpha).real, complex(alpha).imag)
+    be = (ctypes.c_double * 2)(complex(beta).real, complex(beta).imag)
+    need = int(lib.qeb_cgemm_tf32x3_scratch_bytes(op_a, m, n, k))
+    scratch = _SCRATCH.get(need, c.device) if need > 0 else None
+    _lib.check("qeb_cgemm_tf32x3", lib.qeb_cgemm_tf32x3(
+        op_a, m, n, k, al, a.data_ptr(), lda, b.data_ptr(), ldb, be, c.data_ptr(),
+        leading_dimension(c), 0 if scratch is None else scratch.data_ptr(), need,
+        stream_handle()))
+    return c
+
+
 def gemm_tf32(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None,
               alpha: complex = 1.0, beta: complex = 0.0,
               a_packed: PackedOperand | None = None) -> torch.Tensor:
     """Complex c = alpha op(a) b + beta c with split-TF32 tensor-core products.
 
-    op_a = OP_C: a is K x M (op(a) = a^H); OP_N: a is M x K.  ``a_packed``
-    reuses an operand packed earlier with the matching layout.
+    op_a = OP_C: a is K x M (op(a) = a^H); OP_N: a is M x K.  complex64
+    operands with aligned columns go straight to cgemm_tf32x3; otherwise
+    both are packed (``a_packed`` reuses an operand packed earlier with the
+    matching layout) for qeb_tf32_gemm.
     """
+    if a.dtype == torch.complex64 and b.dtype == torch.complex64:
+        out = cgemm_tf32x3(op_a, a, b, c, alpha, beta)
+        if out is not None:
+            return out
     _check_matrix("b", b)
     if op_a == OP_C:
         a_op = a_packed if a_packed is not None else tf32_pack(a, PACK_RAW)

@@ -2,11 +2,13 @@
 
 Restates the reference's SCF loop (qepy_pw/pw/scf.py:_run_scf, :1997-4375)
 for the benchmark cells' feature set: norm-conserving pseudopotentials
-without core correction, LDA (PZ81), no spin, fixed occupations, Davidson,
+without core correction, LDA (PZ81), no spin, fixed or broadened
+(smeared) occupations, Davidson,
 linear or plain-Broyden density mixing, symmetry-reduced k points.  Each
 k point's Hamiltonian and Davidson solve run on the GPU (PlaneWaveHamiltonian,
 davidson); the density is accumulated by the GPU FFT kernels; the charge-grid
-steps (Hartree, XC, mixing, energies) stay on the host as in the reference.
+steps (Hartree, XC, mixing, energies) stay on the device in FP64
+(qe_python_b200.charge), where the reference runs them on the host.
 
 Precision schedules:
   'f64'    plain FP64 everywhere on the GPU;
@@ -34,6 +36,9 @@ from .configs import DIAMOND_CUBIC, displacements, supercell
 from .device import empty_f, require_cuda, to_device_f
 from .diagonalization import PlaneWaveHamiltonian, davidson, lowest_generalized_eigh
 from .pseudo import SyntheticPseudo, synthetic_pseudo
+from .charge import DeviceBroydenMixer, DeviceChargeGrid, DeviceLinearMixer
+from .charge import pz81 as device_pz81
+from .occupations import fixed_occupations, smeared_occupations, smearing_order
 from .pseudo_tables import SpeciesTables, ewald_energy, pz81
 from .symmetry import (
     DensitySymmetrizer,
@@ -68,6 +73,9 @@ class System:
     maxiter: int = 100
     forces: bool = False
     name: str = ""
+    occupations: str = "fixed"   # or "smearing"
+    smearing: str = "gaussian"
+    degauss: float = 0.0         # Ry
 
     @property
     def volume(self) -> float:
@@ -85,17 +93,21 @@ class System:
 def benchmark_system(name: str) -> System:
     """The benchmark cells of qe_python_b200.configs as System objects."""
     pseudo = synthetic_pseudo("X")
-    if name == "scf-fcc2":
+    smear = ("fixed", "gaussian", 0.0)
+    if name in ("scf-fcc2", "scf-fcc2-smear"):
         a = 10.26
         lattice = a / 2.0 * np.array([[-1.0, 0.0, 1.0], [0.0, 1.0, 1.0], [-1.0, 1.0, 0.0]])
         positions = np.array([[0.0, 0.0, 0.0], [0.25, 0.25, 0.25]]) * a
         grid, shift, ecut, ecutrho, nbnd = (4, 4, 4), (1, 1, 1), 20.0, 80.0, 8
         mixing, forces = "linear", False
+        if name == "scf-fcc2-smear":
+            mixing, smear = "plain", ("smearing", "marzari-vanderbilt", 0.02)
     elif name == "scf-dia64":
         lattice = np.eye(3) * 20.52
         positions = supercell(DIAMOND_CUBIC, 2) * 20.52
         grid, shift, ecut, ecutrho, nbnd = (2, 2, 2), (0, 0, 0), 30.0, 180.0, 160
-        mixing, forces = "plain", False
+        mixing, forces = "TF", False
+        smear = _supercell_smearing()
     elif name == "scf-dia8-disp":
         a = 10.26
         lattice = np.eye(3) * a
@@ -107,7 +119,8 @@ def benchmark_system(name: str) -> System:
         lattice = np.eye(3) * a
         positions = supercell(DIAMOND_CUBIC, 3) * a + displacements(216, 0.03)
         grid, shift, ecut, ecutrho, nbnd = None, None, 30.0, 180.0, 480
-        mixing, forces = "plain", True
+        mixing, forces = "TF", True
+        smear = _supercell_smearing()
     else:
         raise KeyError(name)
     labels = ["X"] * len(positions)
@@ -120,7 +133,14 @@ def benchmark_system(name: str) -> System:
         ops = mesh_compatible(points, ops)
         kpoints, weights, _ = reduce_kpoints(points, w, ops)
     return System(lattice, positions, labels, {"X": pseudo}, ecut, ecutrho, nbnd, kpoints, weights,
-                  ops, mixing_mode=mixing, forces=forces, name=name)
+                  ops, mixing_mode=mixing, forces=forces, name=name, occupations=smear[0],
+                  smearing=smear[1], degauss=smear[2])
+
+
+def _supercell_smearing() -> tuple[str, str, float]:
+    from .configs import SUPERCELL_SMEARING as s
+
+    return s["occupations"], s["smearing"], float(s["degauss"])
 
 
 # ---------------------------------------------------------------------------
@@ -203,11 +223,23 @@ def neumaier_metric(residual: np.ndarray, g2: np.ndarray) -> float:
     return total + correction
 
 
-class BroydenMixer:
-    """Plain Broyden mixing of rho(G) in the Coulomb metric
-    (qepy_pw/mixing.py:621-759, mode 'plain')."""
+def thomas_fermi_g2(nelec: float, volume: float) -> float:
+    """Thomas-Fermi screening wavevector squared (bohr^-2) of the uniform
+    electron gas of the cell's mean density (qepy_pw/mixing.py:51-59)."""
+    if not nelec or nelec <= 0.0 or not volume or volume <= 0.0:
+        raise ValueError("Thomas-Fermi mixing needs a positive nelec and volume")
+    rs = (3.0 * volume / (4.0 * np.pi * nelec)) ** (1.0 / 3.0)
+    return float((12.0 / np.pi) ** (2.0 / 3.0) / rs)
 
-    def __init__(self, grid: ChargeGrid, beta: float, ndim: int, cutoff_ry: float) -> None:
+
+class BroydenMixer:
+    """Broyden mixing of rho(G) in the Coulomb metric (qepy_pw/mixing.py:
+    262-413, modes 'plain' and 'TF'; 'TF' scales the updated residual by
+    G^2 / (G^2 + k_TF^2) before the linear step)."""
+
+    def __init__(self, grid: ChargeGrid, beta: float, ndim: int, cutoff_ry: float,
+                 mode: str = "plain", nelec: float | None = None,
+                 volume: float | None = None) -> None:
         self.grid = grid
         self.beta = float(beta)
         self.ndim = int(ndim)
@@ -215,6 +247,12 @@ class BroydenMixer:
         active &= grid.g2 <= cutoff_ry + 1.0e-12
         self.active = np.flatnonzero(active)
         self.g2 = grid.g2[self.active]
+        self.tf_factor = None
+        if mode.lower() == "tf":
+            ks2 = thomas_fermi_g2(nelec, volume)
+            self.tf_factor = self.g2 / (self.g2 + ks2)
+        elif mode.lower() != "plain":
+            raise ValueError(f"mixing_mode {mode!r} is not supported")
         self.dx: list[np.ndarray] = []
         self.df: list[np.ndarray] = []
         self._next = 0
@@ -251,6 +289,8 @@ class BroydenMixer:
                 gamma = np.linalg.lstsq(gram, projection, rcond=1.0e-14)[0]
             cur -= gamma @ dxs
             res -= gamma @ dfs
+        if self.tf_factor is not None:
+            res *= self.tf_factor
         mixed = current + self.beta * residual_g
         mixed[self.active] = cur + self.beta * res
         zero = np.flatnonzero(self.grid.g2 <= 1.0e-14)
@@ -282,6 +322,8 @@ class SCFResult:
     precision_log: list[str] = field(default_factory=list)
     davidson_iterations: list[float] = field(default_factory=list)
     timings: dict[str, float] = field(default_factory=dict)
+    occupations: list[np.ndarray] = field(default_factory=list)
+    fermi_energy_ha: float | None = None
 
     @property
     def total_energy_ry(self) -> float:
@@ -381,6 +423,16 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     volume = system.volume
     nelec = system.nelec
     occupied = int(round(nelec / 2.0))
+    smeared = system.occupations == "smearing"
+    if smeared:
+        if system.degauss <= 0.0:
+            raise ValueError("smearing requires a positive degauss")
+        order = smearing_order(system.smearing)
+    elif system.occupations != "fixed":
+        raise ValueError(f"occupations {system.occupations!r} are not supported")
+    elif system.nbnd < occupied:
+        raise ValueError("nbnd is smaller than the number of occupied states")
+    fermi = None
     bases = make_bases(reciprocal, system.kpoints, system.ecutwfc)
     if min(len(b) for b in bases) < system.nbnd:
         raise ValueError("nbnd exceeds the smallest plane-wave basis")
@@ -393,16 +445,18 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         pos = np.array([p for p, l in zip(system.positions, system.labels) if l == label])
         structure = gpu_structure_factor(grid.vectors, pos, np.ones(len(pos)))
         v_ion_g += table.vloc(q) * structure
-    v_ion = np.ascontiguousarray(grid.to_r(v_ion_g))
+    cgrid = DeviceChargeGrid(grid, device)
+    v_ion = cgrid.to_r(torch.from_numpy(v_ion_g).to(device))
     v_ion_average = float(np.real(np.sum(v_ion_g[grid.g2 < 1.0e-14])))
     charges = np.array([system.pseudos[l].z_valence for l in system.labels])
     e_ion = ewald_energy(system.lattice, system.positions, charges, system.ecutrho,
                          structure=gpu_structure_factor)
     # uniform starting density (no PP_RHOATOM): rho(G=0) = nelec / Omega
-    rho = np.full(shape, nelec / volume)
+    rho = torch.full(shape, nelec / volume, dtype=torch.float64, device=device)
     symmetrizer = DensitySymmetrizer(system.operations, shape) if len(system.operations) > 1 else None
-    mixer = (LinearMixer(system.mixing_beta) if system.mixing_mode == "linear"
-             else BroydenMixer(grid, system.mixing_beta, system.mixing_ndim, system.ecutrho))
+    mixer = (DeviceLinearMixer(system.mixing_beta) if system.mixing_mode == "linear"
+             else DeviceBroydenMixer(cgrid, system.mixing_beta, system.mixing_ndim,
+                                     system.mixing_mode, nelec, volume))
     states = [KPointState(b, shape, device) for b in bases]
     rng = QERandom()
     davidson_tolerance = 0.5 * 1.0e-2  # diago_thr_init 1e-2 Ry -> Ha
@@ -420,10 +474,10 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     while iteration <= system.maxiter:
         t0 = time.perf_counter()
         if input_hxc is None:
-            vh = grid.to_r(hartree(grid.to_g(rho), grid.g2))
-            _eps, vxc = pz81(rho)
+            vh = cgrid.to_r(cgrid.hartree(cgrid.to_g(rho)))
+            _eps, vxc = device_pz81(rho)
             input_hxc = vh + vxc
-        v_eff = v_ion + input_hxc
+        v_dev = v_ion + input_hxc
         if iteration > 1 and np.isfinite(previous_accuracy):
             if iteration == 2:
                 davidson_tolerance = 5.0e-3
@@ -435,7 +489,6 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         # FP32 eigenvalues stall near 1e-7 relative: never ask more of them
         tol = davidson_tolerance if current_precision == "f64" else max(davidson_tolerance, 2.0e-6)
         precision_log.append(current_precision)
-        v_dev = torch.from_numpy(v_eff).to(device)
         tick("v_of_rho", t0)
         t0 = time.perf_counter()
         eigenvalues = []
@@ -458,7 +511,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             # iterations restart from the converged eigenvectors
             # (qepy_pw/pw/scf.py:3503-3556)
             is_ritz = iteration == 1
-            occ_roots = occupied if iteration > 1 else system.nbnd
+            occ_roots = occupied if iteration > 1 and not smeared else system.nbnd
             attempt, total_its = 0, 0.0
             retry_vectors, retry_eigs, retry_applied = start_vectors, initial_eigs, initial_applied
             while True:
@@ -482,22 +535,33 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         torch.cuda.synchronize()
         tick("c_bands", t0)
         t0 = time.perf_counter()
-        # density from the occupied states (FP64 accumulation on the GPU)
+        if smeared:
+            # qepy_pw/pw/scf.py:3685-3695 (degauss halved to Hartree)
+            fermi, band_occ, demet = smeared_occupations(eigenvalues, system.weights, nelec,
+                                                         0.5 * system.degauss, order)
+        else:
+            band_occ, demet = fixed_occupations(system.nbnd, occupied, len(states)), 0.0
+        # density from the occupied states (FP64 accumulation on the GPU),
+        # bands up to the last one with a nonzero occupation (scf.py:1406-1431)
         rho_device.zero_()
-        for state, weight in zip(states, system.weights):
+        for state, weight, occ in zip(states, system.weights, band_occ):
+            active = np.flatnonzero(np.abs(occ) > 1.0e-15)
+            if active.size == 0:
+                continue
+            count = int(active[-1]) + 1
             ws = state.workspace("f64")
-            w = torch.full((occupied,), float(weight) * 2.0 / volume, dtype=torch.float64, device=device)
-            ws.accumulate_density(rho_device, state.vectors[:, :occupied], w)
-        rho_out = rho_device.cpu().numpy()
-        rho_out *= nelec * grid.size / (float(np.sum(rho_out)) * volume)
+            w = torch.from_numpy(float(weight) * occ[:count] / volume).to(device)
+            ws.accumulate_density(rho_device, state.vectors[:, :count], w)
+        rho_out = rho_device * (nelec * grid.size / (float(torch.sum(rho_device)) * volume))
         if symmetrizer is not None:
-            rho_out = symmetrizer.apply(rho_out)
-            rho_out *= nelec * grid.size / (float(np.sum(rho_out)) * volume)
-        band_energy = sum(w * 2.0 * float(np.sum(e[:occupied])) for w, e in zip(system.weights, eigenvalues))
+            sym = symmetrizer.apply(rho_out.cpu().numpy())
+            sym *= nelec * grid.size / (float(np.sum(sym)) * volume)
+            rho_out = torch.from_numpy(sym).to(device)
+        band_energy = sum(w * float(np.sum(e * f)) for w, e, f in zip(system.weights, eigenvalues, band_occ))
         scale = volume / grid.size
-        deband = -scale * float(np.sum(rho_out * input_hxc))
-        residual_g = grid.to_g(rho_out - rho)
-        accuracy = 0.5 * volume * neumaier_metric(residual_g, grid.g2)
+        deband = -scale * float(torch.sum(rho_out * input_hxc))
+        residual_g = cgrid.to_g(rho_out - rho)
+        accuracy = 0.5 * volume * cgrid.residual_metric(residual_g)
         previous_accuracy = accuracy
         tick("sum_band", t0)
         if iteration == 1 and first_diagonalization and accuracy < davidson_tolerance * max(1.0, nelec):
@@ -509,21 +573,21 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         converged = 2.0 * accuracy < system.conv_thr
         if converged:
             rho_energy = rho_out
-        elif isinstance(mixer, BroydenMixer):
+        elif isinstance(mixer, DeviceBroydenMixer):
             rho_energy = mixer.mix(rho, residual_g)
         else:
             rho_energy = mixer.mix(rho, rho_out)
-        rho_energy_g = grid.to_g(rho_energy)
-        vh_g = hartree(rho_energy_g, grid.g2)
-        e_h = volume * 0.5 * float(np.real(np.vdot(rho_energy_g, vh_g)))
-        eps_xc, vxc = pz81(rho_energy)
-        e_xc = scale * float(np.sum(rho_energy * eps_xc))
-        vh = grid.to_r(vh_g)
+        rho_energy_g = cgrid.to_g(rho_energy)
+        vh_g = cgrid.hartree(rho_energy_g)
+        e_h = volume * 0.5 * float(torch.real(torch.vdot(rho_energy_g, vh_g)))
+        eps_xc, vxc = device_pz81(rho_energy)
+        e_xc = scale * float(torch.sum(rho_energy * eps_xc))
+        vh = cgrid.to_r(vh_g)
         hxc = vh + vxc
-        descf = -scale * float(np.sum(rho_energy * hxc) - np.sum(rho_out * hxc))
+        descf = -scale * float(torch.sum(rho_energy * hxc) - torch.sum(rho_out * hxc))
         input_hxc = hxc
         energy_terms = {"one_electron": band_energy + deband, "hartree": e_h, "xc": e_xc,
-                        "ewald": e_ion, "descf": descf}
+                        "ewald": e_ion, "descf": descf, "smearing": demet}
         total = sum(energy_terms.values())
         energies.append(total)
         accuracies.append(accuracy)
@@ -534,13 +598,15 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         if converged:
             break
         iteration += 1
+    rho = rho.cpu().numpy()
     forces = None
     if system.forces and converged:
         from .forces import hellmann_feynman_forces
 
         t0 = time.perf_counter()
-        forces = hellmann_feynman_forces(system, states, tables, grid, rho, occupied)
+        forces = hellmann_feynman_forces(system, states, tables, grid, rho, band_occ)
         tick("forces", t0)
     return SCFResult(converged, total, iteration, energies, accuracies,
                      [s.eigenvalues for s in states], energy_terms, rho, forces,
-                     time.perf_counter() - started, precision_log, david_its, timings)
+                     time.perf_counter() - started, precision_log, david_its, timings,
+                     [np.asarray(f) for f in band_occ], fermi)

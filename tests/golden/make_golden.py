@@ -194,6 +194,8 @@ def scf(name: str, workdir: Path, filename: str) -> None:
         "energy_terms_ry": {k: 2.0 * float(v) for k, v in vars(result.energy_terms).items()},
         "forces_ry_per_bohr": None if result.forces_ha_per_bohr is None
         else (2.0 * np.asarray(result.forces_ha_per_bohr)).tolist(),
+        "fermi_energy_ry": None if getattr(result, "fermi_energy_ha", None) is None
+        else 2.0 * float(result.fermi_energy_ha),
         "reference_wall_seconds": elapsed,
         "reference_runner": "reference Python + NumPy oracle native module, 1 process",
     }
@@ -232,6 +234,66 @@ def setup_tables(workdir: Path) -> None:
         ewald_forces=ewald_forces(lattice, positions, charges, 100.0))
 
 
+def smearing_tables() -> None:
+    """Reference Fermi levels, occupations and smearing energies for seeded
+    eigenvalue sets and every broadening order (smearing.json)."""
+    from qepy_pw.occupations import smeared_occupations, w1gauss, wgauss
+
+    rng = np.random.default_rng(5)
+    cases = []
+    for order in (0, 1, -1, -99):
+        for degauss in (0.005, 0.02):
+            nk = 3
+            eigenvalues = [np.sort(rng.uniform(-0.5, 0.6, 10)) for _ in range(nk)]
+            weights = rng.uniform(0.5, 1.5, nk)
+            weights /= weights.sum()
+            nelec = 11.0
+            fermi, occ, demet = smeared_occupations(eigenvalues, weights, nelec, degauss, order)
+            cases.append({"order": order, "degauss_ha": degauss, "nelec": nelec,
+                          "eigenvalues_ha": [e.tolist() for e in eigenvalues],
+                          "weights": weights.tolist(), "fermi_ha": fermi,
+                          "occupations": [o.tolist() for o in occ], "demet_ha": demet})
+    x = np.linspace(-8.0, 8.0, 161)
+    functions = {str(order): {"wgauss": wgauss(x, order).tolist(), "w1gauss": w1gauss(x, order).tolist()}
+                 for order in (0, 1, 2, -1, -99)}
+    record = {"source": "qepy_pw/occupations.py smeared_occupations, wgauss, w1gauss",
+              "x": x.tolist(), "functions": functions, "cases": cases}
+    (HERE / "smearing.json").write_text(json.dumps(record))
+    print("smearing: %d cases" % len(cases))
+
+
+def mixer_tables() -> None:
+    """The reference SCF's Broyden mixer (DistributedBroydenMixer on the
+    charge-sphere coefficients, qepy_pw/pw/scf.py:3027-3041) in 'plain' and
+    'TF' modes over seven steps of seeded densities on a 9^3 grid of the
+    2-atom fcc cell, sphere |G|^2 <= 20 (broyden.npz)."""
+    from qepy_pw.basis import LocalPotentialWorkspace as RefWorkspace
+    from qepy_pw.mixing import DistributedBroydenMixer
+
+    from qe_python_b200.scf import ChargeGrid
+
+    lattice = 10.26 / 2.0 * np.array([[-1.0, 0.0, 1.0], [0.0, 1.0, 1.0], [-1.0, 1.0, 0.0]])
+    reciprocal = 2.0 * np.pi * np.linalg.inv(lattice).T
+    volume = abs(np.linalg.det(lattice))
+    shape = (9, 9, 9)
+    grid = ChargeGrid(shape, reciprocal, 20.0)
+    rng = np.random.default_rng(8)
+    outs = 0.05 + 0.02 * rng.random((7, *shape))
+    start = 0.05 + 0.02 * rng.random(shape)
+    record = {"shape": np.array(shape), "lattice": lattice, "start": start, "outs": outs}
+    for mode in ("plain", "TF"):
+        workspace = RefWorkspace(grid.miller, shape)
+        mixer = DistributedBroydenMixer(workspace, grid.g2, beta=0.7, ndim=4, g2_cutoff=20.0,
+                                        mode=mode, nelec=8.0, volume=volume)
+        rho, seq = start.copy(), []
+        for out in outs:
+            rho = mixer.mix(rho, out)
+            seq.append(rho.copy())
+        record[f"mixed_{mode}"] = np.array(seq)
+    np.savez_compressed(HERE / "broyden.npz", **record)
+    print("broyden: plain and TF sequences")
+
+
 def si_regression() -> None:
     path = REFERENCE_ROOT / "tests/qe_reference/reference/pw_scf/scf.in.out"
     text = path.read_text()
@@ -257,8 +319,11 @@ def main() -> None:
         hamiltonian_and_davidson()
         setup_tables(workdir)
         si_regression()
+        smearing_tables()
+        mixer_tables()
         if not args.skip_scf:
             scf("scf-fcc2", workdir, "scf_fcc2.json")
+            scf("scf-fcc2-smear", workdir, "scf_fcc2_smear.json")
             scf("scf-dia8-disp", workdir, "scf_dia8_disp.json")
 
 

@@ -3,10 +3,13 @@
 Cell: the 8-atom displaced diamond cell (scf-dia8-disp) reduced to the Gamma
 point and 16 bands so each solve takes seconds.  V_Hxc is a smooth seeded
 field.  Checks:
-  * d E_band / d V_Hxc along a smooth direction vs (E(V+e dV) - E(V-e dV))/2e
-  * d E_band / d tau for two coordinates vs central differences, h = 1e-3 bohr
+  * d E_band / d V_Hxc along a smooth direction vs central differences
+    (steps 1e-4 and 5e-5, Richardson-extrapolated)
+  * d E_band / d tau for two coordinates vs central differences, h = 1e-3 and
+    5e-4 bohr, Richardson-extrapolated
     (tolerance 1e-5 Ha/bohr = 2e-5 Ry/bohr, well inside the 1e-4 Ry/bohr bar)
-  * the mixed-precision gradient against the FP64 gradient (1e-4 Ry/bohr).
+  * the mixed-precision gradient (FP32/split-TF32 solve, FP64 polish)
+    against the FP64 gradient (1e-4 Ry/bohr).
 """
 
 from __future__ import annotations
@@ -25,8 +28,7 @@ def _problem(precision):
     system.kpoints = np.zeros((1, 3))
     system.weights = np.ones(1)
     system.nbnd = 16
-    return BandProblem(system, precision=precision,
-                       tolerance=1e-11 if precision == "f64" else 1e-6)
+    return BandProblem(system, precision=precision, tolerance=1e-10)
 
 
 def _smooth(shape, seed, amplitude):
@@ -50,24 +52,32 @@ def test_band_energy_gradients_match_finite_differences(cuda_device):
     energy = BandEnergy.apply(v, tau, problem)
     energy.backward()
     dv = _smooth(problem.shape, 2, 1.0)
-    eps = 1e-4
 
     def e_at(vv, pos):
         return problem.solve(vv, pos)[0]
 
+    def richardson(f, step):
+        # central differences at step and step/2 combined to cancel the
+        # O(step^2) truncation term: (4 D(h/2) - D(h)) / 3
+        d1 = (f(step) - f(-step)) / (2 * step)
+        d2 = (f(step / 2) - f(-step / 2)) / step
+        return (4.0 * d2 - d1) / 3.0, d1
+
     base_v = v.detach().cpu().numpy()
     base_tau = problem.system.positions.copy()
-    fd_v = (e_at(base_v + eps * dv, base_tau) - e_at(base_v - eps * dv, base_tau)) / (2 * eps)
+    fd_v, plain_v = richardson(lambda e: e_at(base_v + e * dv, base_tau), 1e-4)
     an_v = float(np.sum(v.grad.cpu().numpy() * dv))
-    assert abs(fd_v - an_v) <= 1e-6 * max(1.0, abs(fd_v))
-    h = 1e-3
+    assert abs(fd_v - an_v) <= 1e-6 * max(1.0, abs(fd_v)), (fd_v, plain_v, an_v)
+
+    def moved(atom, axis, e):
+        pos = base_tau.copy()
+        pos[atom, axis] += e
+        return pos
+
     for atom, axis in ((0, 0), (3, 2)):
-        plus, minus = base_tau.copy(), base_tau.copy()
-        plus[atom, axis] += h
-        minus[atom, axis] -= h
-        fd = (e_at(base_v, plus) - e_at(base_v, minus)) / (2 * h)
+        fd, plain = richardson(lambda e: e_at(base_v, moved(atom, axis, e)), 1e-3)
         an = float(tau.grad[atom, axis])
-        assert abs(fd - an) < 1e-5, (atom, axis, fd, an)
+        assert abs(fd - an) < 1e-5, (atom, axis, fd, plain, an)
 
 
 def test_mixed_gradient_matches_fp64(cuda_device):
@@ -76,8 +86,8 @@ def test_mixed_gradient_matches_fp64(cuda_device):
     from qe_python_b200.adjoint import BandEnergy
 
     grads = []
-    for precision in ("f64", "mixed_f32"):
-        problem = _problem("f64" if precision == "f64" else "f32")
+    for precision in ("f64", "mixed"):
+        problem = _problem(precision)
         v = torch.from_numpy(_smooth(problem.shape, 1, 0.2)).cuda().requires_grad_(True)
         tau = torch.from_numpy(problem.system.positions.copy()).cuda().requires_grad_(True)
         BandEnergy.apply(v, tau, problem).backward()

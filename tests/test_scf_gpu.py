@@ -32,3 +32,23 @@ def test_scf_fcc2_matches_reference(cuda_device, precision, e_tol, eig_tol):
     assert abs(result.total_energy_ry - ref["total_energy_ry"]) < e_tol
     for mine, theirs in zip(result.eigenvalues_ha, ref["eigenvalues_ry"]):
         np.testing.assert_allclose(2.0 * np.asarray(mine), theirs, atol=eig_tol)
+
+
+@pytest.mark.parametrize("precision,e_tol,eig_tol", [("f64", 1e-8, 1e-7), ("mixed", 1e-8, 1e-6)])
+def test_scf_fcc2_smearing_matches_reference(cuda_device, precision, e_tol, eig_tol):
+    """Broadened filling (Marzari-Vanderbilt, 0.02 Ry) with Broyden mixing:
+    tests/golden/scf_fcc2_smear.json is the reference's run of the same cell."""
+    from qe_python_b200.scf import benchmark_system, run_scf
+
+    ref = json.loads((GOLDEN / "scf_fcc2_smear.json").read_text())
+    result = run_scf(benchmark_system("scf-fcc2-smear"), precision=precision)
+    assert result.converged
+    assert abs(result.total_energy_ry - ref["total_energy_ry"]) < e_tol
+    # Cold smearing makes the electron count flat around the Fermi level, so
+    # the FP32 stage's 1e-7-level eigenvalue differences move it by 1e-5 Ry
+    # while the energy stays within 1e-8 Ry.
+    assert abs(2.0 * result.fermi_energy_ha - ref["fermi_energy_ry"]) < \
+        (1e-6 if precision == "f64" else 1e-4)
+    assert abs(2.0 * result.energy_terms_ha["smearing"] - ref["energy_terms_ry"]["smearing_ha"]) < e_tol
+    for mine, theirs in zip(result.eigenvalues_ha, ref["eigenvalues_ry"]):
+        np.testing.assert_allclose(2.0 * np.asarray(mine), theirs, atol=eig_tol)
