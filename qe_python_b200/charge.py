@@ -105,6 +105,12 @@ class DeviceBroydenMixer:
         self.prev_in = None
         self.prev_res = None
 
+    def reset(self) -> None:
+        """Forget the secant history (the next step is linear mixing)."""
+        self.dx, self.df = [], []
+        self._next = 0
+        self.prev_in = self.prev_res = None
+
     def mix(self, rho_in: torch.Tensor, residual_g: torch.Tensor) -> torch.Tensor:
         current = self.grid.to_g(rho_in)
         cur = current[self.active]

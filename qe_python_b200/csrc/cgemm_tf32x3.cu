@@ -5,26 +5,35 @@
 // A, B and C are column-major complex64 matrices.  Unlike qeb_tf32_gemm,
 // nothing is packed beforehand: each pipeline stage TMA-loads the raw FP32
 // words of one 128-row by 16-complex slab of A and of B into shared memory,
-// and four converter warps split every value x into hi = tf32(x) and
+// and the worker warps split every value x into hi = tf32(x) and
 // lo = tf32(x - hi) in place, in the 128-byte-swizzled K-major layout that
 // tcgen05.mma reads.  The complex product is carried by real products over
 // (re, im) pairs interleaved along K:
 //   OP_C  Re(conj(a) b) = [a_re, a_im].[b_re, b_im]
 //         Im(conj(a) b) = [a_re, a_im].[b_im, -b_re]       (B1 = swap-negated B)
 //   OP_N  Re(a b)       = [a_re, -a_im].[b_re, b_im]      (A0, A transposed by
-//         Im(a b)       = [a_im, a_re].[b_re, b_im]        the converters)
-// and each real product is hi*hi + hi*lo + lo*hi, three tcgen05.mma.kind::tf32
-// accumulating in FP32 in tensor memory (Re in columns [0, 128), Im in
-// [128, 256)).
+//         Im(a b)       = [a_im, a_re].[b_re, b_im]        the workers)
+// and each real product is hi*hi + hi*lo + lo*hi, three tcgen05.mma.kind::tf32.
 //
-// One CTA = 192 threads computes a 128 x 128 output tile over a K range:
+// Two-level accumulation: the tensor cores add each MMA's products into the
+// FP32 accumulator with an error that grows with the number of additions
+// (measured: 7e-6 relative after 384 MMAs into one accumulator, 2e-4 after
+// 12 000), so each stage's 12 MMAs per accumulator start a fresh tensor-memory
+// accumulator (two buffers of Re and Im, 512 columns) and the worker warps add
+// it into FP32 registers with round-to-nearest.  The result is as accurate
+// as an FP32 FMA GEMM.
+//
+// One CTA = 320 threads computes a 128 x 128 output tile over a K range:
 //   warp 0 lane 0 : TMA producer, two stages
 //   warp 1 lane 0 : MMA issuer; warp 1 owns the tensor-memory allocation
-//   warps 2-5     : converters, then the epilogue (tcgen05.ld, complex store)
-// K is split across CTAs (grid.z) into caller scratch when the output has
-// few tiles; a second kernel sums the slices in a fixed order.  Every wait
-// is bounded; on timeout the CTA records an error code in the device word
-// read by qeb_tf32_gemm_error and unwinds.
+//   warps 2-9     : workers: split the next stage, drain the previous
+//                   stage's accumulator into registers, then store C
+// Worker warp w reads tensor-memory lanes 32 (w % 4) .. +31 (its rows) and
+// columns 64 ((w - 2) / 4) .. +63 of Re and of Im.  K is split across CTAs
+// (grid.z) into caller scratch when the output has few tiles; a second kernel
+// sums the slices in a fixed order.  Every wait is bounded; on timeout the
+// CTA records an error code in the device word read by qeb_tf32_gemm_error
+// and unwinds.
 //
 // Requirements (else QEB_STATUS_EUNSUPPORTED, and the caller uses the packed
 // path): A and B 16-byte aligned with even leading dimensions (TMA rows must
@@ -44,8 +53,11 @@ constexpr int BM = 128, BN = 128;
 constexpr int BKF = 32;      // FP32 words along K per stage (16 complex values)
 constexpr int TILE = 16384;  // bytes of one 128-row x 32-word tile
 constexpr int STAGES = 2;
-constexpr int THREADS = 192;
-constexpr int TMEM_COLS = 2 * BN;
+constexpr int WORKERS = 8;                 // worker warps (2 .. 9)
+constexpr int WORKER_THREADS = 32 * WORKERS;
+constexpr int THREADS = 64 + WORKER_THREADS;
+constexpr int ACC_COLS = 2 * BN;           // Re and Im of one accumulator buffer
+constexpr int TMEM_COLS = 2 * ACC_COLS;    // two buffers
 constexpr uint32_t kIdesc = idesc_tf32(BM, BN);
 
 // Tile slots of one stage.  OP_C: 0 A (raw, then hi), 1 A lo, 2 B (raw, then
@@ -86,8 +98,8 @@ __device__ __forceinline__ void split_tile(unsigned char* tile, unsigned char* l
                                            unsigned char* swap_hi, unsigned char* swap_lo) {
   float4* t = reinterpret_cast<float4*>(tile);
   float4* l = reinterpret_cast<float4*>(lo);
-#pragma unroll 4
-  for (int c = ct; c < TILE / 16; c += 128) {
+#pragma unroll 2
+  for (int c = ct; c < TILE / 16; c += WORKER_THREADS) {
     const float4 v = t[c];
     const float4 h = hi4(v), w = lo4(v, h);
     t[c] = h;
@@ -106,7 +118,7 @@ __device__ __forceinline__ void transpose_a(const unsigned char* raw, unsigned c
                                             unsigned char* a1l, int ct) {
   const float2* x = reinterpret_cast<const float2*>(raw);
 #pragma unroll 2
-  for (int it = ct; it < BM * 8; it += 128) {
+  for (int it = ct; it < BM * 8; it += WORKER_THREADS) {
     const int m = it & (BM - 1), kp = it >> 7;  // kp: pair of K values 2kp, 2kp+1
     const float2 x0 = x[(2 * kp) * BM + m];
     const float2 x1 = x[(2 * kp + 1) * BM + m];
@@ -121,6 +133,30 @@ __device__ __forceinline__ void transpose_a(const unsigned char* raw, unsigned c
   }
 }
 
+// Worker side of one stage's accumulator buffer: wait until its MMAs are
+// done, add Re (columns [0, 64) of this warp's half) and Im into registers,
+// release the buffer.  False on a timed-out wait.
+__device__ __forceinline__ bool drain_accumulator(float (&acc)[BN], uint64_t* acc_full,
+                                                  uint64_t* acc_empty, int i, uint32_t lane_base,
+                                                  int lane) {
+  const int b = i & 1;
+  if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], (i >> 1) & 1))) return false;
+  asm volatile("tcgen05.fence::after_thread_sync;");
+  const uint32_t t = lane_base + b * ACC_COLS;
+#pragma unroll
+  for (int part = 0; part < 4; ++part) {  // Re 0-31, Re 32-63, Im 0-31, Im 32-63
+    float v[32];
+    tmem_ld32(t + (part >> 1) * BN + (part & 1) * 32, v);
+    tmem_wait_ld();
+#pragma unroll
+    for (int j = 0; j < 32; ++j) acc[part * 32 + j] += v[j];
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;");
+  __syncwarp();
+  if (lane == 0) mbar_arrive(&acc_empty[b]);
+  return true;
+}
+
 template <int OP>
 __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
     const __grid_constant__ Maps maps, int M, int N, int kb_per_split, int kb_total, float2 alpha,
@@ -130,9 +166,11 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * S::stage_bytes);
-  uint64_t* conv = full + STAGES;
-  uint64_t* empty = conv + STAGES;
-  uint64_t* done = empty + STAGES;
+  uint64_t* conv = full + STAGES;       // stage split by the workers
+  uint64_t* empty = conv + STAGES;      // stage consumed by the MMAs
+  uint64_t* acc_full = empty + STAGES;  // accumulator buffer written by the MMAs
+  uint64_t* acc_empty = acc_full + 2;   // accumulator buffer drained by the workers
+  uint64_t* done = acc_empty + 2;       // every MMA issued has completed
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
   volatile int* abort_v = abort_flag;
@@ -145,8 +183,12 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&conv[s], 4);  // one arrival per converter warp
+      mbar_init(&conv[s], WORKERS);  // one arrival per worker warp
       mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&acc_full[b], 1);
+      mbar_init(&acc_empty[b], WORKERS);
     }
     mbar_init(done, 1);
     *abort_flag = 0;
@@ -186,20 +228,22 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      const uint32_t t_re = tmem, t_im = tmem + BN;
       for (int i = 0; i < nk; ++i) {
-        const int s = i % STAGES;
-        if (!mbar_wait(&conv[s], (i / STAGES) & 1)) {
+        const int s = i % STAGES, b = i & 1;
+        // the stage is split, and this accumulator buffer was drained (i - 2)
+        if (!mbar_wait(&conv[s], (i / STAGES) & 1) ||
+            (i >= 2 && !mbar_wait(&acc_empty[b], ((i >> 1) - 1) & 1))) {
           atomicExch(error, 12);
           *abort_v = 1;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;");
         const uint32_t st = smem_u32(base + s * S::stage_bytes);
+        const uint32_t t_re = tmem + b * ACC_COLS, t_im = t_re + BN;
 #pragma unroll
         for (int kk = 0; kk < BKF / 8; ++kk) {
           const uint32_t off = kk * 32;  // 8 tf32 words along K
-          const uint32_t acc = (i > 0 || kk > 0) ? 1u : 0u;
+          const uint32_t acc = kk > 0 ? 1u : 0u;
           const uint64_t arh = smem_desc_sw128(st + S::a_re_hi * TILE + off);
           const uint64_t arl = smem_desc_sw128(st + S::a_re_lo * TILE + off);
           const uint64_t aih = smem_desc_sw128(st + S::a_im_hi * TILE + off);
@@ -215,20 +259,26 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
           mma_tf32(t_im, aih, bil, kIdesc, 1u);
           mma_tf32(t_im, ail, bih, kIdesc, 1u);
         }
-        mma_commit(&empty[s]);
+        mma_commit(&empty[s]);     // the stage may be reloaded
+        mma_commit(&acc_full[b]);  // the accumulator buffer may be drained
       }
-      mma_commit(done);  // arrives once every MMA issued above has completed
+      // tensor memory is freed below only after every MMA issued completed
+      mma_commit(done);
+      if (!mbar_wait(done, 0)) atomicExch(error, 14);
     }
   } else {
-    const int ct = threadIdx.x - 64;  // 0..127
-    for (int i = 0; i < nk; ++i) {
+    const int ct = threadIdx.x - 64;          // 0 .. WORKER_THREADS - 1
+    const int quarter = warp & 3;             // tensor-memory lane window
+    const int half = (warp - 2) >> 2;         // column half of Re and Im
+    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16) + half * (BN / 2);
+    float acc[BN];                            // Re [0, 64), Im [64, 128) of this row
+#pragma unroll
+    for (int j = 0; j < BN; ++j) acc[j] = 0.0f;
+    bool ok = true;
+    for (int i = 0; i < nk && ok; ++i) {
       const int s = i % STAGES;
-      const bool ok = __all_sync(0xffffffffu, mbar_wait(&full[s], (i / STAGES) & 1));
-      if (!ok || *abort_v) {
-        if (!ok && lane == 0) {
-          atomicExch(error, 13);
-          *abort_v = 1;
-        }
+      if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (i / STAGES) & 1)) || *abort_v) {
+        ok = false;
         break;
       }
       unsigned char* st = base + s * S::stage_bytes;
@@ -244,37 +294,27 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&conv[s]);
+      if (i > 0 && !drain_accumulator(acc, acc_full, acc_empty, i - 1, lane_base, lane)) ok = false;
     }
-  }
-  __syncwarp();
-
-  if (warp >= 2) {
-    const bool ok = mbar_wait(done, 0);
-    asm volatile("tcgen05.fence::after_thread_sync;");
-    if (!ok && lane == 0) atomicExch(error, 14);
+    if (ok && nk > 0 && !drain_accumulator(acc, acc_full, acc_empty, nk - 1, lane_base, lane))
+      ok = false;
+    if (!ok && lane == 0) {
+      atomicExch(error, 13);
+      *abort_v = 1;
+    }
     const bool aborted = !__all_sync(0xffffffffu, ok) || *abort_v;
-    const int quarter = warp & 3;  // tcgen05.ld lane window of this warp
     const int row = m0 + quarter * 32 + lane;
-    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16);
-    for (int c0 = 0; c0 < BN; c0 += 32) {
-      float re[32], im[32];
-      tmem_ld32(lane_base + c0, re);
-      tmem_ld32(lane_base + BN + c0, im);
-      tmem_wait_ld();
-      if (nk == 0) {
+    if (!aborted && row < M) {
 #pragma unroll
-        for (int j = 0; j < 32; ++j) re[j] = im[j] = 0.0f;
-      }
-      if (aborted || row >= M) continue;
-#pragma unroll
-      for (int j = 0; j < 32; ++j) {
-        const int col = n0 + c0 + j;
-        if (col >= N) break;
+      for (int j = 0; j < BN / 2; ++j) {
+        const int col = n0 + half * (BN / 2) + j;
+        if (col >= N) continue;
+        const float re = acc[j], im = acc[BN / 2 + j];
         if (split != nullptr) {
-          split[(int64_t)blockIdx.z * M * N + row + (int64_t)col * M] = make_float2(re[j], im[j]);
+          split[(int64_t)blockIdx.z * M * N + row + (int64_t)col * M] = make_float2(re, im);
         } else {
           float2* c = C + row + (int64_t)col * ldc;
-          float2 v = make_float2(alpha.x * re[j] - alpha.y * im[j], alpha.x * im[j] + alpha.y * re[j]);
+          float2 v = make_float2(alpha.x * re - alpha.y * im, alpha.x * im + alpha.y * re);
           if (beta.x != 0.0f || beta.y != 0.0f) {
             const float2 o = *c;
             v.x += beta.x * o.x - beta.y * o.y;
@@ -285,6 +325,7 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
       }
     }
   }
+  __syncwarp();
   asm volatile("tcgen05.fence::before_thread_sync;");
   __syncthreads();
   if (warp == 1) {

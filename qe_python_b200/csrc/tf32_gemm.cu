@@ -299,6 +299,10 @@ int tf32_splits(int M, int N, int kp) {
   const int by_depth = ktiles / 8;       // at least 8 K tiles per slice
   if (s > by_depth) s = by_depth;
   if (s > 64) s = 64;
+  // at most 32 K tiles per tensor-memory accumulator: its FP32 additions
+  // lose accuracy with the chain length (see cgemm_tf32x3.cu)
+  const int by_chain = (ktiles + 31) / 32;
+  if (s < by_chain) s = by_chain;
   return s < 1 ? 1 : s;
 }
 

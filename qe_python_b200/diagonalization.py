@@ -26,6 +26,7 @@ from .device import (
     REAL_OF,
     as_numpy,
     empty_f,
+    leading_dimension,
     require_cuda,
     to_device_f,
     zeros_f,
@@ -238,6 +239,13 @@ class PlaneWaveHamiltonian:
         was_vector = vectors.dim() == 1
         if was_vector:
             vectors = vectors[:, None]
+        if self.tensor_gemm and vectors.shape[1] > 0 and \
+                (leading_dimension(vectors) % 2 or vectors.data_ptr() % 16):
+            # the split-TF32 GEMM reads 16-byte aligned columns: one copy here
+            # is cheaper than packing both projector operands
+            aligned = empty_f(vectors.shape[0], vectors.shape[1], self.dtype, self.device)
+            aligned.copy_(vectors)
+            vectors = aligned
         target = None
         if out is not None and isinstance(out, torch.Tensor):
             target = out[:, None] if out.dim() == 1 else out
@@ -471,19 +479,34 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
             projected[block, block] = _hermitize(projected[block, block])
             overlap[block, block] = _hermitize(overlap[block, block])
 
-    def ritz_pairs():
-        """Ritz values, vectors V c and residuals HV c - e V c (:699-726)."""
+    def ritz_values():
+        """Lowest roots and coefficients of the reduced problem (:699-708)."""
         with _timer(timers, "cdiaghg"):
             roots, coefficients = lowest_generalized_eigh(
                 projected[:active, :active], overlap[:active, :active], number_of_roots)
+        return roots.cpu().numpy(), roots, coefficients
+
+    def ritz_columns(coefficients, roots, columns=None):
+        """Ritz vectors V c and residuals HV c - e V c (:709-724) of the
+        selected roots (all when ``columns`` is None)."""
         with _timer(timers, "cegterg:upda"):
-            coeff = coefficients.to(dtype).T.contiguous().T
+            if columns is not None:
+                coefficients = coefficients.index_select(1, columns)
+                roots = roots.index_select(0, columns)
+            coeff = empty_f(coefficients.shape[0], coefficients.shape[1], dtype, device)
+            coeff.copy_(coefficients)
             vectors = K.gemm(K.OP_N, basis_storage[:, :active], coeff)
             residual = K.gemm(K.OP_N, applied_storage[:, :active], coeff)
             K.subtract_band_energies(residual, vectors, roots)
-        return roots.cpu().numpy(), roots, vectors, residual
+        return vectors, residual
 
+    # The reference forms all Ritz vectors and residuals after every reduced
+    # solve.  Only the residuals of the roots still unconverged feed the next
+    # correction block, so those are formed each iteration and the full Ritz
+    # block only where it is consumed (restart, return, residual-norm
+    # tracking); the values are the same columns of the same products.
     update_projected(0)
+    coefficients = None
     if initial_is_ritz:
         if initial_eigenvalues is None:
             values_dev = K.column_inner_products(
@@ -496,27 +519,30 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
         residuals = applied_storage[:, :number_of_roots].clone()
         K.subtract_band_energies(residuals, ritz_vectors, values_dev)
     else:
-        values, values_dev, ritz_vectors, residuals = ritz_pairs()
+        values, values_dev, coefficients = ritz_values()
+        ritz_vectors, residuals = ritz_columns(coefficients, values_dev)
     track = residual_factor is not None or residual_energy_scale is not None
 
     def residual_norms_of(block):
         return np.sqrt(np.maximum(K.column_squared_norms(block).cpu().numpy(), 0.0))
 
+    def full_ritz():
+        """(vectors, residuals) of every root for the current state."""
+        if coefficients is None:  # still the initial Ritz block
+            return ritz_vectors, residuals
+        return ritz_columns(coefficients, values_dev)
+
     residual_norms = residual_norms_of(residuals) if track else np.empty(number_of_roots)
     completed = 0
     unconverged_count = number_of_roots
     unconverged = np.ones(number_of_roots, dtype=bool)
+    # residual columns of the unconverged roots, in root order
+    block, energies = residuals, values_dev
 
     for iteration in range(1, max_iterations + 1):
         completed = iteration
         previous = values
         with _timer(timers, "g_psi"):
-            if unconverged.all():
-                block, energies = residuals, values_dev
-            else:
-                index = torch.as_tensor(np.flatnonzero(unconverged), device=device)
-                block = residuals.index_select(1, index).T.contiguous().T
-                energies = values_dev.index_select(0, index)
             corrections = K.precondition(block, energies, diag)
         # Normalise (cegterg), dropping columns below 1e-14 of the largest norm (:500-524).
         norms2 = K.column_squared_norms(corrections)
@@ -535,8 +561,10 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
         apply_into(basis_storage[:, old:active], applied_storage[:, old:active])
         applications += keep.size
         update_projected(old)
-        values, values_dev, ritz_vectors, residuals = ritz_pairs()
+        values, values_dev, coefficients = ritz_values()
+        ritz_vectors = residuals = None
         if track:
+            ritz_vectors, residuals = full_ritz()
             residual_norms = residual_norms_of(residuals)
         converged = np.abs(values - previous) < root_tolerances
         if residual_factor is not None:
@@ -546,12 +574,17 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
         unconverged = ~converged
         unconverged_count = int(np.count_nonzero(unconverged))
         if unconverged_count == 0:
+            if residuals is None:
+                ritz_vectors, residuals = full_ritz()
             if not track:
                 residual_norms = residual_norms_of(residuals)
             return DavidsonResult(values, ritz_vectors, residual_norms, iteration, True, 0,
                                   applications)
+        index = torch.as_tensor(np.flatnonzero(unconverged), device=device)
         if active + unconverged_count > maximum_subspace:
             # Restart on the Ritz block without a new H application (:843-868).
+            if residuals is None:
+                ritz_vectors, residuals = full_ritz()
             with _timer(timers, "cegterg:last"):
                 active = number_of_roots
                 basis_storage[:, :active] = ritz_vectors
@@ -560,6 +593,17 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
                 K.subtract_band_energies(applied_storage[:, :active], ritz_vectors, -values_dev)
                 projected[:active, :active] = torch.diag(values_dev.to(torch.complex128))
                 overlap[:active, :active] = torch.eye(active, dtype=torch.complex128, device=device)
+            coefficients = None  # the Ritz block is the basis itself now
+        if residuals is not None:
+            if unconverged.all():
+                block = residuals
+            else:
+                block = residuals.index_select(1, index).T.contiguous().T
+        else:
+            _, block = ritz_columns(coefficients, values_dev, index)
+        energies = values_dev.index_select(0, index)
+    if residuals is None:
+        ritz_vectors, residuals = full_ritz()
     if not track:
         residual_norms = residual_norms_of(residuals)
     return DavidsonResult(values, ritz_vectors, residual_norms, completed, False,

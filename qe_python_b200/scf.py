@@ -406,9 +406,18 @@ def projector_terms(system: System, tables: dict, basis) -> tuple:
     return tuple(terms)
 
 
+MIN_FP64_ITERATIONS = 3  # mixed form: FP64 iterations before convergence is accepted
+
+
 def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
-            progress=None) -> SCFResult:
-    """Converge the Kohn-Sham density to ``system.conv_thr`` (Ry) on the GPU."""
+            progress=None, timers=None, pools=None) -> SCFResult:
+    """Converge the Kohn-Sham density to ``system.conv_thr`` (Ry) on the GPU.
+
+    ``timers``: optional object with a ``measure(name)`` context manager,
+    handed to the Hamiltonian and Davidson (the reference's timer names).
+    ``pools``: optional qe_python_b200.pools.KPointPools; each rank then
+    solves its own k points and the density, eigenvalues and nonlocal
+    forces are combined over the pools."""
     if precision not in ("f64", "mixed"):
         raise ValueError("precision must be 'f64' or 'mixed'")
     device = require_cuda()
@@ -458,6 +467,9 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
              else DeviceBroydenMixer(cgrid, system.mixing_beta, system.mixing_ndim,
                                      system.mixing_mode, nelec, volume))
     states = [KPointState(b, shape, device) for b in bases]
+    nk = len(states)
+    local_k = list(pools.local_kpoints(nk)) if pools is not None else list(range(nk))
+    random_drawn = [False] * nk
     rng = QERandom()
     davidson_tolerance = 0.5 * 1.0e-2  # diago_thr_init 1e-2 Ry -> Ha
     previous_accuracy = np.inf
@@ -485,25 +497,40 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
                                                   0.1 * previous_accuracy / max(1.0, nelec)))
         if precision == "mixed" and current_precision == "f32" and np.isfinite(previous_accuracy) \
                 and 2.0 * previous_accuracy < switch_ry:
+            # FP64 from here on.  The Broyden secant pairs of the FP32
+            # iterations describe a slightly different fixed point and the
+            # Davidson threshold was tightened against FP32 residuals: start
+            # both afresh from the current density.
             current_precision = "f64"
+            if isinstance(mixer, DeviceBroydenMixer):
+                mixer.reset()
+            davidson_tolerance = max(5.0e-14, 0.1 * previous_accuracy / max(1.0, nelec))
         # FP32 eigenvalues stall near 1e-7 relative: never ask more of them
         tol = davidson_tolerance if current_precision == "f64" else max(davidson_tolerance, 2.0e-6)
         precision_log.append(current_precision)
         tick("v_of_rho", t0)
         t0 = time.perf_counter()
-        eigenvalues = []
+        local_eigenvalues = {}
         its = []
-        for state, weight in zip(states, system.weights):
+        for k, state in enumerate(states):
+            if k not in local_k:
+                if state.vectors is None and iteration == 1 and not random_drawn[k]:
+                    # keep the shared random stream in step with one rank
+                    rng.pairs(len(state.basis), system.nbnd)
+                    random_drawn[k] = True
+                continue
             ws = state.workspace(current_precision)
             if state.terms is None:
                 state.terms = projector_terms(system, tables, state.basis)
             ham = PlaneWaveHamiltonian(state.basis, None, state.terms, local_workspace=ws,
-                                       real_potential=v_dev, potential_average=v_ion_average)
+                                       real_potential=v_dev, potential_average=v_ion_average,
+                                       timers=timers)
             initial_applied = None
             initial_eigs = None
             if state.vectors is None:
                 start_vectors, initial_eigs, initial_applied = random_starting_subspace(
                     ham, state.basis, rng, system.nbnd)
+                random_drawn[k] = True
             else:
                 start_vectors = state.vectors.to(ham.dtype).T.contiguous().T
             # first SCF iteration: rotate_wfc Ritz vectors (or the first
@@ -521,7 +548,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
                                residual_energy_scale=None, occupied_roots=occ_roots,
                                initial_is_ritz=is_ritz, initial_is_orthonormal=True,
                                initial_eigenvalues=retry_eigs, initial_applied=retry_applied,
-                               operator_into=ham.apply_into, dtype=ham.dtype)
+                               operator_into=ham.apply_into, dtype=ham.dtype, timers=timers)
                 attempt += 1
                 total_its += sol.iterations
                 if sol.converged or sol.number_unconverged <= 5 or attempt >= 6:
@@ -530,8 +557,14 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             its.append(total_its)
             state.vectors = sol.eigenvectors.to(torch.complex128).T.contiguous().T
             state.eigenvalues = np.asarray(sol.eigenvalues)
-            eigenvalues.append(state.eigenvalues)
+            local_eigenvalues[k] = state.eigenvalues
         david_its.append(float(np.mean(its)))
+        if pools is not None:
+            eigenvalues = pools.gather_eigenvalues(nk, local_eigenvalues, system.nbnd, device)
+            for k, values in enumerate(eigenvalues):
+                states[k].eigenvalues = values
+        else:
+            eigenvalues = [local_eigenvalues[k] for k in range(nk)]
         torch.cuda.synchronize()
         tick("c_bands", t0)
         t0 = time.perf_counter()
@@ -544,7 +577,8 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         # density from the occupied states (FP64 accumulation on the GPU),
         # bands up to the last one with a nonzero occupation (scf.py:1406-1431)
         rho_device.zero_()
-        for state, weight, occ in zip(states, system.weights, band_occ):
+        for k in local_k:
+            state, weight, occ = states[k], system.weights[k], band_occ[k]
             active = np.flatnonzero(np.abs(occ) > 1.0e-15)
             if active.size == 0:
                 continue
@@ -552,6 +586,8 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             ws = state.workspace("f64")
             w = torch.from_numpy(float(weight) * occ[:count] / volume).to(device)
             ws.accumulate_density(rho_device, state.vectors[:, :count], w)
+        if pools is not None:
+            pools.sum_(rho_device)
         rho_out = rho_device * (nelec * grid.size / (float(torch.sum(rho_device)) * volume))
         if symmetrizer is not None:
             sym = symmetrizer.apply(rho_out.cpu().numpy())
@@ -570,7 +606,14 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             continue
         first_diagonalization = False
         t0 = time.perf_counter()
-        converged = 2.0 * accuracy < system.conv_thr
+        # The mixed form finishes in FP64, with at least MIN_FP64_ITERATIONS
+        # FP64 iterations: the residual metric weights |drho(G)|^2 by 1/G^2
+        # and hardly sees the high-G density noise of the FP32 iterations,
+        # which mixing removes only a factor (1 - beta) per iteration, while
+        # V_xc passes it on to the eigenvalues.
+        fp64_done = sum(1 for p in precision_log if p == "f64")
+        converged = 2.0 * accuracy < system.conv_thr and current_precision == "f64" and \
+            (precision == "f64" or fp64_done >= MIN_FP64_ITERATIONS)
         if converged:
             rho_energy = rho_out
         elif isinstance(mixer, DeviceBroydenMixer):
@@ -604,7 +647,10 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         from .forces import hellmann_feynman_forces
 
         t0 = time.perf_counter()
-        forces = hellmann_feynman_forces(system, states, tables, grid, rho, band_occ)
+        forces = hellmann_feynman_forces(system, [states[k] for k in local_k], tables, grid, rho,
+                                         [band_occ[k] for k in local_k],
+                                         weights=[system.weights[k] for k in local_k],
+                                         pools=pools)
         tick("forces", t0)
     return SCFResult(converged, total, iteration, energies, accuracies,
                      [s.eigenvalues for s in states], energy_terms, rho, forces,
