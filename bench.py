@@ -56,6 +56,9 @@ def parse_args():
     p.add_argument("--impl", choices=("b200", "reference"), default="b200")
     p.add_argument("--bands", type=int, default=256)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--apply-only", choices=("f32", "f64"), default=None,
+                   help="profiling driver: build the workload, apply H|psi> --steps times "
+                        "in the given precision, print a checksum, no timing")
     p.add_argument("--cpu-seconds", type=float, default=10.0,
                    help="approximate CPU time budget of the cpu_baseline sample")
     p.add_argument("--scf", default="scf-fcc2",
@@ -390,18 +393,21 @@ def run_b200(args) -> None:
 
     # end to end through the public API with pinned host buffers
     ws, ham, psi_dev, _ = forms["mixed"]
-    # column-major pinned host buffers: the copies are single contiguous DMAs
-    host_in = torch.from_numpy(np.ascontiguousarray(work.psi.T.astype(np.complex64))).pin_memory().T
-    host_out = torch.empty((nb, npw), dtype=torch.complex64, pin_memory=True).T
+    # pinned host buffers with the graph buffers' (nbands, ld) storage shape:
+    # each copy is one contiguous DMA
+    ld = mixed_graph.input_storage.shape[1]
+    host_in_storage = torch.zeros((nb, ld), dtype=torch.complex64).pin_memory()
+    host_in_storage[:, :npw] = torch.from_numpy(work.psi.T.astype(np.complex64))
+    host_out_storage = torch.empty((nb, ld), dtype=torch.complex64, pin_memory=True)
     e2e_times = []
     for i in range(args.warmup + args.steps):
         flush.fill_(1.0)
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(stream)
-        mixed_graph.input.copy_(host_in, non_blocking=True)
+        mixed_graph.input_storage.copy_(host_in_storage, non_blocking=True)
         mixed_graph.replay()
-        host_out.copy_(mixed_graph.output, non_blocking=True)
+        host_out_storage.copy_(mixed_graph.output_storage, non_blocking=True)
         b.record(stream)
         torch.cuda.synchronize()
         if i >= args.warmup:
@@ -484,7 +490,8 @@ def run_b200(args) -> None:
         "roofline": roofline,
         "gpu_launches": int(launches),
         "e2e": {"value": world * nb / (e2e_ms / 1e3), "unit": "bands/s",
-                "h2d_bytes_per_step": npw * nb * 8, "d2h_bytes_per_step": npw * nb * 8},
+                "h2d_bytes_per_step": host_in_storage.numel() * 8,
+                "d2h_bytes_per_step": host_out_storage.numel() * 8},
         "clocks": graph_clocks.summary(),
         "clocks_staged": clocks.summary(),
     }
@@ -507,8 +514,36 @@ def run_b200(args) -> None:
         dist.destroy_process_group()
 
 
+def apply_only(args) -> None:
+    """One workload, ``args.steps`` H|psi> applications, nothing timed: the
+    command line the ncu captures under profiles/ use."""
+    import torch
+
+    from qe_python_b200.basis import LocalPotentialWorkspace, make_bases
+    from qe_python_b200.device import to_device_f
+    from qe_python_b200.diagonalization import PlaneWaveHamiltonian
+    from qe_python_b200.workloads import hpsi_microbench
+
+    work = hpsi_microbench(nbands=args.bands)
+    basis = make_bases(work.reciprocal, np.zeros(3), 30.0)[0]
+    ws = LocalPotentialWorkspace(basis, work.shape, precision=args.apply_only)
+    ham = PlaneWaveHamiltonian(basis, None, ((work.beta, work.coupling),), local_workspace=ws,
+                               real_potential=torch.from_numpy(work.potential).cuda(),
+                               potential_average=0.0)
+    psi = to_device_f(work.psi, ham.dtype, ham.device)
+    out = None
+    for _ in range(max(1, args.steps)):
+        out = ham.apply(psi)
+    torch.cuda.synchronize()
+    print(json.dumps({"apply_only": args.apply_only, "applications": max(1, args.steps),
+                      "checksum": float(out.abs().sum())}))
+
+
 def main():
     args = parse_args()
+    if args.apply_only is not None:
+        apply_only(args)
+        return
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":

@@ -88,6 +88,21 @@ int qeb_apply_local_profiled(const qeb_local_plan* plan, void* scratch, int64_t 
                              const void* potential_native, const void* kinetic, void* out,
                              int64_t ld_out, void* stream, float* pass_ms);
 
+/* qeb_apply_local for nk <= 16 k points on one grid in one launch per pass
+ * (grid.z = k point): plans[k], psi[k] (ld_psi[k], nbands[k] columns),
+ * kinetic[k] (may be NULL), out[k] (ld_out[k]); one potential.  The k points'
+ * stick buffers are carved from one scratch of qeb_local_multi_scratch_bytes()
+ * bytes.  Chosen-form batching of the per-k apply_serial_spatial calls of
+ * qepy_pw/pw/scf.py:3396-3411 (no counterpart in the reference).  Grids
+ * without a four-step factorisation run one launch sequence per k point. */
+int64_t qeb_local_multi_scratch_bytes(int nk, const qeb_local_plan* const* plans,
+                                      const int64_t* nbands);
+int qeb_apply_local_multi(int nk, const qeb_local_plan* const* plans, void* scratch,
+                          int64_t scratch_bytes, const void* const* psi, const int64_t* ld_psi,
+                          const int64_t* nbands, const void* potential_native,
+                          const void* const* kinetic, void* const* out, const int64_t* ld_out,
+                          void* stream);
+
 /* density[(x*ny + y)*nz + z] += sum_b weights[b] |FFT^+(psi[:, b])(x,y,z)|^2
  * (float64 accumulation; weights is a device float64 array of nbands).
  * Replaces accumulate_density_serial(_spatial)
@@ -201,6 +216,14 @@ int64_t qeb_cgemm_tf32x3_scratch_bytes(int op_a, int M, int N, int K);
 int qeb_cgemm_tf32x3(int op_a, int M, int N, int K, const double* alpha, const void* A,
                      int64_t lda, const void* B, int64_t ldb, const double* beta, void* C,
                      int64_t ldc, void* scratch, int64_t scratch_bytes, void* stream);
+/* The same with the K split chosen by the caller (splits <= 0: the built-in
+ * choice, qeb_cgemm_tf32x3_default_splits); a split needs splits*M*N*8 bytes
+ * of scratch, less lowers it. */
+int qeb_cgemm_tf32x3_default_splits(int op_a, int M, int N, int K);
+int qeb_cgemm_tf32x3_ex(int op_a, int M, int N, int K, const double* alpha, const void* A,
+                        int64_t lda, const void* B, int64_t ldb, const double* beta, void* C,
+                        int64_t ldc, void* scratch, int64_t scratch_bytes, int splits,
+                        void* stream);
 
 /* ------------------------------------------------------------------------
  * Davidson column kernels (precision QEB_F64 / QEB_F32 selects the vector

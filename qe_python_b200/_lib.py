@@ -41,6 +41,8 @@ SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_apply_local", _I, [_P, _P, _L, _P, _L, _L, _P, _P, _P, _L, _P]),
     ("qeb_apply_local_profiled", _I, [_P, _P, _L, _P, _L, _L, _P, _P, _P, _L, _P, _P]),
     ("qeb_accumulate_density", _I, [_P, _P, _L, _P, _L, _L, _P, _P, _P]),
+    ("qeb_local_multi_scratch_bytes", _L, [_I, _P, _P]),
+    ("qeb_apply_local_multi", _I, [_I, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P, _P]),
     ("qeb_zgemm_scratch_bytes", _L, [_I, _I, _I, _I, _I]),
     ("qeb_zgemm", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
     ("qeb_cgemm", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
@@ -54,6 +56,8 @@ SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_tf32_gemm_error", _I, [_P]),
     ("qeb_cgemm_tf32x3_scratch_bytes", _L, [_I, _I, _I, _I]),
     ("qeb_cgemm_tf32x3", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
+    ("qeb_cgemm_tf32x3_default_splits", _I, [_I, _I, _I, _I]),
+    ("qeb_cgemm_tf32x3_ex", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _I, _P]),
     ("qeb_column_squared_norms", _I, [_I, _L, _L, _P, _L, _P, _P]),
     ("qeb_column_diagonal_expectations", _I, [_I, _L, _L, _P, _L, _P, _P, _P]),
     ("qeb_column_inner_products", _I, [_I, _L, _L, _P, _L, _P, _L, _P, _P]),

@@ -1,0 +1,78 @@
+"""Launch-shape selection by measurement.
+
+The first time a kernel family meets a new problem class (a key built from
+the sizes that change its best shape), each candidate shape is run and timed
+with CUDA events on the current stream, and the fastest is kept for the rest
+of the process; QEB_AUTOTUNE_CACHE=<file.json> keeps the table across runs.
+Tuned choices:
+  * the band batch of one local H|psi> launch (the stick buffer of a batch
+    that fits the 126 MB L2 is re-read from L2 by pass B and pass C);
+  * the K split of the split-TF32 GEMM (CTAs per output tile) and whether a
+    mid-sized complex64 product runs on the tensor cores or the FP32 pipes.
+Inside CUDA-graph capture nothing is timed: a known choice is used, else the
+first candidate (the kernels' own default).  QEB_AUTOTUNE=0 turns timing off
+(always the first candidate), e.g. for profiler captures.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+import threading
+
+import torch
+
+
+class Autotuner:
+    def __init__(self, path: str | None = None, repeats: int = 3) -> None:
+        self.path = path
+        self.repeats = int(repeats)
+        self.table: dict[str, object] = {}
+        self.timings: dict[str, dict[str, float]] = {}
+        self._lock = threading.Lock()
+        self.enabled = os.environ.get("QEB_AUTOTUNE", "1") != "0"
+        if path and os.path.exists(path):
+            with open(path) as handle:
+                self.table = json.load(handle)
+
+    def choose(self, key: str, candidates: list, run) -> object:
+        """The fastest candidate for ``key``; ``run(candidate)`` launches the
+        work on the current stream (it may run several times)."""
+        if not candidates:
+            raise ValueError("no candidates")
+        known = self.table.get(key)
+        if known in candidates:
+            return known
+        if len(candidates) == 1 or not self.enabled or not torch.cuda.is_available() or \
+                torch.cuda.is_current_stream_capturing():
+            return candidates[0]
+        with self._lock:
+            stream = torch.cuda.current_stream()
+            for c in candidates:  # warm-up: first-use allocations, caches
+                run(c)
+            times = {}
+            for c in candidates:
+                start = torch.cuda.Event(enable_timing=True)
+                end = torch.cuda.Event(enable_timing=True)
+                torch.cuda.synchronize()
+                start.record(stream)
+                for _ in range(self.repeats):
+                    run(c)
+                end.record(stream)
+                end.synchronize()
+                times[c] = start.elapsed_time(end) / self.repeats
+            best = min(candidates, key=lambda c: times[c])
+            self.table[key] = best
+            self.timings[key] = {str(c): t for c, t in times.items()}
+            if self.path:
+                with open(self.path, "w") as handle:
+                    json.dump(self.table, handle, indent=1, sort_keys=True)
+        return best
+
+
+def bucket(n: int) -> int:
+    """Smallest power of two >= n (problem-size class of a tuning key)."""
+    return 1 << max(0, int(n - 1).bit_length())
+
+
+TUNER = Autotuner(os.environ.get("QEB_AUTOTUNE_CACHE"))

@@ -24,6 +24,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .autotune import TUNER, bucket
 from .device import (
     REAL_OF,
     as_numpy,
@@ -453,8 +454,22 @@ class LocalPotentialWorkspace:
         nb = vectors.shape[1]
         if nb == 0:
             return
-        batch = nb if self.serial_fft_batch_size is None else max(1, int(self.serial_fft_batch_size))
-        batch = min(batch, 65535)
+        if self.serial_fft_batch_size is not None:
+            batch = max(1, int(self.serial_fft_batch_size))
+        elif self.pass_times is not None or nb <= 32:
+            batch = nb
+        else:
+            # bands per launch, by measurement: a batch whose stick buffer
+            # stays in L2 between the passes can beat one launch of all bands
+            top = bucket(nb)
+            candidates = [top] + [b for b in (256, 128, 64, 32) if b < top]
+            key = f"local_apply/{self.precision}/{self.shape}/{self.plane_waves}/{top}"
+            batch = TUNER.choose(key, candidates, lambda b: self._run_apply(
+                potential, vectors, kinetic, target, min(b, nb)))
+        self._run_apply(potential, vectors, kinetic, target, min(batch, nb, 65535))
+
+    def _run_apply(self, potential, vectors, kinetic, target, batch: int) -> None:
+        nb = vectors.shape[1]
         lib = _lib.load()
         stream = stream_handle()
         ld_in, ld_out = leading_dimension(vectors), leading_dimension(target)
@@ -527,3 +542,36 @@ def apply_local_potential(vg: np.ndarray, indices: np.ndarray, coefficients: np.
     """V psi through the GPU workspace (qepy_pw/basis.py:1691-1698)."""
     workspace = LocalPotentialWorkspace(indices, vg.shape)
     return workspace.apply(workspace.prepare_potential(vg), coefficients)
+
+
+_MULTI_SCRATCH = FFTScratchPool()
+
+
+def apply_local_multi(workspaces, potential: torch.Tensor, vectors, kinetics, targets) -> None:
+    """targets[k] = (T_k + V) vectors[k] for several k points on one grid, one
+    launch per FFT pass (qeb_apply_local_multi; at most 16 k points per call,
+    more are taken 16 at a time).  ``potential`` is the native (nz, nx, ny)
+    grid in the workspaces' precision; ``kinetics[k]`` may be None."""
+    nk_all = len(workspaces)
+    if not (len(vectors) == len(kinetics) == len(targets) == nk_all):
+        raise ValueError("one vector block, kinetic term and target per workspace")
+    lib = _lib.load()
+    stream = stream_handle()
+    for start in range(0, nk_all, 16):
+        part = range(start, min(nk_all, start + 16))
+        nk = len(part)
+        plans = (ctypes.c_void_p * nk)(*[workspaces[k]._plan.value for k in part])
+        nbands = (ctypes.c_int64 * nk)(*[vectors[k].shape[1] for k in part])
+        need = int(lib.qeb_local_multi_scratch_bytes(nk, plans, nbands))
+        if need < 0:
+            raise ValueError("invalid plans or band counts")
+        scratch = _MULTI_SCRATCH.buffer("sticks", max(need, 256), workspaces[start].device)
+        psi = (ctypes.c_void_p * nk)(*[vectors[k].data_ptr() for k in part])
+        ld_psi = (ctypes.c_int64 * nk)(*[leading_dimension(vectors[k]) for k in part])
+        kin = (ctypes.c_void_p * nk)(*[0 if kinetics[k] is None else kinetics[k].data_ptr()
+                                       for k in part])
+        out = (ctypes.c_void_p * nk)(*[targets[k].data_ptr() for k in part])
+        ld_out = (ctypes.c_int64 * nk)(*[leading_dimension(targets[k]) for k in part])
+        _lib.check("qeb_apply_local_multi", lib.qeb_apply_local_multi(
+            nk, plans, scratch.data_ptr(), need, psi, ld_psi, nbands, potential.data_ptr(), kin,
+            out, ld_out, stream))

@@ -399,11 +399,12 @@ int choose_splits(int M, int N, int K) {
 
 template <int OP>
 int launch(const Maps& maps, int M, int N, int K, float2 al, float2 be, float2* C, int64_t ldc,
-           void* scratch, int64_t scratch_bytes, int* err, cudaStream_t s) {
+           void* scratch, int64_t scratch_bytes, int requested_splits, int* err, cudaStream_t s) {
   cudaError_t e = qeb::raise_smem_limit(cgemm_tf32x3_kernel<OP>, smem_bytes<OP>());
   if (e != cudaSuccess) return qeb::cuda_status(e, "cgemm_tf32x3 shared-memory limit");
   const int kblocks = (2 * K + BKF - 1) / BKF;
-  int splits = choose_splits(M, N, K);
+  int splits = requested_splits > 0 ? (requested_splits < kblocks ? requested_splits : kblocks)
+                                    : choose_splits(M, N, K);
   const int64_t slice = (int64_t)M * N * 8;
   if (splits > 1 && (scratch == nullptr || scratch_bytes < splits * slice)) {
     const int64_t fit = scratch == nullptr ? 0 : scratch_bytes / slice;
@@ -427,6 +428,12 @@ int launch(const Maps& maps, int M, int N, int K, float2 al, float2 be, float2* 
 
 }  // namespace
 
+extern "C" int qeb_cgemm_tf32x3_default_splits(int op_a, int M, int N, int K) {
+  (void)op_a;
+  if (M <= 0 || N <= 0 || K <= 0) return 1;
+  return choose_splits(M, N, K);
+}
+
 extern "C" int64_t qeb_cgemm_tf32x3_scratch_bytes(int op_a, int M, int N, int K) {
   (void)op_a;
   if (M <= 0 || N <= 0 || K <= 0) return 0;
@@ -438,6 +445,14 @@ extern "C" int qeb_cgemm_tf32x3(int op_a, int M, int N, int K, const double* alp
                                 int64_t lda, const void* B, int64_t ldb, const double* beta,
                                 void* C, int64_t ldc, void* scratch, int64_t scratch_bytes,
                                 void* stream) {
+  return qeb_cgemm_tf32x3_ex(op_a, M, N, K, alpha, A, lda, B, ldb, beta, C, ldc, scratch,
+                             scratch_bytes, 0, stream);
+}
+
+extern "C" int qeb_cgemm_tf32x3_ex(int op_a, int M, int N, int K, const double* alpha,
+                                   const void* A, int64_t lda, const void* B, int64_t ldb,
+                                   const double* beta, void* C, int64_t ldc, void* scratch,
+                                   int64_t scratch_bytes, int splits, void* stream) {
   if ((op_a != QEB_OP_N && op_a != QEB_OP_C) || M < 0 || N < 0 || K < 0 || alpha == nullptr ||
       beta == nullptr || ldc < (M > 0 ? M : 1) || ldb < (K > 0 ? K : 1) ||
       lda < (op_a == QEB_OP_N ? (M > 0 ? M : 1) : (K > 0 ? K : 1))) {
@@ -475,6 +490,7 @@ extern "C" int qeb_cgemm_tf32x3(int op_a, int M, int N, int K, const double* alp
   const float2 be = make_float2((float)beta[0], (float)beta[1]);
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   float2* c = static_cast<float2*>(C);
-  return op_a == QEB_OP_C ? launch<QEB_OP_C>(maps, M, N, K, al, be, c, ldc, scratch, scratch_bytes, err, s)
-                          : launch<QEB_OP_N>(maps, M, N, K, al, be, c, ldc, scratch, scratch_bytes, err, s);
+  return op_a == QEB_OP_C
+             ? launch<QEB_OP_C>(maps, M, N, K, al, be, c, ldc, scratch, scratch_bytes, splits, err, s)
+             : launch<QEB_OP_N>(maps, M, N, K, al, be, c, ldc, scratch, scratch_bytes, splits, err, s);
 }

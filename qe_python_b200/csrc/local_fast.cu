@@ -82,19 +82,18 @@ size_t b_smem(const qeb_local_plan* p) {
 
 // ---------------------------------------------------------------------------
 template <typename T, class F>
-__global__ void __launch_bounds__(kThreads) four_pass_a(
+__device__ __forceinline__ void pass_a_body(
     const C2<T>* __restrict__ psi, int64_t ld, int nst, int nz_pad,
     const int32_t* __restrict__ entry_g, const int32_t* __restrict__ entry_z,
     const int32_t* __restrict__ entry_stick, const int32_t* __restrict__ stick_off,
-    const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks) {
+    const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks, int block_x, int64_t band) {
   constexpr int nz = F::n;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2<T>* lines = reinterpret_cast<C2<T>*>(smem_raw);
   C2<T>* tw = lines + kSticksPerBlock * nz_pad;
   C2<T>* xbuf = tw + nz;
-  const int s0 = blockIdx.x * kSticksPerBlock;
+  const int s0 = block_x * kSticksPerBlock;
   const int nsl = min(kSticksPerBlock, nst - s0);
-  const int64_t band = blockIdx.y;
   for (int i = threadIdx.x; i < nz; i += kThreads) tw[i] = tw_z[i];
   for (int i = threadIdx.x; i < kSticksPerBlock * nz_pad; i += kThreads) lines[i] = qeb::mk<T>(0, 0);
   __syncthreads();
@@ -130,20 +129,19 @@ __global__ void __launch_bounds__(kThreads) four_pass_a(
 }
 
 template <typename T, class F>
-__global__ void __launch_bounds__(kThreads) four_pass_c(
+__device__ __forceinline__ void pass_c_body(
     const C2<T>* __restrict__ sticks, int nst, int nz_pad, const int32_t* __restrict__ entry_g,
     const int32_t* __restrict__ entry_z, const int32_t* __restrict__ entry_stick,
     const int32_t* __restrict__ stick_off, const C2<T>* __restrict__ tw_z,
     const C2<T>* __restrict__ psi, int64_t ld, const T* __restrict__ kinetic, T inv_n,
-    C2<T>* __restrict__ out, int64_t ldo) {
+    C2<T>* __restrict__ out, int64_t ldo, int block_x, int64_t band) {
   constexpr int nz = F::n;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2<T>* lines = reinterpret_cast<C2<T>*>(smem_raw);
   C2<T>* tw = lines + kSticksPerBlock * nz_pad;
   C2<T>* xbuf = tw + nz;
-  const int s0 = blockIdx.x * kSticksPerBlock;
+  const int s0 = block_x * kSticksPerBlock;
   const int nsl = min(kSticksPerBlock, nst - s0);
-  const int64_t band = blockIdx.y;
   for (int i = threadIdx.x; i < nz; i += kThreads) tw[i] = tw_z[i];
   const C2<T>* in = sticks + band * (int64_t)nz * nst;
   for (int i = threadIdx.x; i < nz * nsl; i += kThreads) {
@@ -188,19 +186,17 @@ __global__ void __launch_bounds__(kThreads) four_pass_c(
 
 // MODE 0: local potential; MODE 1: density accumulation.
 template <typename T, class F, int MODE>
-__global__ void __launch_bounds__(kThreads) four_pass_b(
+__device__ __forceinline__ void pass_b_body(
     C2<T>* __restrict__ sticks, int nst, int nz, int nay, int nx_pad,
     const int32_t* __restrict__ stick_pos, const int32_t* __restrict__ y_to_ay,
     const C2<T>* __restrict__ tw_xy, const T* __restrict__ potential,
-    const double* __restrict__ weights, double* __restrict__ density) {
+    const double* __restrict__ weights, double* __restrict__ density, int z, int64_t band) {
   constexpr int n = F::n;  // nx == ny
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2<T>* plane = reinterpret_cast<C2<T>*>(smem_raw);  // [nay][nx_pad]
   C2<T>* tw = plane + (size_t)nay * nx_pad;
   C2<T>* xbuf = tw + n;
   int* yay = reinterpret_cast<int*>(xbuf + kWarps * F::per_warp * F::scratch);
-  const int z = blockIdx.x;
-  const int64_t band = blockIdx.y;
   for (int i = threadIdx.x; i < n; i += kThreads) {
     tw[i] = tw_xy[i];
     yay[i] = y_to_ay[i];
@@ -294,6 +290,93 @@ __global__ void __launch_bounds__(kThreads) four_pass_b(
   for (int s = threadIdx.x; s < nst; s += kThreads) srow[s] = plane[stick_pos[s]];
 }
 
+// ---------------------------------------------------------------------------
+// Launch wrappers: one plan (grid.x, grid.y = blocks, bands) or a batch of
+// k points on the same grid (grid.z = k; blocks past a k point's sticks or
+// bands return at once).
+
+template <typename T, class F>
+__global__ void __launch_bounds__(kThreads) four_pass_a(
+    const C2<T>* __restrict__ psi, int64_t ld, int nst, int nz_pad,
+    const int32_t* __restrict__ entry_g, const int32_t* __restrict__ entry_z,
+    const int32_t* __restrict__ entry_stick, const int32_t* __restrict__ stick_off,
+    const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks) {
+  pass_a_body<T, F>(psi, ld, nst, nz_pad, entry_g, entry_z, entry_stick, stick_off, tw_z, sticks,
+                    blockIdx.x, blockIdx.y);
+}
+
+template <typename T, class F>
+__global__ void __launch_bounds__(kThreads) four_pass_c(
+    const C2<T>* __restrict__ sticks, int nst, int nz_pad, const int32_t* __restrict__ entry_g,
+    const int32_t* __restrict__ entry_z, const int32_t* __restrict__ entry_stick,
+    const int32_t* __restrict__ stick_off, const C2<T>* __restrict__ tw_z,
+    const C2<T>* __restrict__ psi, int64_t ld, const T* __restrict__ kinetic, T inv_n,
+    C2<T>* __restrict__ out, int64_t ldo) {
+  pass_c_body<T, F>(sticks, nst, nz_pad, entry_g, entry_z, entry_stick, stick_off, tw_z, psi, ld,
+                    kinetic, inv_n, out, ldo, blockIdx.x, blockIdx.y);
+}
+
+template <typename T, class F, int MODE>
+__global__ void __launch_bounds__(kThreads) four_pass_b(
+    C2<T>* __restrict__ sticks, int nst, int nz, int nay, int nx_pad,
+    const int32_t* __restrict__ stick_pos, const int32_t* __restrict__ y_to_ay,
+    const C2<T>* __restrict__ tw_xy, const T* __restrict__ potential,
+    const double* __restrict__ weights, double* __restrict__ density) {
+  pass_b_body<T, F, MODE>(sticks, nst, nz, nay, nx_pad, stick_pos, y_to_ay, tw_xy, potential,
+                          weights, density, blockIdx.x, blockIdx.y);
+}
+
+template <typename T>
+struct KDesc {
+  const C2<T>* psi;
+  C2<T>* out;
+  const T* kinetic;
+  C2<T>* sticks;
+  const int32_t* entry_g;
+  const int32_t* entry_z;
+  const int32_t* entry_stick;
+  const int32_t* stick_off;
+  const int32_t* stick_pos;
+  const int32_t* y_to_ay;
+  int64_t ld, ldo;
+  int nst, nay, nb;
+};
+
+template <typename T>
+struct KBatch {
+  KDesc<T> k[QEB_MAX_KBATCH];
+};
+
+template <typename T, class F>
+__global__ void __launch_bounds__(kThreads) four_pass_a_multi(const __grid_constant__ KBatch<T> kb,
+                                                              int nz_pad, const C2<T>* tw_z) {
+  const KDesc<T>& d = kb.k[blockIdx.z];
+  if ((int)blockIdx.x * kSticksPerBlock >= d.nst || (int)blockIdx.y >= d.nb) return;
+  pass_a_body<T, F>(d.psi, d.ld, d.nst, nz_pad, d.entry_g, d.entry_z, d.entry_stick, d.stick_off,
+                    tw_z, d.sticks, blockIdx.x, blockIdx.y);
+}
+
+template <typename T, class F>
+__global__ void __launch_bounds__(kThreads) four_pass_b_multi(const __grid_constant__ KBatch<T> kb,
+                                                              int nz, int nx_pad,
+                                                              const C2<T>* tw_xy,
+                                                              const T* potential) {
+  const KDesc<T>& d = kb.k[blockIdx.z];
+  if ((int)blockIdx.y >= d.nb) return;
+  pass_b_body<T, F, 0>(d.sticks, d.nst, nz, d.nay, nx_pad, d.stick_pos, d.y_to_ay, tw_xy,
+                       potential, nullptr, nullptr, blockIdx.x, blockIdx.y);
+}
+
+template <typename T, class F>
+__global__ void __launch_bounds__(kThreads) four_pass_c_multi(const __grid_constant__ KBatch<T> kb,
+                                                              int nz_pad, const C2<T>* tw_z,
+                                                              T inv_n) {
+  const KDesc<T>& d = kb.k[blockIdx.z];
+  if ((int)blockIdx.x * kSticksPerBlock >= d.nst || (int)blockIdx.y >= d.nb) return;
+  pass_c_body<T, F>(d.sticks, d.nst, nz_pad, d.entry_g, d.entry_z, d.entry_stick, d.stick_off,
+                    tw_z, d.psi, d.ld, d.kinetic, inv_n, d.out, d.ldo, blockIdx.x, blockIdx.y);
+}
+
 template <typename T>
 const C2<T>* tw_at(const qeb_local_plan* p, int which) {
   const C2<T>* base = static_cast<const C2<T>*>(p->tw);
@@ -324,6 +407,10 @@ struct SetLimits {
       err = qeb::raise_smem_limit(four_pass_a<T, F>, s);
       if (err == cudaSuccess)
         err = qeb::raise_smem_limit(four_pass_c<T, F>, s);
+      if (err == cudaSuccess)
+        err = qeb::raise_smem_limit(four_pass_a_multi<T, F>, s);
+      if (err == cudaSuccess)
+        err = qeb::raise_smem_limit(four_pass_c_multi<T, F>, s);
     }
     if (err == cudaSuccess && p->fast_xy >= 0 && F::n == p->nx) {
       const size_t s = b_smem<T, F>(p);
@@ -334,6 +421,8 @@ struct SetLimits {
       err = qeb::raise_smem_limit(four_pass_b<T, F, 0>, s);
       if (err == cudaSuccess)
         err = qeb::raise_smem_limit(four_pass_b<T, F, 1>, s);
+      if (err == cudaSuccess)
+        err = qeb::raise_smem_limit(four_pass_b_multi<T, F>, s);
     }
     return qeb::cuda_status(err, "four-step shared memory attribute");
   }
@@ -380,6 +469,101 @@ struct PassB {
     return QEB_OK;
   }
 };
+
+template <typename T>
+struct PassAMulti {
+  const KBatch<T>* kb; const qeb_local_plan* p0; int nk; int sblocks; int nb; cudaStream_t s;
+  template <class F>
+  int operator()() const {
+    const dim3 grid(sblocks, (unsigned)nb, (unsigned)nk);
+    four_pass_a_multi<T, F><<<grid, kThreads, ac_smem<T, F>(p0->nz_pad), s>>>(*kb, p0->nz_pad,
+                                                                             tw_at<T>(p0, 2));
+    return QEB_OK;
+  }
+};
+
+template <typename T>
+struct PassBMulti {
+  const KBatch<T>* kb; const qeb_local_plan* p0; int nk; int nb; size_t smem; const T* potential;
+  cudaStream_t s;
+  template <class F>
+  int operator()() const {
+    const dim3 grid(p0->nz, (unsigned)nb, (unsigned)nk);
+    four_pass_b_multi<T, F><<<grid, kThreads, smem, s>>>(*kb, p0->nz, p0->nx_pad, tw_at<T>(p0, 0),
+                                                        potential);
+    return QEB_OK;
+  }
+};
+
+template <typename T>
+struct PassCMulti {
+  const KBatch<T>* kb; const qeb_local_plan* p0; int nk; int sblocks; int nb; cudaStream_t s;
+  template <class F>
+  int operator()() const {
+    const dim3 grid(sblocks, (unsigned)nb, (unsigned)nk);
+    const T inv_n = T(1.0 / ((double)p0->nx * p0->ny * p0->nz));
+    four_pass_c_multi<T, F><<<grid, kThreads, ac_smem<T, F>(p0->nz_pad), s>>>(
+        *kb, p0->nz_pad, tw_at<T>(p0, 2), inv_n);
+    return QEB_OK;
+  }
+};
+
+// Largest pass-B shared memory over the batch (the plane holds nay rows).
+template <typename T>
+struct BSmem {
+  const qeb_local_plan* p;
+  size_t* out;
+  template <class F>
+  int operator()() const {
+    *out = b_smem<T, F>(p);
+    return QEB_OK;
+  }
+};
+
+template <typename T>
+int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* sticks,
+                  const void* const* psi, const int64_t* ld, const int64_t* nb,
+                  const void* potential, const void* const* kinetic, void* const* out,
+                  const int64_t* ldo, cudaStream_t s) {
+  KBatch<T> kb;
+  int max_nb = 0, max_blocks = 0;
+  size_t smem_b = 0;
+  for (int k = 0; k < nk; ++k) {
+    const qeb_local_plan* p = plans[k];
+    KDesc<T>& d = kb.k[k];
+    d.psi = static_cast<const C2<T>*>(psi[k]);
+    d.out = static_cast<C2<T>*>(out[k]);
+    d.kinetic = static_cast<const T*>(kinetic[k]);
+    d.sticks = static_cast<C2<T>*>(sticks[k]);
+    d.entry_g = p->entry_g;
+    d.entry_z = p->entry_z;
+    d.entry_stick = p->entry_stick;
+    d.stick_off = p->stick_off;
+    d.stick_pos = p->stick_pos;
+    d.y_to_ay = p->y_to_ay;
+    d.ld = ld[k];
+    d.ldo = ldo[k];
+    d.nst = p->nst;
+    d.nay = p->nay;
+    d.nb = (int)nb[k];
+    max_nb = max(max_nb, d.nb);
+    max_blocks = max(max_blocks, (p->nst + kSticksPerBlock - 1) / kSticksPerBlock);
+    size_t sb = 0;
+    int rc = with_variant(p->fast_xy, BSmem<T>{p, &sb});
+    if (rc) return rc;
+    smem_b = sb > smem_b ? sb : smem_b;
+  }
+  if (max_nb == 0) return QEB_OK;
+  const qeb_local_plan* p0 = plans[0];
+  int rc;
+  if ((rc = with_variant(p0->fast_z, PassAMulti<T>{&kb, p0, nk, max_blocks, max_nb, s}))) return rc;
+  if ((rc = with_variant(p0->fast_xy,
+                         PassBMulti<T>{&kb, p0, nk, max_nb, smem_b, static_cast<const T*>(potential), s})))
+    return rc;
+  if ((rc = with_variant(p0->fast_z, PassCMulti<T>{&kb, p0, nk, max_blocks, max_nb, s}))) return rc;
+  qeb::count_launches(3);
+  return qeb::cuda_status(cudaGetLastError(), "four-step apply_local_multi launch");
+}
 
 template <typename T>
 int apply_t(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64_t ld, int64_t nb,
@@ -459,6 +643,17 @@ int fast_smem_limits(const qeb_local_plan* p) {
     if (rc) return rc;
   }
   return QEB_OK;
+}
+
+int fast_apply_multi(int nk, const qeb_local_plan* const* plans, void* const* sticks,
+                     const void* const* psi, const int64_t* ld, const int64_t* nb,
+                     const void* potential, const void* const* kinetic, void* const* out,
+                     const int64_t* ldo, cudaStream_t stream) {
+  if (plans[0]->precision == QEB_F64)
+    return apply_multi_t<double>(nk, plans, sticks, psi, ld, nb, potential, kinetic, out, ldo,
+                                 stream);
+  return apply_multi_t<float>(nk, plans, sticks, psi, ld, nb, potential, kinetic, out, ldo,
+                              stream);
 }
 
 int fast_apply(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,

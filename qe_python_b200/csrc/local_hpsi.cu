@@ -539,6 +539,79 @@ extern "C" int qeb_apply_local(const qeb_local_plan* p, void* scratch, int64_t s
                              ldo, s);
 }
 
+static int64_t round_up_256(int64_t n) { return (n + 255) / 256 * 256; }
+
+extern "C" int64_t qeb_local_multi_scratch_bytes(int nk, const qeb_local_plan* const* plans,
+                                                 const int64_t* nbands) {
+  if (nk < 1 || plans == nullptr || nbands == nullptr) return -1;
+  int64_t total = 0;
+  for (int k = 0; k < nk; ++k) {
+    const int64_t b = qeb_local_scratch_bytes(plans[k], nbands[k]);
+    if (b < 0) return -1;
+    total += round_up_256(b);
+  }
+  return total;
+}
+
+extern "C" int qeb_apply_local_multi(int nk, const qeb_local_plan* const* plans, void* scratch,
+                                     int64_t scratch_bytes, const void* const* psi,
+                                     const int64_t* ld_psi, const int64_t* nbands,
+                                     const void* potential_native, const void* const* kinetic,
+                                     void* const* out, const int64_t* ld_out, void* stream) {
+  if (nk < 1 || nk > QEB_MAX_KBATCH || plans == nullptr || psi == nullptr || ld_psi == nullptr ||
+      nbands == nullptr || kinetic == nullptr || out == nullptr || ld_out == nullptr) {
+    qeb::set_error("apply_local_multi: 1..%d k points with non-null argument arrays",
+                   QEB_MAX_KBATCH);
+    return QEB_EINVAL;
+  }
+  const int64_t need = qeb_local_multi_scratch_bytes(nk, plans, nbands);
+  if (need < 0 || scratch_bytes < need) {
+    qeb::set_error("apply_local_multi: scratch of %lld bytes is below the %lld required",
+                   (long long)scratch_bytes, (long long)need);
+    return need < 0 ? QEB_EINVAL : QEB_ESCRATCH;
+  }
+  const qeb_local_plan* p0 = plans[0];
+  bool fused = p0 != nullptr && p0->fast_xy >= 0 && p0->fast_z >= 0;
+  void* sticks[QEB_MAX_KBATCH];
+  unsigned char* cursor = static_cast<unsigned char*>(scratch);
+  for (int k = 0; k < nk; ++k) {
+    const qeb_local_plan* p = plans[k];
+    int rc = check_call(p, cursor, qeb_local_scratch_bytes(p, nbands[k]), psi[k], ld_psi[k],
+                        nbands[k], "apply_local_multi");
+    if (rc) return rc;
+    if (nbands[k] > 0 && (potential_native == nullptr || out[k] == nullptr || ld_out[k] < p->npw)) {
+      qeb::set_error("apply_local_multi: null potential/output or short output leading dimension");
+      return QEB_EINVAL;
+    }
+    if (nbands[k] > 65535) {
+      qeb::set_error("apply_local_multi: at most 65535 bands per k point");
+      return QEB_EINVAL;
+    }
+    if (p->nx != p0->nx || p->ny != p0->ny || p->nz != p0->nz || p->precision != p0->precision ||
+        p->device != p0->device) {
+      qeb::set_error("apply_local_multi: every k point must use the same grid, precision and device");
+      return QEB_EINVAL;
+    }
+    fused = fused && p->fast_xy == p0->fast_xy && p->fast_z == p0->fast_z &&
+            p->nx_pad == p0->nx_pad && p->nz_pad == p0->nz_pad;
+    sticks[k] = cursor;
+    cursor += round_up_256(qeb_local_scratch_bytes(p, nbands[k]));
+  }
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (fused)
+    return qeb::fast_apply_multi(nk, plans, sticks, psi, ld_psi, nbands, potential_native, kinetic,
+                                 out, ld_out, s);
+  // grids without a four-step variant: one launch sequence per k point
+  for (int k = 0; k < nk; ++k) {
+    const int rc = qeb_apply_local(plans[k], sticks[k],
+                                   qeb_local_scratch_bytes(plans[k], nbands[k]), psi[k],
+                                   ld_psi[k], nbands[k], potential_native, kinetic[k], out[k],
+                                   ld_out[k], stream);
+    if (rc) return rc;
+  }
+  return QEB_OK;
+}
+
 extern "C" int qeb_accumulate_density(const qeb_local_plan* p, void* scratch,
                                       int64_t scratch_bytes, const void* psi, int64_t ld,
                                       int64_t nbands, const double* weights, double* density,

@@ -7,6 +7,9 @@
 
 #include "qeb_common.cuh"
 
+// k points one batched local apply handles (qeb_apply_local_multi).
+#define QEB_MAX_KBATCH 16
+
 struct qeb_local_plan {
   int nx, ny, nz;
   int64_t npw;
@@ -45,5 +48,11 @@ int fast_apply(const qeb_local_plan* p, void* sticks, const void* psi, int64_t l
                cudaStream_t stream, cudaEvent_t* events);
 int fast_density(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
                  const double* weights, double* density, cudaStream_t stream);
+// The three passes once for nk <= QEB_MAX_KBATCH plans on one grid (same
+// four-step variants, precision and device): grid.z = k point.
+int fast_apply_multi(int nk, const qeb_local_plan* const* plans, void* const* sticks,
+                     const void* const* psi, const int64_t* ld, const int64_t* nb,
+                     const void* potential, const void* const* kinetic, void* const* out,
+                     const int64_t* ldo, cudaStream_t stream);
 
 }  // namespace qeb

@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import kernels as K
-from .basis import LocalPotentialWorkspace, PlaneWaveBasis
+from .basis import LocalPotentialWorkspace, PlaneWaveBasis, apply_local_multi
 from .device import (
     COMPLEX_OF,
     REAL_OF,
@@ -233,6 +233,19 @@ class PlaneWaveHamiltonian:
         with _timer(self.timers, "h_psi"):
             return self._apply(coefficients, out=out)
 
+    def add_nonlocal(self, vectors: torch.Tensor, target: torch.Tensor) -> None:
+        """target += sum |beta> D <beta|vectors> (calbec, D, add)."""
+        if self.projectors.beta is None or vectors.shape[1] == 0:
+            return
+        if self.tensor_gemm and (leading_dimension(vectors) % 2 or vectors.data_ptr() % 16):
+            aligned = empty_f(vectors.shape[0], vectors.shape[1], self.dtype, self.device)
+            aligned.copy_(vectors)
+            vectors = aligned
+        with _timer(self.timers, "h_psi:calbec"):
+            becp = self.calbec(vectors)
+        with _timer(self.timers, "add_vuspsi"):
+            self.add_projectors(self.couple(becp), target)
+
     def _apply(self, coefficients, out=None):
         host = not isinstance(coefficients, torch.Tensor)
         vectors = to_device_f(coefficients, self.dtype, self.device)
@@ -283,6 +296,12 @@ class HpsiGraph:
         self.nbands = int(nbands)
         self.input = zeros_f(npw, self.nbands, ham.dtype, ham.device)
         self.output = zeros_f(npw, self.nbands, ham.dtype, ham.device)
+        # the (nbands, ld) row-major storage behind the column-major buffers:
+        # one contiguous block, so a host copy of the same shape is one DMA
+        self.input_storage = self.input.T.as_strided(
+            (self.nbands, leading_dimension(self.input)), (leading_dimension(self.input), 1))
+        self.output_storage = self.output.T.as_strided(
+            (self.nbands, leading_dimension(self.output)), (leading_dimension(self.output), 1))
         stream = torch.cuda.Stream(device=ham.device)
         stream.wait_stream(torch.cuda.current_stream())
         with torch.cuda.stream(stream):
@@ -391,6 +410,96 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
     tensors.  ``dtype`` selects the basis precision (default complex128, or
     the dtype of ``initial_vectors`` when it is a tensor).
     """
+    steps = davidson_steps(diagonal, number_of_roots, initial_vectors=initial_vectors,
+                           tolerance=tolerance, max_iterations=max_iterations,
+                           subspace_multiplier=subspace_multiplier,
+                           residual_factor=residual_factor,
+                           residual_energy_scale=residual_energy_scale,
+                           occupied_roots=occupied_roots, initial_is_ritz=initial_is_ritz,
+                           initial_is_orthonormal=initial_is_orthonormal,
+                           initial_eigenvalues=initial_eigenvalues,
+                           initial_applied=initial_applied, global_dimension=global_dimension,
+                           global_row_indices=global_row_indices, timers=timers, dtype=dtype)
+
+    def apply_into(vectors, destination):
+        if operator_into is not None:
+            operator_into(vectors, destination)
+        else:
+            destination[...] = operator(vectors)
+
+    try:
+        request = next(steps)
+        while True:
+            apply_into(*request)
+            request = steps.send(None)
+    except StopIteration as done:
+        return done.value
+
+
+def apply_hamiltonians(hamiltonians, requests) -> None:
+    """destination = H_index vectors for every (index, vectors, destination)
+    request: the local parts of all k points in one launch per FFT pass
+    (basis.apply_local_multi), then each k point's projector products."""
+    if not requests:
+        return
+    hams = [hamiltonians[index] for index, _, _ in requests]
+    first = hams[0]
+    batched = len(requests) > 1 and all(
+        h.local_workspace.precision == first.local_workspace.precision and
+        h.local_workspace.shape == first.local_workspace.shape and
+        h.dtype == first.dtype for h in hams)
+    if not batched:
+        for (_, vectors, destination), ham in zip(requests, hams):
+            ham.apply_into(vectors, destination)
+        return
+    vectors = [to_device_f(v, first.dtype, first.device) for _, v, _ in requests]
+    with _timer(first.timers, "h_psi"):
+        with _timer(first.timers, "vloc_psi"):
+            apply_local_multi([h.local_workspace for h in hams], first._potential, vectors,
+                              [h._kinetic_kernel for h in hams],
+                              [destination for _, _, destination in requests])
+        for v, (_, _, destination), ham in zip(vectors, requests, hams):
+            ham.add_nonlocal(v, destination)
+
+
+def run_lockstep(problems, apply_batch) -> list:
+    """Drive several ``davidson_steps`` generators together: every round
+    collects each unfinished problem's pending H application and hands them
+    to ``apply_batch([(index, vectors, destination), ...])`` at once (the
+    chosen form's batching of all k points into one launch per FFT pass).
+    Each problem runs the same operations as alone; returns the results in
+    order."""
+    results = [None] * len(problems)
+    pending = {}
+    for index, steps in enumerate(problems):
+        try:
+            pending[index] = next(steps)
+        except StopIteration as done:
+            results[index] = done.value
+    while pending:
+        apply_batch([(index, vectors, destination)
+                     for index, (vectors, destination) in pending.items()])
+        following = {}
+        for index in pending:
+            try:
+                following[index] = problems[index].send(None)
+            except StopIteration as done:
+                results[index] = done.value
+        pending = following
+    return results
+
+
+def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
+                   tolerance: float = 1.0e-8, max_iterations: int = 40,
+                   subspace_multiplier: int = 4, residual_factor: float | None = 10.0,
+                   residual_energy_scale: float | None = None, occupied_roots: int | None = None,
+                   initial_is_ritz: bool = False, initial_is_orthonormal: bool = False,
+                   initial_eigenvalues=None, initial_applied=None,
+                   global_dimension: int | None = None, global_row_indices=None, timers=None,
+                   dtype: torch.dtype | None = None):
+    """The Davidson algorithm of ``davidson`` as a generator: it yields
+    ``(vectors, destination)`` whenever it needs destination = H vectors and
+    returns the DavidsonResult (StopIteration.value)."""
     device = require_cuda()
     diag = to_device_f(diagonal, torch.float64, device).reshape(-1)
     local_dimension = diag.numel()
@@ -446,14 +555,8 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
     basis_storage[:, :active] = basis0
     del basis0, trial
 
-    def apply_into(vectors, destination):
-        if operator_into is not None:
-            operator_into(vectors, destination)
-        else:
-            destination[...] = operator(vectors)
-
     if initial_applied is None:
-        apply_into(basis_storage[:, :active], applied_storage[:, :active])
+        yield basis_storage[:, :active], applied_storage[:, :active]
         applications = active
     else:
         supplied = to_device_f(initial_applied, dtype, device)
@@ -558,7 +661,7 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
         selected = torch.as_tensor(keep.astype(np.int64), device=device)
         K.normalize_columns(corrections, norms2, selected, basis_storage[:, old:active])
         del ritz_vectors, residuals, corrections, block
-        apply_into(basis_storage[:, old:active], applied_storage[:, old:active])
+        yield basis_storage[:, old:active], applied_storage[:, old:active]
         applications += keep.size
         update_projected(old)
         values, values_dev, coefficients = ritz_values()

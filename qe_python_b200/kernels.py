@@ -13,6 +13,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from .autotune import TUNER, bucket
 from .device import empty_f, is_column_major, leading_dimension, stream_handle
 
 OP_N = 0
@@ -226,11 +227,13 @@ def tf32_error() -> int:
 
 
 def cgemm_tf32x3(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None,
-                 alpha: complex = 1.0, beta: complex = 0.0) -> torch.Tensor | None:
+                 alpha: complex = 1.0, beta: complex = 0.0,
+                 splits: int | None = None) -> torch.Tensor | None:
     """Split-TF32 c = alpha op(a) b + beta c reading complex64 a and b directly
-    (qeb_cgemm_tf32x3).  Returns None, touching nothing, when a or b lacks
+    (qeb_cgemm_tf32x3_ex).  Returns None, touching nothing, when a or b lacks
     16-byte aligned columns (odd leading dimension); callers then use the
-    packed path."""
+    packed path.  ``splits``: CTAs per output tile along K; None lets the
+    autotuner pick among the built-in choice, half and twice it."""
     _check_matrix("a", a)
     _check_matrix("b", b)
     if a.dtype != torch.complex64 or b.dtype != torch.complex64:
@@ -259,15 +262,37 @@ def cgemm_tf32x3(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | 
     if k == 0:  # empty contraction: c = beta c
         return c.zero_() if complex(beta) == 0 else c.mul_(beta)
     lib = _lib.load()
+    if splits is None:
+        default = int(lib.qeb_cgemm_tf32x3_default_splits(op_a, m, n, k))
+        kblocks = (2 * k + 31) // 32
+        candidates = sorted({default, max(1, default // 2), min(2 * default, max(1, kblocks // 4))})
+        candidates.remove(default)
+        candidates.insert(0, default)
+        key = f"cgemm_tf32x3/{op_a}/{bucket(m)}/{bucket(n)}/{bucket(k)}"
+        probe = []
+
+        def run(s_):  # into a scratch output: c may be accumulated into (beta != 0)
+            if not probe:
+                probe.append(empty_f(m, n, torch.complex64, c.device))
+            _cgemm_tf32x3_launch(lib, op_a, m, n, k, 1.0, a, lda, b, ldb, 0.0, probe[0], s_)
+
+        splits = TUNER.choose(key, candidates, run)
+    _cgemm_tf32x3_launch(lib, op_a, m, n, k, alpha, a, lda, b, ldb, beta, c, splits)
+    return c
+
+
+def _cgemm_tf32x3_launch(lib, op_a, m, n, k, alpha, a, lda, b, ldb, beta, c, splits):
     al = (ctypes.c_double * 2)(complex(alpha).real, complex(alpha).imag)
     be = (ctypes.c_double * 2)(complex(beta).real, complex(beta).imag)
-    need = int(lib.qeb_cgemm_tf32x3_scratch_bytes(op_a, m, n, k))
+    if splits and splits > 1:
+        need = int(splits) * m * n * 8
+    else:
+        need = 0 if splits == 1 else int(lib.qeb_cgemm_tf32x3_scratch_bytes(op_a, m, n, k))
     scratch = _SCRATCH.get(need, c.device) if need > 0 else None
-    _lib.check("qeb_cgemm_tf32x3", lib.qeb_cgemm_tf32x3(
+    _lib.check("qeb_cgemm_tf32x3_ex", lib.qeb_cgemm_tf32x3_ex(
         op_a, m, n, k, al, a.data_ptr(), lda, b.data_ptr(), ldb, be, c.data_ptr(),
         leading_dimension(c), 0 if scratch is None else scratch.data_ptr(), need,
-        stream_handle()))
-    return c
+        int(splits or 0), stream_handle()))
 
 
 def gemm_tf32(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None,

@@ -34,7 +34,14 @@ from . import kernels as K
 from .basis import LocalPotentialWorkspace, fft_shape, make_bases
 from .configs import DIAMOND_CUBIC, displacements, supercell
 from .device import empty_f, require_cuda, to_device_f
-from .diagonalization import PlaneWaveHamiltonian, davidson, lowest_generalized_eigh
+from .diagonalization import (
+    PlaneWaveHamiltonian,
+    apply_hamiltonians,
+    davidson,
+    davidson_steps,
+    lowest_generalized_eigh,
+    run_lockstep,
+)
 from .pseudo import SyntheticPseudo, synthetic_pseudo
 from .charge import DeviceBroydenMixer, DeviceChargeGrid, DeviceLinearMixer
 from .charge import pz81 as device_pz81
@@ -409,15 +416,54 @@ def projector_terms(system: System, tables: dict, basis) -> tuple:
 MIN_FP64_ITERATIONS = 3  # mixed form: FP64 iterations before convergence is accepted
 
 
+def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, tol, occ_roots,
+                   is_ritz, timers):
+    """One k point's diagonalisation as a generator of H applications: the
+    Davidson of qepy_pw/pw/scf.py:3496-3556 (20 iterations), repeated up to
+    five more times from its last vectors while more than five roots remain
+    unconverged.  Returns (DavidsonResult, Davidson iterations)."""
+    attempt, total_its = 0, 0.0
+    vectors, eigs, applied = start_vectors, initial_eigs, initial_applied
+    while True:
+        sol = yield from davidson_steps(
+            ham.diagonal, system.nbnd, initial_vectors=vectors, tolerance=tol, max_iterations=20,
+            subspace_multiplier=system.diago_david_ndim, residual_factor=None,
+            residual_energy_scale=None, occupied_roots=occ_roots, initial_is_ritz=is_ritz,
+            initial_is_orthonormal=True, initial_eigenvalues=eigs, initial_applied=applied,
+            timers=timers, dtype=ham.dtype)
+        attempt += 1
+        total_its += sol.iterations
+        if sol.converged or sol.number_unconverged <= 5 or attempt >= 6:
+            return sol, total_its
+        vectors, eigs, applied = sol.eigenvectors, sol.eigenvalues, None
+
+
+def _drive(steps, ham):
+    """Run a generator of H applications with one Hamiltonian."""
+    try:
+        request = next(steps)
+        while True:
+            ham.apply_into(*request)
+            request = steps.send(None)
+    except StopIteration as done:
+        return done.value
+
+
 def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
-            progress=None, timers=None, pools=None) -> SCFResult:
+            progress=None, timers=None, pools=None, fp32_floor: float = 2.0e-6,
+            batch_kpoints: bool | None = None) -> SCFResult:
     """Converge the Kohn-Sham density to ``system.conv_thr`` (Ry) on the GPU.
 
     ``timers``: optional object with a ``measure(name)`` context manager,
     handed to the Hamiltonian and Davidson (the reference's timer names).
     ``pools``: optional qe_python_b200.pools.KPointPools; each rank then
     solves its own k points and the density, eigenvalues and nonlocal
-    forces are combined over the pools."""
+    forces are combined over the pools.  ``batch_kpoints`` (default: on for
+    the mixed form) runs the k points' Davidson solves in lockstep with one
+    launch per FFT pass for all of them; the results are those of the
+    k-by-k loop."""
+    if batch_kpoints is None:
+        batch_kpoints = precision == "mixed"
     if precision not in ("f64", "mixed"):
         raise ValueError("precision must be 'f64' or 'mixed'")
     device = require_cuda()
@@ -506,12 +552,14 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
                 mixer.reset()
             davidson_tolerance = max(5.0e-14, 0.1 * previous_accuracy / max(1.0, nelec))
         # FP32 eigenvalues stall near 1e-7 relative: never ask more of them
-        tol = davidson_tolerance if current_precision == "f64" else max(davidson_tolerance, 2.0e-6)
+        # than ``fp32_floor`` (Ha)
+        tol = davidson_tolerance if current_precision == "f64" else max(davidson_tolerance, fp32_floor)
         precision_log.append(current_precision)
         tick("v_of_rho", t0)
         t0 = time.perf_counter()
         local_eigenvalues = {}
         its = []
+        hams, solves = {}, {}
         for k, state in enumerate(states):
             if k not in local_k:
                 if state.vectors is None and iteration == 1 and not random_drawn[k]:
@@ -537,23 +585,21 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             # pass's eigenvectors when the iteration is repeated); later
             # iterations restart from the converged eigenvectors
             # (qepy_pw/pw/scf.py:3503-3556)
-            is_ritz = iteration == 1
             occ_roots = occupied if iteration > 1 and not smeared else system.nbnd
-            attempt, total_its = 0, 0.0
-            retry_vectors, retry_eigs, retry_applied = start_vectors, initial_eigs, initial_applied
-            while True:
-                sol = davidson(ham.apply, ham.diagonal, system.nbnd, initial_vectors=retry_vectors,
-                               tolerance=tol, max_iterations=20,
-                               subspace_multiplier=system.diago_david_ndim, residual_factor=None,
-                               residual_energy_scale=None, occupied_roots=occ_roots,
-                               initial_is_ritz=is_ritz, initial_is_orthonormal=True,
-                               initial_eigenvalues=retry_eigs, initial_applied=retry_applied,
-                               operator_into=ham.apply_into, dtype=ham.dtype, timers=timers)
-                attempt += 1
-                total_its += sol.iterations
-                if sol.converged or sol.number_unconverged <= 5 or attempt >= 6:
-                    break
-                retry_vectors, retry_eigs, retry_applied = sol.eigenvectors, sol.eigenvalues, None
+            hams[k] = ham
+            solves[k] = _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied,
+                                       tol, occ_roots, iteration == 1, timers)
+        order = sorted(solves)
+        if batch_kpoints and len(order) > 1:
+            # chosen form: the k points' Davidson solves advance together and
+            # each round's H applications share one launch per FFT pass
+            outcomes = run_lockstep([solves[k] for k in order],
+                                    lambda requests: apply_hamiltonians(
+                                        [hams[k] for k in order], requests))
+        else:
+            outcomes = [_drive(solves[k], hams[k]) for k in order]
+        for k, (sol, total_its) in zip(order, outcomes):
+            state = states[k]
             its.append(total_its)
             state.vectors = sol.eigenvectors.to(torch.complex128).T.contiguous().T
             state.eigenvalues = np.asarray(sol.eigenvalues)
