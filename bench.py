@@ -61,35 +61,48 @@ def parse_args():
                         "in the given precision, print a checksum, no timing")
     p.add_argument("--cpu-seconds", type=float, default=10.0,
                    help="approximate CPU time budget of the cpu_baseline sample")
-    p.add_argument("--scf", default="scf-fcc2",
-                   help="benchmark cell whose SCF-to-1e-8 Ry time is reported beside the "
-                        "H|psi> rate (scf-fcc2, scf-dia8-disp, scf-dia64, scf-dia216, none)")
+    p.add_argument("--scf", default="scf-dia216,scf-dia64",
+                   help="comma-separated benchmark cells whose SCF-to-1e-8 Ry times (plain "
+                        "and mixed) are reported beside the H|psi> rate (scf-fcc2, "
+                        "scf-fcc2-smear, scf-dia8-disp, scf-dia64, scf-dia216, or none)")
     return p.parse_args()
 
 
 def scf_times(name: str) -> dict:
-    """Wall time of the GPU SCF to conv_thr = 1e-8 Ry, plain FP64 and mixed."""
+    """Wall time of the GPU SCF to conv_thr = 1e-8 Ry, plain FP64 and mixed,
+    with the mixed form's energy, eigenvalue and force differences from the
+    FP64 run."""
     import torch
 
     from qe_python_b200.scf import benchmark_system, run_scf
 
     out = {"cell": name, "conv_thr_ry": 1.0e-8}
+    results = {}
     for precision in ("f64", "mixed"):
         system = benchmark_system(name)
         torch.cuda.synchronize()
         started = time.perf_counter()
         result = run_scf(system, precision=precision)
         torch.cuda.synchronize()
+        results[precision] = result
         out[precision] = {
             "seconds": time.perf_counter() - started,
             "converged": bool(result.converged),
             "iterations": result.iterations,
             "total_energy_ry": result.total_energy_ry,
             "precision_per_iteration": result.precision_log,
+            "davidson_iterations": float(sum(result.davidson_iterations)),
             "phase_seconds": {k: round(v, 3) for k, v in result.timings.items()},
         }
     out["mixed_speedup"] = out["f64"]["seconds"] / out["mixed"]["seconds"]
     out["energy_difference_ry"] = out["mixed"]["total_energy_ry"] - out["f64"]["total_energy_ry"]
+    a, b = results["mixed"], results["f64"]
+    out["max_eigenvalue_difference_ry"] = max(
+        float(np.max(np.abs(2.0 * (np.asarray(x) - np.asarray(y)))))
+        for x, y in zip(a.eigenvalues_ha, b.eigenvalues_ha))
+    if a.forces_ha_per_bohr is not None and b.forces_ha_per_bohr is not None:
+        out["max_force_difference_ry_per_bohr"] = float(
+            np.max(np.abs(2.0 * (a.forces_ha_per_bohr - b.forces_ha_per_bohr))))
     return out
 
 
@@ -496,7 +509,8 @@ def run_b200(args) -> None:
         "clocks_staged": clocks.summary(),
     }
     if args.scf and args.scf != "none":
-        line["scf"] = scf_times(args.scf)
+        legs = [scf_times(name) for name in args.scf.split(",") if name]
+        line["scf"] = legs[0] if len(legs) == 1 else legs
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample = 16

@@ -58,6 +58,20 @@ __device__ __forceinline__ C2<T> small_tw(int m) {
   }
 }
 
+// u * exp(sgn 2 pi i m / 8) for the compile-time m = 1, 2, 3 of the length-8
+// split: multiplications by (1 +- i)/sqrt(2) and +-i without table loads.
+template <typename T, bool BWD>
+__device__ __forceinline__ C2<T> mul_w8(C2<T> u, int m) {
+  constexpr T r = T(0.70710678118654752440084436210484903928L);  // 1/sqrt(2)
+  // forward (BWD false) rotates by -45 degrees per step, backward by +45
+  if (m == 2) return BWD ? mk<T>(-u.im, u.re) : mk<T>(u.im, -u.re);
+  if (m == 1)
+    return BWD ? mk<T>(r * (u.re - u.im), r * (u.re + u.im))
+               : mk<T>(r * (u.re + u.im), r * (u.im - u.re));
+  return BWD ? mk<T>(-r * (u.re + u.im), r * (u.re - u.im))
+             : mk<T>(r * (u.im - u.re), -r * (u.re + u.im));
+}
+
 // In-register DFT of compile-time length N (sign +1 if BWD else -1).
 template <typename T, int N, bool BWD>
 __device__ __forceinline__ void dft(C2<T>* v) {
@@ -76,8 +90,14 @@ __device__ __forceinline__ void dft(C2<T>* v) {
       for (int n1 = 0; n1 < A; ++n1) u[n1] = v[B * n1 + n2];
       dft<T, A, BWD>(u);
 #pragma unroll
-      for (int k1 = 0; k1 < A; ++k1)
-        y[n2][k1] = (n2 * k1 == 0) ? u[k1] : cmul(u[k1], small_tw<T, N, BWD>(n2 * k1));
+      for (int k1 = 0; k1 < A; ++k1) {
+        if (n2 * k1 == 0)
+          y[n2][k1] = u[k1];
+        else if constexpr (N == 8)
+          y[n2][k1] = mul_w8<T, BWD>(u[k1], n2 * k1);
+        else
+          y[n2][k1] = cmul(u[k1], small_tw<T, N, BWD>(n2 * k1));
+      }
     }
 #pragma unroll
     for (int k1 = 0; k1 < A; ++k1) {

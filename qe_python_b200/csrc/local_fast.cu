@@ -524,7 +524,7 @@ template <typename T>
 int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* sticks,
                   const void* const* psi, const int64_t* ld, const int64_t* nb,
                   const void* potential, const void* const* kinetic, void* const* out,
-                  const int64_t* ldo, cudaStream_t s) {
+                  const int64_t* ldo, cudaStream_t s, cudaEvent_t* ev = nullptr) {
   KBatch<T> kb;
   int max_nb = 0, max_blocks = 0;
   size_t smem_b = 0;
@@ -556,31 +556,17 @@ int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* stick
   if (max_nb == 0) return QEB_OK;
   const qeb_local_plan* p0 = plans[0];
   int rc;
+  if (ev) cudaEventRecord(ev[0], s);
   if ((rc = with_variant(p0->fast_z, PassAMulti<T>{&kb, p0, nk, max_blocks, max_nb, s}))) return rc;
+  if (ev) cudaEventRecord(ev[1], s);
   if ((rc = with_variant(p0->fast_xy,
                          PassBMulti<T>{&kb, p0, nk, max_nb, smem_b, static_cast<const T*>(potential), s})))
     return rc;
-  if ((rc = with_variant(p0->fast_z, PassCMulti<T>{&kb, p0, nk, max_blocks, max_nb, s}))) return rc;
-  qeb::count_launches(3);
-  return qeb::cuda_status(cudaGetLastError(), "four-step apply_local_multi launch");
-}
-
-template <typename T>
-int apply_t(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64_t ld, int64_t nb,
-            const T* potential, const T* kinetic, C2<T>* out, int64_t ldo, cudaStream_t s,
-            cudaEvent_t* ev) {
-  int rc;
-  if (ev) cudaEventRecord(ev[0], s);
-  if ((rc = with_variant(p->fast_z, PassA<T>{p, sticks, psi, ld, nb, s}))) return rc;
-  if (ev) cudaEventRecord(ev[1], s);
-  if ((rc = with_variant(p->fast_xy, PassB<T, 0>{p, sticks, nb, potential, nullptr, nullptr, s})))
-    return rc;
   if (ev) cudaEventRecord(ev[2], s);
-  if ((rc = with_variant(p->fast_z, PassC<T>{p, sticks, psi, ld, nb, kinetic, out, ldo, s})))
-    return rc;
+  if ((rc = with_variant(p0->fast_z, PassCMulti<T>{&kb, p0, nk, max_blocks, max_nb, s}))) return rc;
   if (ev) cudaEventRecord(ev[3], s);
   qeb::count_launches(3);
-  return qeb::cuda_status(cudaGetLastError(), "four-step apply_local launch");
+  return qeb::cuda_status(cudaGetLastError(), "four-step apply_local_multi launch");
 }
 
 template <typename T>
@@ -656,17 +642,21 @@ int fast_apply_multi(int nk, const qeb_local_plan* const* plans, void* const* st
                               stream);
 }
 
+// One plan runs through the batched kernels with a batch of one, so a k point
+// gives the same bits alone and inside a batch.
 int fast_apply(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
                const void* potential, const void* kinetic, void* out, int64_t ldo,
                cudaStream_t stream, cudaEvent_t* events) {
+  const qeb_local_plan* plans[1] = {p};
+  void* st[1] = {sticks};
+  const void* ps[1] = {psi};
+  const void* kin[1] = {kinetic};
+  void* o[1] = {out};
+  const int64_t lds[1] = {ld}, nbs[1] = {nb}, ldos[1] = {ldo};
   if (p->precision == QEB_F64)
-    return apply_t<double>(p, static_cast<C2<double>*>(sticks), static_cast<const C2<double>*>(psi),
-                           ld, nb, static_cast<const double*>(potential),
-                           static_cast<const double*>(kinetic), static_cast<C2<double>*>(out), ldo,
-                           stream, events);
-  return apply_t<float>(p, static_cast<C2<float>*>(sticks), static_cast<const C2<float>*>(psi), ld,
-                        nb, static_cast<const float*>(potential), static_cast<const float*>(kinetic),
-                        static_cast<C2<float>*>(out), ldo, stream, events);
+    return apply_multi_t<double>(1, plans, st, ps, lds, nbs, potential, kin, o, ldos, stream,
+                                 events);
+  return apply_multi_t<float>(1, plans, st, ps, lds, nbs, potential, kin, o, ldos, stream, events);
 }
 
 int fast_density(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,

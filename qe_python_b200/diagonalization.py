@@ -81,6 +81,7 @@ class _DeviceProjectors:
     """
 
     def __init__(self, terms, npw: int, dtype: torch.dtype, device: torch.device) -> None:
+        self.npw, self.dtype = int(npw), dtype
         betas, couplings, diagonals = [], [], []
         self.host_diagonal = np.zeros(npw)
         self.device_diagonal = torch.zeros(npw, dtype=torch.float64, device=device)
@@ -165,7 +166,12 @@ class PlaneWaveHamiltonian:
     def __init__(self, basis: PlaneWaveBasis, potential_g, projector_terms=(),
                  local_workspace: LocalPotentialWorkspace | None = None, timers=None,
                  real_potential=None, native_potential_layout: bool = False,
-                 potential_average: float | None = None, precision: str | None = None) -> None:
+                 potential_average: float | None = None, precision: str | None = None,
+                 device_projectors: "_DeviceProjectors | None" = None) -> None:
+        """``device_projectors``: the device form of ``projector_terms`` built
+        by an earlier Hamiltonian of the same basis and precision (its
+        ``projectors`` attribute); the SCF reuses it across iterations because
+        the projectors depend on the ions only."""
         self.basis = basis
         self.potential_g = potential_g
         if local_workspace is None:
@@ -195,7 +201,12 @@ class PlaneWaveHamiltonian:
         self._kinetic = torch.from_numpy(kinetic).to(self.device)
         self._kinetic_kernel = self._kinetic.to(REAL_OF[self.dtype])
         self._potential = local_workspace.native_potential(real_potential, self.native_potential_layout)
-        self.projectors = _DeviceProjectors(projector_terms, len(basis), self.dtype, self.device)
+        if device_projectors is not None:
+            if device_projectors.dtype != self.dtype or device_projectors.npw != len(basis):
+                raise ValueError("device_projectors were built for another basis or precision")
+            self.projectors = device_projectors
+        else:
+            self.projectors = _DeviceProjectors(projector_terms, len(basis), self.dtype, self.device)
         # chosen form: projector GEMMs as split-TF32 tcgen05 products
         self.tensor_gemm = self.dtype == torch.complex64
         self.projector_terms = tuple(projector_terms)
@@ -205,7 +216,10 @@ class PlaneWaveHamiltonian:
     def calbec(self, vectors: torch.Tensor) -> torch.Tensor:
         """becp = beta^H psi (projector_overlaps, _native_fft.pyx:694-731)."""
         p = self.projectors
-        if p.packed_conj is not None and self.tensor_gemm:
+        if self.tensor_gemm:
+            out = K.cgemm_tf32x3(K.OP_C, p.beta, vectors)
+            if out is not None:
+                return out
             return K.gemm_tf32(K.OP_C, p.beta, vectors, a_packed=p.packed_conj)
         return K.gemm(K.OP_C, p.beta, vectors)
 
@@ -216,7 +230,10 @@ class PlaneWaveHamiltonian:
     def add_projectors(self, coupled: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
         """target += beta coupled (add_projector_product, _native_fft.pyx:782-836)."""
         p = self.projectors
-        if p.packed_plain is not None and self.tensor_gemm:
+        if self.tensor_gemm:
+            out = K.cgemm_tf32x3(K.OP_N, p.beta, coupled, target, beta=1.0)
+            if out is not None:
+                return out
             return K.gemm_tf32(K.OP_N, p.beta, coupled, target, beta=1.0, a_packed=p.packed_plain)
         return K.gemm(K.OP_N, p.beta, coupled, target, beta=1.0)
 

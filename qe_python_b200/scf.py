@@ -348,6 +348,8 @@ class KPointState:
         self.vectors: torch.Tensor | None = None
         self.eigenvalues: np.ndarray | None = None
         self.terms = None
+        # projector operands on the device per precision (fixed ions)
+        self.device_projectors: dict = {}
 
     def workspace(self, precision: str) -> LocalPotentialWorkspace:
         if precision not in self.workspaces:
@@ -572,7 +574,10 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
                 state.terms = projector_terms(system, tables, state.basis)
             ham = PlaneWaveHamiltonian(state.basis, None, state.terms, local_workspace=ws,
                                        real_potential=v_dev, potential_average=v_ion_average,
-                                       timers=timers)
+                                       timers=timers,
+                                       device_projectors=state.device_projectors.get(
+                                           current_precision))
+            state.device_projectors[current_precision] = ham.projectors
             initial_applied = None
             initial_eigs = None
             if state.vectors is None:
@@ -589,16 +594,16 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             hams[k] = ham
             solves[k] = _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied,
                                        tol, occ_roots, iteration == 1, timers)
-        order = sorted(solves)
-        if batch_kpoints and len(order) > 1:
+        k_order = sorted(solves)
+        if batch_kpoints and len(k_order) > 1:
             # chosen form: the k points' Davidson solves advance together and
             # each round's H applications share one launch per FFT pass
-            outcomes = run_lockstep([solves[k] for k in order],
+            outcomes = run_lockstep([solves[k] for k in k_order],
                                     lambda requests: apply_hamiltonians(
-                                        [hams[k] for k in order], requests))
+                                        [hams[k] for k in k_order], requests))
         else:
-            outcomes = [_drive(solves[k], hams[k]) for k in order]
-        for k, (sol, total_its) in zip(order, outcomes):
+            outcomes = [_drive(solves[k], hams[k]) for k in k_order]
+        for k, (sol, total_its) in zip(k_order, outcomes):
             state = states[k]
             its.append(total_its)
             state.vectors = sol.eigenvectors.to(torch.complex128).T.contiguous().T

@@ -1,6 +1,6 @@
 """All k points in one launch per FFT pass (qeb_apply_local_multi) and the
-lockstep Davidson built on it: the batched results are bit-identical to the
-k-by-k ones, because every k point runs the same per-band arithmetic."""
+lockstep Davidson built on it: a batched H application is bit-identical to
+the k-by-k one (single plans run through the same batched kernels)."""
 
 from __future__ import annotations
 
@@ -68,11 +68,15 @@ def test_batched_local_and_full_apply_equal_per_k(cuda_device, precision):
 
 
 def test_lockstep_scf_reproduces_k_by_k_scf(cuda_device):
+    """The H applications are bit-identical; the density kernel sums bands
+    with FP64 atomics, whose order varies from run to run, so two SCFs agree
+    to the last bits rather than bit for bit."""
     from qe_python_b200.scf import benchmark_system, run_scf
 
     a = run_scf(benchmark_system("scf-fcc2"), precision="mixed", batch_kpoints=True)
     b = run_scf(benchmark_system("scf-fcc2"), precision="mixed", batch_kpoints=False)
     assert a.converged and b.converged
-    assert a.energies_ha == b.energies_ha
+    assert len(a.energies_ha) == len(b.energies_ha)
+    np.testing.assert_allclose(a.energies_ha, b.energies_ha, rtol=1e-12, atol=0)
     for x, y in zip(a.eigenvalues_ha, b.eigenvalues_ha):
-        np.testing.assert_array_equal(x, y)
+        np.testing.assert_allclose(x, y, rtol=0, atol=1e-10)
