@@ -24,9 +24,10 @@ import torch
 
 
 class Autotuner:
-    def __init__(self, path: str | None = None, repeats: int = 3) -> None:
+    def __init__(self, path: str | None = None, repeats: int = 3, margin: float = 0.05) -> None:
         self.path = path
         self.repeats = int(repeats)
+        self.margin = float(margin)
         self.table: dict[str, object] = {}
         self.timings: dict[str, dict[str, float]] = {}
         self._lock = threading.Lock()
@@ -43,31 +44,45 @@ class Autotuner:
         known = self.table.get(key)
         if known in candidates:
             return known
-        if len(candidates) == 1 or not self.enabled or not torch.cuda.is_available() or \
+        if len(candidates) == 1 or not self.enabled or not _cuda() or \
                 torch.cuda.is_current_stream_capturing():
             return candidates[0]
         with self._lock:
             stream = torch.cuda.current_stream()
             for c in candidates:  # warm-up: first-use allocations, caches
                 run(c)
-            times = {}
-            for c in candidates:
-                start = torch.cuda.Event(enable_timing=True)
-                end = torch.cuda.Event(enable_timing=True)
-                torch.cuda.synchronize()
-                start.record(stream)
-                for _ in range(self.repeats):
+            samples = {c: [] for c in candidates}
+            for _ in range(self.repeats):  # interleaved, median per candidate
+                for c in candidates:
+                    start = torch.cuda.Event(enable_timing=True)
+                    end = torch.cuda.Event(enable_timing=True)
+                    start.record(stream)
                     run(c)
-                end.record(stream)
-                end.synchronize()
-                times[c] = start.elapsed_time(end) / self.repeats
+                    end.record(stream)
+                    end.synchronize()
+                    samples[c].append(start.elapsed_time(end))
+            times = {c: sorted(v)[len(v) // 2] for c, v in samples.items()}
+            # the first candidate is the kernel's own default: another one
+            # must beat it by the margin to be chosen
             best = min(candidates, key=lambda c: times[c])
+            if times[best] > (1.0 - self.margin) * times[candidates[0]]:
+                best = candidates[0]
             self.table[key] = best
             self.timings[key] = {str(c): t for c, t in times.items()}
             if self.path:
                 with open(self.path, "w") as handle:
                     json.dump(self.table, handle, indent=1, sort_keys=True)
         return best
+
+
+_HAVE_CUDA = None
+
+
+def _cuda() -> bool:
+    global _HAVE_CUDA
+    if _HAVE_CUDA is None:
+        _HAVE_CUDA = torch.cuda.is_available()
+    return _HAVE_CUDA
 
 
 def bucket(n: int) -> int:

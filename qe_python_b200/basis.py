@@ -456,13 +456,13 @@ class LocalPotentialWorkspace:
             return
         if self.serial_fft_batch_size is not None:
             batch = max(1, int(self.serial_fft_batch_size))
-        elif self.pass_times is not None or nb <= 32:
+        elif self.pass_times is not None or nb < 128:
             batch = nb
         else:
             # bands per launch, by measurement: a batch whose stick buffer
             # stays in L2 between the passes can beat one launch of all bands
             top = bucket(nb)
-            candidates = [top] + [b for b in (256, 128, 64, 32) if b < top]
+            candidates = [top] + [b for b in (128, 64) if b < top]
             key = f"local_apply/{self.precision}/{self.shape}/{self.plane_waves}/{top}"
             batch = TUNER.choose(key, candidates, lambda b: self._run_apply(
                 potential, vectors, kinetic, target, min(b, nb)))

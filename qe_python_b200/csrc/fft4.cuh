@@ -170,6 +170,64 @@ __device__ __forceinline__ void four_forward(C2<T>* v, int lane, C2<T>* x, const
   __syncwarp(mask);
 }
 
+// Per-lane four-step twiddles held in registers: a line group processes
+// many lines with the same lane roles, so lane j's inverse factors
+// conj(w)^(j k), k < N1, and lane k's forward factors w^(k q), q < N2, are
+// loaded once instead of once per line.
+template <typename T, class F>
+struct LaneTwiddles {
+  C2<T> inv[F::N1];
+  C2<T> fwd[F::N2];
+  __device__ __forceinline__ void load(int lane, const C2<T>* tw) {
+#pragma unroll
+    for (int k = 0; k < F::N1; ++k) {
+      C2<T> w = tw[(lane * k) % F::n];
+      w.im = -w.im;
+      inv[k] = w;
+    }
+#pragma unroll
+    for (int q = 0; q < F::N2; ++q) fwd[q] = tw[(lane * q) % F::n];
+  }
+};
+
+template <typename T, class F>
+__device__ __forceinline__ void four_inverse(C2<T>* v, int lane, C2<T>* x,
+                                             const LaneTwiddles<T, F>& w, unsigned mask) {
+  if (lane < F::N2) {
+    dft<T, F::N1, true>(v);
+#pragma unroll
+    for (int k = 1; k < F::N1; ++k) v[k] = cmul(v[k], w.inv[k]);
+#pragma unroll
+    for (int k = 0; k < F::N1; ++k) x[k * F::xstride + lane] = v[k];
+  }
+  __syncwarp(mask);
+  if (lane < F::N1) {
+#pragma unroll
+    for (int i = 0; i < F::N2; ++i) v[i] = x[lane * F::xstride + i];
+    dft<T, F::N2, true>(v);
+  }
+  __syncwarp(mask);
+}
+
+template <typename T, class F>
+__device__ __forceinline__ void four_forward(C2<T>* v, int lane, C2<T>* x,
+                                             const LaneTwiddles<T, F>& w, unsigned mask) {
+  if (lane < F::N1) {
+    dft<T, F::N2, false>(v);
+#pragma unroll
+    for (int q = 1; q < F::N2; ++q) v[q] = cmul(v[q], w.fwd[q]);
+#pragma unroll
+    for (int q = 0; q < F::N2; ++q) x[lane * F::xstride + q] = v[q];
+  }
+  __syncwarp(mask);
+  if (lane < F::N2) {
+#pragma unroll
+    for (int k = 0; k < F::N1; ++k) v[k] = x[k * F::xstride + lane];
+    dft<T, F::N1, false>(v);
+  }
+  __syncwarp(mask);
+}
+
 // Host: upload the composite small-DFT twiddles to the current device.
 int init_small_dft_twiddles();
 

@@ -208,6 +208,8 @@ __device__ __forceinline__ void pass_b_body(
   __syncthreads();
   const GroupIds<F> g;
   C2<T>* x = xbuf + g.gid * F::scratch;
+  qeb::LaneTwiddles<T, F> lw;
+  lw.load(g.lig, tw);
   // inverse transforms along x of the active rows (D1 in, D2 out, in place)
   if (g.valid) {
     for (int r = g.gid; r < nay; r += g.ngroups) {
@@ -217,7 +219,7 @@ __device__ __forceinline__ void pass_b_body(
 #pragma unroll
         for (int i = 0; i < F::N1; ++i) v[i] = row[g.lig + F::N2 * i];
       }
-      qeb::four_inverse<T, F>(v, g.lig, x, tw, g.mask);
+      qeb::four_inverse<T, F>(v, g.lig, x, lw, g.mask);
       if (g.lig < F::N1) {
 #pragma unroll
         for (int p = 0; p < F::N2; ++p) row[g.lig + F::N1 * p] = v[p];
@@ -239,14 +241,14 @@ __device__ __forceinline__ void pass_b_body(
           v[i] = (ay >= 0) ? plane[ay * nx_pad + col] : qeb::mk<T>(0, 0);
         }
       }
-      qeb::four_inverse<T, F>(v, g.lig, x, tw, g.mask);
+      qeb::four_inverse<T, F>(v, g.lig, x, lw, g.mask);
       if (MODE == 0) {
         if (g.lig < F::N1) {
           const T* vcol = potential + ((int64_t)z * n + col) * n;
 #pragma unroll
           for (int p = 0; p < F::N2; ++p) v[p] = qeb::scale(v[p], __ldg(vcol + g.lig + F::N1 * p));
         }
-        qeb::four_forward<T, F>(v, g.lig, x, tw, g.mask);
+        qeb::four_forward<T, F>(v, g.lig, x, lw, g.mask);
         if (g.lig < F::N2) {
 #pragma unroll
           for (int i = 0; i < F::N1; ++i) {
@@ -278,7 +280,7 @@ __device__ __forceinline__ void pass_b_body(
 #pragma unroll
         for (int p = 0; p < F::N2; ++p) v[p] = row[g.lig + F::N1 * p];
       }
-      qeb::four_forward<T, F>(v, g.lig, x, tw, g.mask);
+      qeb::four_forward<T, F>(v, g.lig, x, lw, g.mask);
       if (g.lig < F::N2) {
 #pragma unroll
         for (int i = 0; i < F::N1; ++i) row[g.lig + F::N2 * i] = v[i];

@@ -15,11 +15,18 @@ COMPLEX_OF = {torch.float64: torch.complex128, torch.float32: torch.complex64}
 REAL_OF = {torch.complex128: torch.float64, torch.complex64: torch.float32}
 
 
+_CUDA_SEEN = False
+
+
 def require_cuda() -> torch.device:
-    if not torch.cuda.is_available():
-        raise RuntimeError(
-            "qe_b200 needs a CUDA device: the hot path has no CPU fallback"
-        )
+    """The current CUDA device; raises when there is none (no CPU fallback)."""
+    global _CUDA_SEEN
+    if not _CUDA_SEEN:  # the device query is slow; a process keeps its GPUs
+        if not torch.cuda.is_available():
+            raise RuntimeError(
+                "qe_b200 needs a CUDA device: the hot path has no CPU fallback"
+            )
+        _CUDA_SEEN = True
     return torch.device("cuda", torch.cuda.current_device())
 
 

@@ -347,6 +347,69 @@ class HpsiGraph:
         return out
 
 
+class HostStreamedHpsi:
+    """H|psi> of host-resident band blocks with the PCIe copies overlapped.
+
+    The bands are cut into chunks; chunk c is copied in on one stream, its
+    H|psi> replayed from a captured graph on the compute stream, and its
+    result copied out on a third stream, so chunk c's compute overlaps chunk
+    c+1's input and chunk c-1's output copies (H|psi> is independent per
+    band).  Host buffers are pinned, with the (nbands, ld) storage layout of
+    the device buffers so that each copy is one contiguous DMA.
+    """
+
+    def __init__(self, ham: PlaneWaveHamiltonian, nbands: int, chunk: int = 64,
+                 buffers: int = 2) -> None:
+        self.ham = ham
+        self.nbands = int(nbands)
+        self.chunk = max(1, min(int(chunk), self.nbands))
+        self.graphs = [HpsiGraph(ham, self.chunk) for _ in range(max(1, int(buffers)))]
+        self.ld = self.graphs[0].input_storage.shape[1]
+        self.copy_in = torch.cuda.Stream(device=ham.device)
+        self.copy_out = torch.cuda.Stream(device=ham.device)
+        self.compute = torch.cuda.Stream(device=ham.device)
+
+    def host_buffers(self) -> tuple[torch.Tensor, torch.Tensor]:
+        """Pinned (nbands, ld) input and output storage; band b's plane-wave
+        coefficients are row b, columns [0, npw)."""
+        dtype = self.ham.dtype
+        make = lambda: torch.zeros((self.nbands, self.ld), dtype=dtype).pin_memory()  # noqa: E731
+        return make(), make()
+
+    def __call__(self, host_in: torch.Tensor, host_out: torch.Tensor) -> None:
+        """host_out = H host_in (both from host_buffers()); returns once the
+        copies are queued; synchronise the device (or copy_out) to read."""
+        if tuple(host_in.shape) != (self.nbands, self.ld) or host_in.shape != host_out.shape:
+            raise ValueError("use buffers of host_buffers()")
+        n = len(self.graphs)
+        ready_in, done_compute, done_out = [], [], []
+        current = torch.cuda.current_stream(self.ham.device)
+        for stream in (self.copy_in, self.copy_out, self.compute):
+            stream.wait_stream(current)
+        for index, start in enumerate(range(0, self.nbands, self.chunk)):
+            stop = min(self.nbands, start + self.chunk)
+            graph = self.graphs[index % n]
+            with torch.cuda.stream(self.copy_in):
+                if index >= n:  # the buffer's previous result has left the device
+                    self.copy_in.wait_event(done_out[index - n])
+                graph.input_storage[:stop - start].copy_(host_in[start:stop], non_blocking=True)
+                if stop - start < self.chunk:
+                    graph.input_storage[stop - start:].zero_()
+                ready_in.append(torch.cuda.Event())
+                ready_in[-1].record(self.copy_in)
+            with torch.cuda.stream(self.compute):
+                self.compute.wait_event(ready_in[-1])
+                graph.replay()
+                done_compute.append(torch.cuda.Event())
+                done_compute[-1].record(self.compute)
+            with torch.cuda.stream(self.copy_out):
+                self.copy_out.wait_event(done_compute[-1])
+                host_out[start:stop].copy_(graph.output_storage[:stop - start], non_blocking=True)
+                done_out.append(torch.cuda.Event())
+                done_out[-1].record(self.copy_out)
+        current.wait_stream(self.copy_out)
+
+
 # ---------------------------------------------------------------------------
 # Davidson
 

@@ -265,9 +265,15 @@ def cgemm_tf32x3(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | 
     if splits is None:
         default = int(lib.qeb_cgemm_tf32x3_default_splits(op_a, m, n, k))
         kblocks = (2 * k + 31) // 32
-        candidates = sorted({default, max(1, default // 2), min(2 * default, max(1, kblocks // 4))})
-        candidates.remove(default)
-        candidates.insert(0, default)
+        tiles = ((m + 127) // 128) * ((n + 127) // 128)
+        if default == 1 and not 148 < tiles < 296:
+            # enough output tiles for full waves: the K split stays off
+            candidates = [1]
+        else:
+            candidates = sorted({default, max(1, default // 2),
+                                 min(2 * default, max(1, kblocks // 4))})
+            candidates.remove(default)
+            candidates.insert(0, default)
         key = f"cgemm_tf32x3/{op_a}/{bucket(m)}/{bucket(n)}/{bucket(k)}"
         probe = []
 
