@@ -404,6 +404,19 @@ def run_b200(args) -> None:
     fp64_graph_ms, fp64_graph = graph_loop("fp64")
     del fp64_graph
 
+    # eigenvalue error of the chosen form's H|psi>: Rayleigh quotients
+    # <psi|H|psi>/<psi|psi> per band, FP32/split-TF32 H against FP64 H on the
+    # same (FP32-representable) vectors, reductions in FP64
+    psi64 = forms["mixed"][2].to(torch.complex128)
+    rq = {}
+    for name in ("mixed", "fp64"):
+        _ws, ham, _psi, _out = forms[name]
+        hpsi = ham.apply(psi64.to(ham.dtype).T.contiguous().T).to(torch.complex128)
+        num = torch.real(torch.sum(psi64.conj() * hpsi, dim=0))
+        den = torch.real(torch.sum(psi64.conj() * psi64, dim=0))
+        rq[name] = (num / den).cpu().numpy()
+    rayleigh_error_ry = float(np.max(np.abs(2.0 * (rq["mixed"] - rq["fp64"]))))
+
     # end to end through the public API with pinned host buffers
     ws, ham, psi_dev, _ = forms["mixed"]
     # end to end from pinned host memory to pinned host memory through the
@@ -495,6 +508,9 @@ def run_b200(args) -> None:
         "staged": {"ms_per_step": staged_ms, "value": world * nb / (staged_ms / 1e3),
                    "note": "same kernels launched one by one with events between stages"},
         "graph": "value/ms_per_step time one CUDA-graph replay of the whole H|psi>",
+        "rayleigh_quotient_error_ry": {
+            "value": rayleigh_error_ry,
+            "note": "max over the 256 bands of |<psi|H|psi>/<psi|psi>| mixed form minus FP64 form"},
         "stages_ms": {n: round(t, 5) for n, t in zip(names, mean_stage)},
         "kernel_shares": shares,
         "fft_passes": {"ms": fft_ms, "algorithmic_bytes": fft_bytes,

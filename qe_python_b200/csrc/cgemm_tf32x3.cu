@@ -305,22 +305,38 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
     const bool aborted = !__all_sync(0xffffffffu, ok) || *abort_v;
     const int row = m0 + quarter * 32 + lane;
     if (!aborted && row < M) {
+      const int cbase = n0 + half * (BN / 2);
+      if (split != nullptr) {
 #pragma unroll
-      for (int j = 0; j < BN / 2; ++j) {
-        const int col = n0 + half * (BN / 2) + j;
-        if (col >= N) continue;
-        const float re = acc[j], im = acc[BN / 2 + j];
-        if (split != nullptr) {
-          split[(int64_t)blockIdx.z * M * N + row + (int64_t)col * M] = make_float2(re, im);
-        } else {
-          float2* c = C + row + (int64_t)col * ldc;
-          float2 v = make_float2(alpha.x * re - alpha.y * im, alpha.x * im + alpha.y * re);
-          if (beta.x != 0.0f || beta.y != 0.0f) {
-            const float2 o = *c;
-            v.x += beta.x * o.x - beta.y * o.y;
-            v.y += beta.x * o.y + beta.y * o.x;
+        for (int j = 0; j < BN / 2; ++j) {
+          const int col = cbase + j;
+          if (col < N)
+            split[(int64_t)blockIdx.z * M * N + row + (int64_t)col * M] =
+                make_float2(acc[j], acc[BN / 2 + j]);
+        }
+      } else {
+        const bool use_beta = beta.x != 0.0f || beta.y != 0.0f;
+        float2* crow = C + row;
+        // 8 columns at a time: their C loads are all issued before the
+        // first store, so the read-modify-write does not wait on one load
+        // per column
+#pragma unroll
+        for (int j0 = 0; j0 < BN / 2; j0 += 8) {
+          float2 old[8];
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            const int col = cbase + j0 + jj;
+            old[jj] = make_float2(0.f, 0.f);
+            if (use_beta && col < N) old[jj] = crow[(int64_t)col * ldc];
           }
-          *c = v;
+#pragma unroll
+          for (int jj = 0; jj < 8; ++jj) {
+            const int col = cbase + j0 + jj;
+            const float re = acc[j0 + jj], im = acc[BN / 2 + j0 + jj];
+            const float vx = alpha.x * re - alpha.y * im + beta.x * old[jj].x - beta.y * old[jj].y;
+            const float vy = alpha.x * im + alpha.y * re + beta.x * old[jj].y + beta.y * old[jj].x;
+            if (col < N) crow[(int64_t)col * ldc] = make_float2(vx, vy);
+          }
         }
       }
     }

@@ -250,6 +250,15 @@ class PlaneWaveHamiltonian:
         with _timer(self.timers, "h_psi"):
             return self._apply(coefficients, out=out)
 
+    def _side_stream(self) -> torch.cuda.Stream:
+        """The stream of the projector products that overlap the FFT passes
+        (one per Hamiltonian and device)."""
+        stream = getattr(self, "_stream_side", None)
+        if stream is None:
+            stream = torch.cuda.Stream(device=self.device)
+            self._stream_side = stream
+        return stream
+
     def add_nonlocal(self, vectors: torch.Tensor, target: torch.Tensor) -> None:
         """target += sum |beta> D <beta|vectors> (calbec, D, add)."""
         if self.projectors.beta is None or vectors.shape[1] == 0:
@@ -281,13 +290,29 @@ class PlaneWaveHamiltonian:
             target = out[:, None] if out.dim() == 1 else out
         if target is None:
             target = empty_f(vectors.shape[0], vectors.shape[1], self.dtype, self.device)
-        with _timer(self.timers, "vloc_psi"):
+        nonlocal_part = self.projectors.beta is not None and vectors.shape[1] > 0
+        if nonlocal_part and self.timers is None:
+            # beta^H psi and D becp need only psi: they run on a side stream
+            # while the FFT passes write the local part into target, and the
+            # projector add joins after both
+            main = torch.cuda.current_stream(self.device)
+            side = self._side_stream()
+            side.wait_stream(main)
+            with torch.cuda.stream(side):
+                coupled = self.couple(self.calbec(vectors))
             self.local_workspace._launch_apply(self._potential, vectors, self._kinetic_kernel, target)
-        if self.projectors.beta is not None and vectors.shape[1] > 0:
-            with _timer(self.timers, "h_psi:calbec"):
-                becp = self.calbec(vectors)
-            with _timer(self.timers, "add_vuspsi"):
-                self.add_projectors(self.couple(becp), target)
+            main.wait_stream(side)
+            coupled.record_stream(main)
+            self.add_projectors(coupled, target)
+        else:
+            with _timer(self.timers, "vloc_psi"):
+                self.local_workspace._launch_apply(self._potential, vectors, self._kinetic_kernel,
+                                                   target)
+            if nonlocal_part:
+                with _timer(self.timers, "h_psi:calbec"):
+                    becp = self.calbec(vectors)
+                with _timer(self.timers, "add_vuspsi"):
+                    self.add_projectors(self.couple(becp), target)
         if host:
             result = as_numpy(target)
             if out is not None and not isinstance(out, torch.Tensor):

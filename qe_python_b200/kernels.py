@@ -23,16 +23,18 @@ _PREC = {torch.complex128: _lib.QEB_F64, torch.complex64: _lib.QEB_F32}
 
 
 class _Scratch:
-    """Grow-only device scratch for split-K partial tiles (per device)."""
+    """Grow-only device scratch for split-K partial tiles, one buffer per
+    (device, stream): products issued on different streams never share it."""
 
     def __init__(self) -> None:
-        self._buffers: dict[torch.device, torch.Tensor] = {}
+        self._buffers: dict[tuple, torch.Tensor] = {}
 
     def get(self, nbytes: int, device: torch.device) -> torch.Tensor:
-        current = self._buffers.get(device)
+        key = (device, torch.cuda.current_stream(device).cuda_stream)
+        current = self._buffers.get(key)
         if current is None or current.numel() < nbytes:
             current = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
-            self._buffers[device] = current
+            self._buffers[key] = current
         return current
 
 
