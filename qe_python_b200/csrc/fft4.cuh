@@ -118,8 +118,11 @@ struct Four {
   static constexpr int G = (N1_ > N2_) ? N1_ : N2_;
   static constexpr int per_warp = 32 / G;
   static constexpr int R = G;  // registers (complex) per lane
-  // exchange buffer of one group: N1 rows of N2 (+1 pad) values
-  static constexpr int xstride = N2_ + 1;
+  // exchange buffer of one group: N1 rows of N2 values at an odd stride, so
+  // the N1 lanes reading one column of it (8-byte or 16-byte values) fall on
+  // distinct banks: N2 + 1 for even N2, N2 itself for odd N2 (an even stride
+  // such as 16 for N2 = 15 put all of them on one bank)
+  static constexpr int xstride = N2_ | 1;
   static constexpr int scratch = N1_ * xstride;
 };
 

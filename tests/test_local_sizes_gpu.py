@@ -88,3 +88,32 @@ def test_density_fast_matches_generic(cuda_device, precision, rtol):
         ws.accumulate_density(rho, psi, weights)
         results.append(rho.cpu().numpy())
     assert np.max(np.abs(results[0] - results[1])) <= rtol * np.max(np.abs(results[1]))
+
+
+FOUR_STEP_LENGTHS = (16, 24, 32, 36, 48, 64, 72, 90, 96, 108, 128, 135, 144, 180)
+
+
+@pytest.mark.parametrize("n", FOUR_STEP_LENGTHS)
+def test_every_four_step_length(cuda_device, n):
+    """Each listed four-step length (cubic n^3 grid, G sphere of radius n/6)
+    in both precisions against the oracle, the factor pairs with an odd N2
+    (8 x 9, 9 x 15, 12 x 15) included: their line groups exchange through a
+    buffer of stride N2."""
+    import torch
+
+    length = 10.0
+    reciprocal = 2.0 * np.pi * np.linalg.inv(np.eye(3) * length).T
+    ecut = (2.0 * np.pi * (n / 6.0) / length) ** 2
+    basis = make_bases(reciprocal, np.zeros(3), ecut)[0]
+    shape = (n, n, n)
+    rng = np.random.default_rng(n)
+    nb = 3
+    psi = np.asfortranarray(rng.standard_normal((len(basis), nb)) + 1j * rng.standard_normal((len(basis), nb)))
+    v = np.ascontiguousarray(rng.uniform(-1.0, 1.0, shape))
+    expected_out = _oracle(basis.indices, shape, psi, v, basis.kinetic)
+    scale = np.max(np.abs(expected_out))
+    for precision, tol in (("f64", 1e-12), ("f32", 3e-5)):
+        ws = _workspace(basis, shape, precision, False)
+        got = ws.apply(torch.from_numpy(v).cuda(), torch.from_numpy(psi).cuda(),
+                       diagonal=torch.from_numpy(basis.kinetic).cuda()).cpu().numpy()
+        assert np.max(np.abs(got - expected_out)) <= tol * scale, precision
