@@ -165,6 +165,167 @@ __global__ void reduce_partials(int M, int N, int splits, const C2<T>* __restric
   }
 }
 
+// ---------------------------------------------------------------------------
+// Skinny products: one side of the output has at most 16 columns.  The tiled
+// kernel above wastes most of a 64-wide tile there and reads the large
+// operand once per tile column; these kernels stream the large operand once
+// from HBM and keep the narrow one in shared memory.  Cases of the hot path:
+// calbec and the projector add for a few unconverged bands, the Davidson
+// rows of a few correction vectors (new^H [HV, V]) and their Ritz columns.
+
+constexpr int kSkinnyMax = 16;
+constexpr int kSkinnyThreads = 256;
+constexpr int kSkinnyColumns = kSkinnyThreads / 32;  // large-operand columns per block (OP_C)
+constexpr int kSkinnyChunkC = 128;                   // K rows staged per step (OP_C)
+constexpr int kSkinnyChunkN = 64;                    // K rows staged per step (OP_N)
+
+int skinny_width(int n) { return n <= 4 ? 4 : (n <= 8 ? 8 : 16); }
+
+// D[mb, ns] = sum_k conj(X[k, mb]) Y[k, ns] over this block's K range, one
+// warp per large column mb, Y rows staged [ns][k].  splits == 1: the block
+// writes C directly; else the partial slice blockIdx.y of P (Mb x Ns).
+// Output mapping: swapped == 0: C[mb, ns] = alpha D + beta C;
+//                 swapped == 1: C[ns, mb] = alpha conj(D) + beta C.
+template <typename T, int NS>
+__global__ void __launch_bounds__(kSkinnyThreads) skinny_c_kernel(
+    int Mb, int Ns, int K, int krange, const C2<T>* __restrict__ X, int64_t ldx,
+    const C2<T>* __restrict__ Y, int64_t ldy, C2<T> alpha, C2<T> beta, C2<T>* C, int64_t ldc,
+    int swapped, C2<T>* __restrict__ P) {
+  __shared__ C2<T> ys[NS][kSkinnyChunkC];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int mb = blockIdx.x * kSkinnyColumns + warp;
+  const int kbeg = blockIdx.y * krange;
+  const int kend = min(K, kbeg + krange);
+  const C2<T> zero = qeb::mk<T>(0, 0);
+  C2<T> acc[NS];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) acc[n] = zero;
+  const C2<T>* xcol = X + (int64_t)(mb < Mb ? mb : 0) * ldx;
+  for (int k0 = kbeg; k0 < kend; k0 += kSkinnyChunkC) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < NS * kSkinnyChunkC; i += kSkinnyThreads) {
+      const int n = i / kSkinnyChunkC, kk = i - n * kSkinnyChunkC;
+      const int k = k0 + kk;
+      ys[n][kk] = (n < Ns && k < kend) ? Y[k + (int64_t)n * ldy] : zero;
+    }
+    __syncthreads();
+    if (mb < Mb) {
+      C2<T> xv[kSkinnyChunkC / 32];
+#pragma unroll
+      for (int j = 0; j < kSkinnyChunkC / 32; ++j) {
+        const int k = k0 + lane + 32 * j;
+        xv[j] = (k < kend) ? xcol[k] : zero;
+      }
+#pragma unroll
+      for (int j = 0; j < kSkinnyChunkC / 32; ++j) {
+        const int kk = lane + 32 * j;
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+          const C2<T> y = ys[n][kk];
+          // conj(x) * y
+          acc[n].re = fma(xv[j].re, y.re, acc[n].re);
+          acc[n].re = fma(xv[j].im, y.im, acc[n].re);
+          acc[n].im = fma(xv[j].re, y.im, acc[n].im);
+          acc[n].im = fma(-xv[j].im, y.re, acc[n].im);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int n = 0; n < NS; ++n) {
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+      acc[n].re += __shfl_xor_sync(0xffffffffu, acc[n].re, off);
+      acc[n].im += __shfl_xor_sync(0xffffffffu, acc[n].im, off);
+    }
+  }
+  if (lane != 0 || mb >= Mb) return;
+  const bool use_beta = beta.re != T(0) || beta.im != T(0);
+#pragma unroll
+  for (int n = 0; n < NS; ++n) {
+    if (n >= Ns) break;
+    if (P != nullptr) {
+      P[(int64_t)blockIdx.y * Mb * Ns + mb + (int64_t)n * Mb] = acc[n];
+    } else {
+      C2<T> d = acc[n];
+      if (swapped) d.im = -d.im;
+      C2<T>* c = swapped ? C + n + (int64_t)mb * ldc : C + mb + (int64_t)n * ldc;
+      C2<T> v = qeb::cmul(alpha, d);
+      if (use_beta) v = v + qeb::cmul(beta, *c);
+      *c = v;
+    }
+  }
+}
+
+// Sum of the skinny partial slices in ascending order, then the output
+// mapping of skinny_c_kernel.
+template <typename T>
+__global__ void skinny_reduce(int Mb, int Ns, int splits, const C2<T>* __restrict__ P,
+                              C2<T> alpha, C2<T> beta, C2<T>* C, int64_t ldc, int swapped) {
+  const int64_t total = (int64_t)Mb * Ns;
+  const bool use_beta = beta.re != T(0) || beta.im != T(0);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    C2<T> d = P[i];
+    for (int s = 1; s < splits; ++s) d = d + P[(int64_t)s * total + i];
+    const int64_t mb = i % Mb, n = i / Mb;
+    if (swapped) d.im = -d.im;
+    C2<T>* c = swapped ? C + n + mb * ldc : C + mb + n * ldc;
+    C2<T> v = qeb::cmul(alpha, d);
+    if (use_beta) v = v + qeb::cmul(beta, *c);
+    *c = v;
+  }
+}
+
+// C[m, n] = alpha sum_k A[m, k] B[k, n] + beta C[m, n] for N <= NS: one
+// thread per row m, B rows staged [k][n] (every lane reads the same entry).
+template <typename T, int NS>
+__global__ void __launch_bounds__(kSkinnyThreads) skinny_n_kernel(
+    int M, int N, int K, C2<T> alpha, const C2<T>* __restrict__ A, int64_t lda,
+    const C2<T>* __restrict__ B, int64_t ldb, C2<T> beta, C2<T>* C, int64_t ldc) {
+  __shared__ C2<T> bs[kSkinnyChunkN][NS];
+  const int m = blockIdx.x * kSkinnyThreads + threadIdx.x;
+  const C2<T> zero = qeb::mk<T>(0, 0);
+  C2<T> acc[NS];
+#pragma unroll
+  for (int n = 0; n < NS; ++n) acc[n] = zero;
+  const C2<T>* arow = A + (m < M ? m : 0);
+  for (int k0 = 0; k0 < K; k0 += kSkinnyChunkN) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < NS * kSkinnyChunkN; i += kSkinnyThreads) {
+      const int n = i / kSkinnyChunkN, kk = i - n * kSkinnyChunkN;
+      const int k = k0 + kk;
+      bs[kk][n] = (n < N && k < K) ? B[k + (int64_t)n * ldb] : zero;
+    }
+    __syncthreads();
+    if (m < M) {
+      const int kn = min(kSkinnyChunkN, K - k0);
+#pragma unroll 8
+      for (int kk = 0; kk < kn; ++kk) {
+        const C2<T> a = arow[(int64_t)(k0 + kk) * lda];
+#pragma unroll
+        for (int n = 0; n < NS; ++n) {
+          const C2<T> b = bs[kk][n];
+          acc[n].re = fma(a.re, b.re, acc[n].re);
+          acc[n].re = fma(-a.im, b.im, acc[n].re);
+          acc[n].im = fma(a.re, b.im, acc[n].im);
+          acc[n].im = fma(a.im, b.re, acc[n].im);
+        }
+      }
+    }
+  }
+  if (m >= M) return;
+  const bool use_beta = beta.re != T(0) || beta.im != T(0);
+#pragma unroll
+  for (int n = 0; n < NS; ++n) {
+    if (n >= N) break;
+    C2<T>* c = C + m + (int64_t)n * ldc;
+    C2<T> v = qeb::cmul(alpha, acc[n]);
+    if (use_beta) v = v + qeb::cmul(beta, *c);
+    *c = v;
+  }
+}
+
 int g_sm_count = 0;
 
 int sm_count() {
@@ -188,6 +349,93 @@ int choose_splits(int M, int N, int K) {
   return s < 1 ? 1 : s;
 }
 
+// Skinny OP_C plan: the narrow side (N, else M when N is wide), the large
+// side Mb and the number of K slices (about four waves, each >= 1024 deep).
+struct SkinnyC {
+  bool use = false, swapped = false;
+  int mb = 0, ns = 0, splits = 1;
+};
+
+SkinnyC skinny_c_plan(int M, int N, int K) {
+  SkinnyC p;
+  if (N <= kSkinnyMax) {
+    p.use = true, p.mb = M, p.ns = N;
+  } else if (M <= kSkinnyMax) {
+    p.use = true, p.swapped = true, p.mb = N, p.ns = M;
+  } else {
+    return p;
+  }
+  const int groups = (p.mb + kSkinnyColumns - 1) / kSkinnyColumns;
+  int want = (4 * sm_count() + groups - 1) / groups;
+  int by_depth = K / 1024;
+  if (by_depth < 1) by_depth = 1;
+  int s = want < by_depth ? want : by_depth;
+  if (s > 64) s = 64;
+  p.splits = s < 1 ? 1 : s;
+  return p;
+}
+
+template <typename T, int NS>
+void launch_skinny_c(const SkinnyC& p, int K, int krange, const C2<T>* X, int64_t ldx,
+                     const C2<T>* Y, int64_t ldy, C2<T> al, C2<T> be, C2<T>* C, int64_t ldc,
+                     C2<T>* partials, cudaStream_t stream) {
+  const dim3 grid((p.mb + kSkinnyColumns - 1) / kSkinnyColumns, p.splits);
+  skinny_c_kernel<T, NS><<<grid, kSkinnyThreads, 0, stream>>>(
+      p.mb, p.ns, K, krange, X, ldx, Y, ldy, al, be, C, ldc, p.swapped ? 1 : 0, partials);
+}
+
+template <typename T>
+int gemm_skinny_c(int M, int N, int K, C2<T> al, const C2<T>* A, int64_t lda, const C2<T>* B,
+                  int64_t ldb, C2<T> be, C2<T>* C, int64_t ldc, void* scratch,
+                  int64_t scratch_bytes, cudaStream_t stream) {
+  SkinnyC p = skinny_c_plan(M, N, K);
+  const int64_t slice_bytes = (int64_t)p.mb * p.ns * (int64_t)sizeof(C2<T>);
+  if (p.splits > 1) {
+    const int64_t fit = (scratch == nullptr) ? 0 : scratch_bytes / slice_bytes;
+    if (fit < p.splits) p.splits = (int)(fit < 1 ? 1 : fit);
+  }
+  int krange = (K + p.splits - 1) / p.splits;
+  krange = (krange + kSkinnyChunkC - 1) / kSkinnyChunkC * kSkinnyChunkC;
+  if (krange < 1) krange = kSkinnyChunkC;
+  p.splits = K > 0 ? (K + krange - 1) / krange : 1;
+  // large operand X and narrow operand Y of D = X^H Y
+  const C2<T>* X = p.swapped ? B : A;
+  const C2<T>* Y = p.swapped ? A : B;
+  const int64_t ldx = p.swapped ? ldb : lda, ldy = p.swapped ? lda : ldb;
+  C2<T>* partials = p.splits > 1 ? static_cast<C2<T>*>(scratch) : nullptr;
+  const int width = skinny_width(p.ns);
+  if (width == 4)
+    launch_skinny_c<T, 4>(p, K, krange, X, ldx, Y, ldy, al, be, C, ldc, partials, stream);
+  else if (width == 8)
+    launch_skinny_c<T, 8>(p, K, krange, X, ldx, Y, ldy, al, be, C, ldc, partials, stream);
+  else
+    launch_skinny_c<T, 16>(p, K, krange, X, ldx, Y, ldy, al, be, C, ldc, partials, stream);
+  qeb::count_launches(p.splits > 1 ? 2 : 1);
+  if (p.splits > 1) {
+    const int64_t total = (int64_t)p.mb * p.ns;
+    int blocks = (int)((total + 255) / 256);
+    if (blocks > 4 * sm_count()) blocks = 4 * sm_count();
+    skinny_reduce<T><<<blocks, 256, 0, stream>>>(p.mb, p.ns, p.splits, partials, al, be, C, ldc,
+                                                p.swapped ? 1 : 0);
+  }
+  return qeb::cuda_status(cudaGetLastError(), "zgemm skinny launch");
+}
+
+template <typename T>
+int gemm_skinny_n(int M, int N, int K, C2<T> al, const C2<T>* A, int64_t lda, const C2<T>* B,
+                  int64_t ldb, C2<T> be, C2<T>* C, int64_t ldc, cudaStream_t stream) {
+  const dim3 grid((M + kSkinnyThreads - 1) / kSkinnyThreads);
+  const int width = skinny_width(N);
+  if (width == 4)
+    skinny_n_kernel<T, 4><<<grid, kSkinnyThreads, 0, stream>>>(M, N, K, al, A, lda, B, ldb, be, C, ldc);
+  else if (width == 8)
+    skinny_n_kernel<T, 8><<<grid, kSkinnyThreads, 0, stream>>>(M, N, K, al, A, lda, B, ldb, be, C, ldc);
+  else
+    skinny_n_kernel<T, 16><<<grid, kSkinnyThreads, 0, stream>>>(M, N, K, al, A, lda, B, ldb, be, C, ldc);
+  qeb::count_launches(1);
+  return qeb::cuda_status(cudaGetLastError(), "zgemm skinny launch");
+}
+
 template <typename T>
 int gemm(int opa, int M, int N, int K, const double* alpha, const void* A, int64_t lda,
          const void* B, int64_t ldb, const double* beta, void* C, int64_t ldc, void* scratch,
@@ -209,6 +457,14 @@ int gemm(int opa, int M, int N, int K, const double* alpha, const void* A, int64
   }
   const C2<T> al = qeb::mk<T>((T)alpha[0], (T)alpha[1]);
   const C2<T> be = qeb::mk<T>((T)beta[0], (T)beta[1]);
+  if (K > 0 && opa == QEB_OP_C && (N <= kSkinnyMax || M <= kSkinnyMax))
+    return gemm_skinny_c<T>(M, N, K, al, static_cast<const C2<T>*>(A), lda,
+                            static_cast<const C2<T>*>(B), ldb, be, static_cast<C2<T>*>(C), ldc,
+                            scratch, scratch_bytes, stream);
+  if (K > 0 && opa == QEB_OP_N && N <= kSkinnyMax)
+    return gemm_skinny_n<T>(M, N, K, al, static_cast<const C2<T>*>(A), lda,
+                            static_cast<const C2<T>*>(B), ldb, be, static_cast<C2<T>*>(C), ldc,
+                            stream);
   const size_t smem = sizeof(Tile<T>);
   static bool configured[2] = {false, false};
   if (!configured[opa]) {
@@ -258,6 +514,10 @@ int gemm(int opa, int M, int N, int K, const double* alpha, const void* A, int64
 extern "C" int64_t qeb_zgemm_scratch_bytes(int opa, int M, int N, int K, int precision) {
   if (opa != QEB_OP_C || M <= 0 || N <= 0 || K <= 0) return 0;
   const int64_t elem = (precision == QEB_F64) ? 16 : 8;
+  if (N <= kSkinnyMax || M <= kSkinnyMax) {
+    const SkinnyC p = skinny_c_plan(M, N, K);
+    return p.splits > 1 ? (int64_t)p.splits * p.mb * p.ns * elem : 0;
+  }
   const int splits = choose_splits(M, N, K);
   return splits > 1 ? (int64_t)splits * M * N * elem : 0;
 }

@@ -216,7 +216,7 @@ class PlaneWaveHamiltonian:
     def calbec(self, vectors: torch.Tensor) -> torch.Tensor:
         """becp = beta^H psi (projector_overlaps, _native_fft.pyx:694-731)."""
         p = self.projectors
-        if self.tensor_gemm:
+        if self.tensor_gemm and not K.is_skinny(K.OP_C, p.beta.shape[1], vectors.shape[1]):
             out = K.cgemm_tf32x3(K.OP_C, p.beta, vectors)
             if out is not None:
                 return out
@@ -230,7 +230,7 @@ class PlaneWaveHamiltonian:
     def add_projectors(self, coupled: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
         """target += beta coupled (add_projector_product, _native_fft.pyx:782-836)."""
         p = self.projectors
-        if self.tensor_gemm:
+        if self.tensor_gemm and not K.is_skinny(K.OP_N, p.beta.shape[0], coupled.shape[1]):
             out = K.cgemm_tf32x3(K.OP_N, p.beta, coupled, target, beta=1.0)
             if out is not None:
                 return out
@@ -508,7 +508,7 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
              initial_is_orthonormal: bool = False, initial_eigenvalues=None,
              initial_applied=None, mpi=None, global_dimension: int | None = None,
              global_row_indices=None, timers=None, operator_into=None,
-             dtype: torch.dtype | None = None) -> DavidsonResult:
+             dtype: torch.dtype | None = None, lock_converged: bool = False) -> DavidsonResult:
     """Lowest eigenpairs by restarted block Davidson (diagonalization.py:527-880).
 
     ``operator(C)`` / ``operator_into(C, out)`` act on column-major device
@@ -524,7 +524,8 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
                            initial_is_orthonormal=initial_is_orthonormal,
                            initial_eigenvalues=initial_eigenvalues,
                            initial_applied=initial_applied, global_dimension=global_dimension,
-                           global_row_indices=global_row_indices, timers=timers, dtype=dtype)
+                           global_row_indices=global_row_indices, timers=timers, dtype=dtype,
+                           lock_converged=lock_converged)
 
     def apply_into(vectors, destination):
         if operator_into is not None:
@@ -601,10 +602,18 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
                    initial_is_ritz: bool = False, initial_is_orthonormal: bool = False,
                    initial_eigenvalues=None, initial_applied=None,
                    global_dimension: int | None = None, global_row_indices=None, timers=None,
-                   dtype: torch.dtype | None = None):
+                   dtype: torch.dtype | None = None, lock_converged: bool = False):
     """The Davidson algorithm of ``davidson`` as a generator: it yields
     ``(vectors, destination)`` whenever it needs destination = H vectors and
-    returns the DavidsonResult (StopIteration.value)."""
+    returns the DavidsonResult (StopIteration.value).
+
+    ``lock_converged`` (chosen form; the reference never locks): at each
+    restart the roots already converged leave the reduced problem.  Their
+    Ritz vectors are kept aside, later corrections are projected out of
+    their span, and the restarted subspace holds only the unconverged roots,
+    so the FP64 reduced eigensolve of the following iterations has the size
+    of the unconverged set instead of all roots.  Results differ from the
+    unlocked solve below the convergence threshold of the locked roots."""
     device = require_cuda()
     diag = to_device_f(diagonal, torch.float64, device).reshape(-1)
     local_dimension = diag.numel()
@@ -687,11 +696,15 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
             projected[block, block] = _hermitize(projected[block, block])
             overlap[block, block] = _hermitize(overlap[block, block])
 
+    nroot = number_of_roots  # roots of the reduced problem (fewer once some are locked)
+    root_ids = np.arange(number_of_roots)  # their indices among all roots
+    locked = {"vectors": None, "count": 0, "values": [], "ids": [], "norms": []}
+
     def ritz_values():
         """Lowest roots and coefficients of the reduced problem (:699-708)."""
         with _timer(timers, "cdiaghg"):
             roots, coefficients = lowest_generalized_eigh(
-                projected[:active, :active], overlap[:active, :active], number_of_roots)
+                projected[:active, :active], overlap[:active, :active], nroot)
         return roots.cpu().numpy(), roots, coefficients
 
     def ritz_columns(coefficients, roots, columns=None):
@@ -752,6 +765,11 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
         previous = values
         with _timer(timers, "g_psi"):
             corrections = K.precondition(block, energies, diag)
+        if locked["count"]:
+            span = locked["vectors"][:, :locked["count"]]
+            for _ in range(2):  # classical Gram-Schmidt, repeated once
+                K.gemm(K.OP_N, span, K.gemm(K.OP_C, span, corrections), corrections,
+                       alpha=-1.0, beta=1.0)
         # Normalise (cegterg), dropping columns below 1e-14 of the largest norm (:500-524).
         norms2 = K.column_squared_norms(corrections)
         norms_host = norms2.cpu().numpy()
@@ -774,11 +792,12 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
         if track:
             ritz_vectors, residuals = full_ritz()
             residual_norms = residual_norms_of(residuals)
-        converged = np.abs(values - previous) < root_tolerances
+        tolerances = root_tolerances[root_ids]
+        converged = np.abs(values - previous) < tolerances
         if residual_factor is not None:
-            converged &= residual_norms < residual_factor * root_tolerances
+            converged &= residual_norms < residual_factor * tolerances
         if residual_energy_scale is not None:
-            converged &= residual_norms ** 2 < residual_energy_scale * root_tolerances
+            converged &= residual_norms ** 2 < residual_energy_scale * tolerances
         unconverged = ~converged
         unconverged_count = int(np.count_nonzero(unconverged))
         if unconverged_count == 0:
@@ -786,15 +805,59 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
                 ritz_vectors, residuals = full_ritz()
             if not track:
                 residual_norms = residual_norms_of(residuals)
-            return DavidsonResult(values, ritz_vectors, residual_norms, iteration, True, 0,
-                                  applications)
+            return DavidsonResult(*_with_locked(locked, root_ids, values, ritz_vectors,
+                                                residual_norms),
+                                  iteration, True, 0, applications)
         index = torch.as_tensor(np.flatnonzero(unconverged), device=device)
-        if active + unconverged_count > maximum_subspace:
+        lockable = None
+        if lock_converged and active + unconverged_count > maximum_subspace:
+            # Roots that may leave the reduced problem: converged, occupied
+            # (tight threshold) and with |r|^2 below that threshold, so the
+            # eigenvalue error of the frozen vector is below it as well.
+            if residuals is None:
+                ritz_vectors, residuals = full_ritz()
+            norms_now = residual_norms if track else residual_norms_of(residuals)
+            lockable = converged & (root_ids < occupied_roots) & (norms_now ** 2 < tolerance)
+            if not lockable.any():
+                lockable = None
+        if lockable is not None:
+            # Lock them and restart on the Ritz block of the others.
+            with _timer(timers, "cegterg:last"):
+                keep_roots = ~lockable
+                done = torch.as_tensor(np.flatnonzero(lockable), device=device)
+                rest = torch.as_tensor(np.flatnonzero(keep_roots), device=device)
+                count = done.numel()
+                if locked["vectors"] is None:
+                    locked["vectors"] = empty_f(local_dimension, number_of_roots, dtype, device)
+                first = locked["count"]
+                locked["vectors"][:, first:first + count] = _select_columns(ritz_vectors, done)
+                locked["count"] = first + count
+                locked["values"].extend(values[lockable].tolist())
+                locked["ids"].extend(root_ids[lockable].tolist())
+                locked["norms"].extend(np.asarray(norms_now[lockable]).tolist())
+                nroot = int(np.count_nonzero(keep_roots))
+                root_ids = root_ids[keep_roots]
+                values = values[keep_roots]
+                values_dev = values_dev.index_select(0, rest)
+                if track:
+                    residual_norms = residual_norms[keep_roots]
+                ritz_vectors = _select_columns(ritz_vectors, rest)
+                residuals = _select_columns(residuals, rest)
+                active = nroot
+                basis_storage[:, :active] = ritz_vectors
+                applied_storage[:, :active] = residuals
+                K.subtract_band_energies(applied_storage[:, :active], ritz_vectors, -values_dev)
+                projected[:active, :active] = torch.diag(values_dev.to(torch.complex128))
+                overlap[:active, :active] = torch.eye(active, dtype=torch.complex128, device=device)
+                unconverged = unconverged[keep_roots]
+                index = torch.as_tensor(np.flatnonzero(unconverged), device=device)
+            coefficients = None
+        elif active + unconverged_count > maximum_subspace:
             # Restart on the Ritz block without a new H application (:843-868).
             if residuals is None:
                 ritz_vectors, residuals = full_ritz()
             with _timer(timers, "cegterg:last"):
-                active = number_of_roots
+                active = nroot
                 basis_storage[:, :active] = ritz_vectors
                 # H psi = residual + e psi, rebuilt in place (:855-860).
                 applied_storage[:, :active] = residuals
@@ -814,5 +877,25 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
         ritz_vectors, residuals = full_ritz()
     if not track:
         residual_norms = residual_norms_of(residuals)
-    return DavidsonResult(values, ritz_vectors, residual_norms, completed, False,
-                          unconverged_count, applications)
+    return DavidsonResult(*_with_locked(locked, root_ids, values, ritz_vectors, residual_norms),
+                          completed, False, unconverged_count, applications)
+
+
+def _select_columns(matrix: torch.Tensor, index: torch.Tensor) -> torch.Tensor:
+    """Columns ``index`` of a column-major matrix, column-major."""
+    return matrix.T.index_select(0, index).T
+
+
+def _with_locked(locked: dict, root_ids, values, vectors, norms):
+    """(eigenvalues, eigenvectors, residual norms) of all roots: the locked
+    ones and those of the reduced problem, in ascending eigenvalue order."""
+    count = locked["count"]
+    if not count:
+        return values, vectors, norms
+    all_values = np.concatenate([np.asarray(locked["values"]), np.asarray(values)])
+    all_norms = np.concatenate([np.asarray(locked["norms"]), np.asarray(norms)])
+    order = np.argsort(all_values, kind="stable")
+    stacked = torch.cat([locked["vectors"][:, :count], vectors], dim=1)
+    out = empty_f(stacked.shape[0], stacked.shape[1], stacked.dtype, stacked.device)
+    out.copy_(_select_columns(stacked, torch.as_tensor(order, device=stacked.device)))
+    return all_values[order], out, all_norms[order]

@@ -58,19 +58,30 @@ def _check_matrix(name: str, t: torch.Tensor) -> None:
 TENSOR_MIN_MACS = 1 << 21
 
 
+SKINNY_MAX = 16  # narrow output side at or below which qeb_zgemm/qeb_cgemm stream the wide operand
+
+
+def is_skinny(op_a: int, m: int, n: int) -> bool:
+    """Whether the FMA library routes op(a) b (output m x n) to its skinny
+    kernels: n <= 16, or m <= 16 for op_a = OP_C.  Those stream the large
+    operand once at HBM speed, which the tiled tensor-core kernel cannot do
+    for so narrow an output."""
+    return n <= SKINNY_MAX or (op_a == OP_C and m <= SKINNY_MAX)
+
+
 def gemm(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = None,
          alpha: complex = 1.0, beta: complex = 0.0, tensor: bool | None = None) -> torch.Tensor:
     """c = alpha op(a) b + beta c with op(a) = a (OP_N) or a^H (OP_C).
 
     complex128: FP64 (qeb_zgemm).  complex64: split-TF32 tensor-core products
     (qeb_cgemm_tf32x3) when ``tensor`` is True, or when it is None and the
-    product is large; else FP32 FMA (qeb_cgemm).
+    product is large and not skinny; else FP32 FMA (qeb_cgemm).
     """
     if tensor is not False and a.dtype == torch.complex64 and b.dtype == torch.complex64:
         m = a.shape[1] if op_a == OP_C else a.shape[0]
         k = a.shape[0] if op_a == OP_C else a.shape[1]
         n = b.shape[1] if b.dim() == 2 else 1
-        if tensor or m * n * k >= TENSOR_MIN_MACS:
+        if tensor or (m * n * k >= TENSOR_MIN_MACS and not is_skinny(op_a, m, n)):
             out = cgemm_tf32x3(op_a, a, b, c, alpha, beta)
             if out is not None:
                 return out

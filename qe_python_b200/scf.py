@@ -419,7 +419,7 @@ MIN_FP64_ITERATIONS = 3  # mixed form: FP64 iterations before convergence is acc
 
 
 def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, tol, occ_roots,
-                   is_ritz, timers):
+                   is_ritz, timers, lock=False):
     """One k point's diagonalisation as a generator of H applications: the
     Davidson of qepy_pw/pw/scf.py:3496-3556 (20 iterations), repeated up to
     five more times from its last vectors while more than five roots remain
@@ -432,7 +432,7 @@ def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, to
             subspace_multiplier=system.diago_david_ndim, residual_factor=None,
             residual_energy_scale=None, occupied_roots=occ_roots, initial_is_ritz=is_ritz,
             initial_is_orthonormal=True, initial_eigenvalues=eigs, initial_applied=applied,
-            timers=timers, dtype=ham.dtype)
+            timers=timers, dtype=ham.dtype, lock_converged=lock)
         attempt += 1
         total_its += sol.iterations
         if sol.converged or sol.number_unconverged <= 5 or attempt >= 6:
@@ -453,7 +453,7 @@ def _drive(steps, ham):
 
 def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             progress=None, timers=None, pools=None, fp32_floor: float = 2.0e-6,
-            batch_kpoints: bool | None = None) -> SCFResult:
+            batch_kpoints: bool | None = None, lock_converged: bool | None = None) -> SCFResult:
     """Converge the Kohn-Sham density to ``system.conv_thr`` (Ry) on the GPU.
 
     ``timers``: optional object with a ``measure(name)`` context manager,
@@ -463,9 +463,15 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     forces are combined over the pools.  ``batch_kpoints`` (default: on for
     the mixed form) runs the k points' Davidson solves in lockstep with one
     launch per FFT pass for all of them; the results are those of the
-    k-by-k loop."""
+    k-by-k loop.  ``lock_converged`` (off unless asked for) locks the
+    converged roots at each Davidson restart (``davidson_steps``; the
+    reference never locks).  On the 216-atom cell it made each Davidson
+    iteration cheaper, but the locked vectors, frozen at the Davidson
+    threshold, held the FP32 iterations near dr2 = 5e-5 Ry and the SCF took
+    more iterations overall."""
     if batch_kpoints is None:
         batch_kpoints = precision == "mixed"
+    lock_converged = bool(lock_converged)
     if precision not in ("f64", "mixed"):
         raise ValueError("precision must be 'f64' or 'mixed'")
     device = require_cuda()
@@ -593,7 +599,8 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             occ_roots = occupied if iteration > 1 and not smeared else system.nbnd
             hams[k] = ham
             solves[k] = _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied,
-                                       tol, occ_roots, iteration == 1, timers)
+                                       tol, occ_roots, iteration == 1, timers,
+                                       lock=lock_converged)
         k_order = sorted(solves)
         if batch_kpoints and len(k_order) > 1:
             # chosen form: the k points' Davidson solves advance together and

@@ -149,8 +149,12 @@ def test_hamiltonian_matches_oracle_composition(cuda_device):
     np.testing.assert_allclose(h.diagonal.cpu().numpy(), want, rtol=1e-12, atol=1e-12)
 
 
+@pytest.mark.parametrize("lock", [False, True])
 @pytest.mark.parametrize("precision,tol", [("f64", 1e-9), ("f32", 2e-5)])
-def test_davidson_matches_dense_eigenvalues(cuda_device, precision, tol):
+def test_davidson_matches_dense_eigenvalues(cuda_device, precision, tol, lock):
+    """With ``lock_converged`` the roots converged at a restart leave the
+    reduced problem (subspace of twice the roots, so restarts happen); the
+    eigenpairs must be the same to the tolerance."""
     import torch
 
     basis, shape, vr, species, phases, coupling = _system(seed=5)
@@ -169,9 +173,10 @@ def test_davidson_matches_dense_eigenvalues(cuda_device, precision, tol):
     # eigenvalue change alone (residual_factor=None, as the SCF driver calls it)
     result = davidson(h.apply, h.diagonal, 8, initial_vectors=_f(start).to(dtype),
                       tolerance=1e-11 if precision == "f64" else 1e-6, max_iterations=200,
-                      subspace_multiplier=4, operator_into=h.apply_into,
-                      residual_factor=10.0 if precision == "f64" else None)
+                      subspace_multiplier=2 if lock else 4, operator_into=h.apply_into,
+                      residual_factor=10.0 if precision == "f64" else None, lock_converged=lock)
     assert result.converged
+    assert np.all(np.diff(result.eigenvalues) >= 0)
     np.testing.assert_allclose(result.eigenvalues, exact, atol=tol)
     # Ritz vectors are H-eigenvectors: ||H x - e x|| small
     hx = h.apply(result.eigenvectors)
@@ -225,3 +230,35 @@ def test_davidson_matches_reference_golden(cuda_device):
     np.testing.assert_allclose(result.eigenvalues, d["eigenvalues"], atol=5e-9)
     # the trajectory follows the reference's within a couple of iterations
     assert abs(result.iterations - float(d["iterations"])) <= 2
+
+
+@pytest.mark.parametrize("op,m,n,k", [
+    (K.OP_C, 300, 3, 30000),   # calbec of a few bands: narrow N, split K
+    (K.OP_C, 5, 700, 30000),   # Davidson rows of a few new vectors: narrow M (swapped)
+    (K.OP_C, 16, 16, 2000),    # both narrow, at the limit
+    (K.OP_C, 40, 9, 100),      # one K slice
+    (K.OP_N, 30000, 3, 960),   # Ritz columns / projector add of a few bands
+    (K.OP_N, 5000, 16, 37),    # ragged K chunk
+    (K.OP_N, 77, 1, 1),
+])
+@pytest.mark.parametrize("dtype,rtol", [(np.complex128, 1e-13), (np.complex64, 2e-6)])
+def test_skinny_products(cuda_device, op, m, n, k, dtype, rtol):
+    """Outputs with at most 16 columns on one side go through the streaming
+    kernels of qeb_zgemm / qeb_cgemm; strided operands (leading dimension
+    above the row count) and alpha, beta != 0 included."""
+    import torch
+
+    rng = np.random.default_rng(m + 7 * n + 13 * k)
+    def rnd(*shape):
+        return (rng.standard_normal(shape) + 1j * rng.standard_normal(shape)).astype(dtype)
+    rows_a = k if op == K.OP_C else m
+    a_full, b_full, c_full = rnd(rows_a + 3, (m if op == K.OP_C else k)), rnd(k + 5, n), rnd(m + 2, n)
+    a, b, c0 = a_full[:rows_a], b_full[:k], c_full[:m]
+    alpha, beta = 0.3 + 0.9j, -0.5 + 0.25j
+    ta, tb, tc = _f(a_full)[:rows_a], _f(b_full)[:k], _f(c_full.copy())[:m]
+    assert K.is_skinny(op, m, n)
+    got = K.gemm(op, ta, tb, tc, alpha=alpha, beta=beta).cpu().numpy()
+    a64, b64 = a.astype(np.complex128), b.astype(np.complex128)
+    exp = alpha * ((a64.conj().T if op == K.OP_C else a64) @ b64) + beta * c0
+    scale = max(1.0, np.sqrt(k)) * max(1.0, np.max(np.abs(exp)))
+    assert np.max(np.abs(got - exp)) <= rtol * scale
