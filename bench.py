@@ -71,21 +71,25 @@ def parse_args():
 def scf_times(name: str) -> dict:
     """Wall time of the GPU SCF to conv_thr = 1e-8 Ry, plain FP64 and mixed,
     with the mixed form's energy, eigenvalue and force differences from the
-    FP64 run."""
+    FP64 run.  A third run, FP64 with the mixed form's guard bands
+    (``f64_guard_bands``), separates what the guard bands save from what the
+    precision saves."""
     import torch
 
-    from qe_python_b200.scf import benchmark_system, run_scf
+    from qe_python_b200.scf import MIXED_GUARD_BANDS, benchmark_system, run_scf
 
     out = {"cell": name, "conv_thr_ry": 1.0e-8}
     results = {}
-    for precision in ("f64", "mixed"):
+    runs = (("f64", "f64", {}), ("mixed", "mixed", {}),
+            ("f64_guard_bands", "f64", {"guard_bands": MIXED_GUARD_BANDS}))
+    for label, precision, options in runs:
         system = benchmark_system(name)
         torch.cuda.synchronize()
         started = time.perf_counter()
-        result = run_scf(system, precision=precision)
+        result = run_scf(system, precision=precision, **options)
         torch.cuda.synchronize()
-        results[precision] = result
-        out[precision] = {
+        results[label] = result
+        out[label] = {
             "seconds": time.perf_counter() - started,
             "converged": bool(result.converged),
             "iterations": result.iterations,
@@ -95,6 +99,9 @@ def scf_times(name: str) -> dict:
             "phase_seconds": {k: round(v, 3) for k, v in result.timings.items()},
         }
     out["mixed_speedup"] = out["f64"]["seconds"] / out["mixed"]["seconds"]
+    out["guard_bands"] = MIXED_GUARD_BANDS
+    out["mixed_speedup_over_f64_guard_bands"] = (out["f64_guard_bands"]["seconds"]
+                                                 / out["mixed"]["seconds"])
     out["energy_difference_ry"] = out["mixed"]["total_energy_ry"] - out["f64"]["total_energy_ry"]
     a, b = results["mixed"], results["f64"]
     out["max_eigenvalue_difference_ry"] = max(

@@ -416,10 +416,11 @@ def projector_terms(system: System, tables: dict, basis) -> tuple:
 
 
 MIN_FP64_ITERATIONS = 3  # mixed form: FP64 iterations before convergence is accepted
+MIXED_GUARD_BANDS = 24  # mixed form: extra Davidson roots beyond nbnd (run_scf guard_bands)
 
 
 def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, tol, occ_roots,
-                   is_ritz, timers, lock=False):
+                   is_ritz, timers, lock=False, nroots=None):
     """One k point's diagonalisation as a generator of H applications: the
     Davidson of qepy_pw/pw/scf.py:3496-3556 (20 iterations), repeated up to
     five more times from its last vectors while more than five roots remain
@@ -428,7 +429,8 @@ def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, to
     vectors, eigs, applied = start_vectors, initial_eigs, initial_applied
     while True:
         sol = yield from davidson_steps(
-            ham.diagonal, system.nbnd, initial_vectors=vectors, tolerance=tol, max_iterations=20,
+            ham.diagonal, nroots or system.nbnd, initial_vectors=vectors, tolerance=tol,
+            max_iterations=20,
             subspace_multiplier=system.diago_david_ndim, residual_factor=None,
             residual_energy_scale=None, occupied_roots=occ_roots, initial_is_ritz=is_ritz,
             initial_is_orthonormal=True, initial_eigenvalues=eigs, initial_applied=applied,
@@ -453,7 +455,8 @@ def _drive(steps, ham):
 
 def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             progress=None, timers=None, pools=None, fp32_floor: float = 2.0e-6,
-            batch_kpoints: bool | None = None, lock_converged: bool | None = None) -> SCFResult:
+            batch_kpoints: bool | None = None, lock_converged: bool | None = None,
+            guard_bands: int | None = None) -> SCFResult:
     """Converge the Kohn-Sham density to ``system.conv_thr`` (Ry) on the GPU.
 
     ``timers``: optional object with a ``measure(name)`` context manager,
@@ -472,6 +475,18 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     if batch_kpoints is None:
         batch_kpoints = precision == "mixed"
     lock_converged = bool(lock_converged)
+    # ``guard_bands`` (chosen form): Davidson solves nbnd + guard roots, the
+    # guard roots at the loose threshold of empty bands; only the nbnd
+    # requested bands enter occupations, density and energies.  Under
+    # smearing every requested band converges to the tight threshold, and a
+    # multiplet cut by the last one converges slowly; with fixed occupations
+    # the empty requested bands already play that part.  Default: on for the
+    # mixed form with smearing.  The plain form solves exactly nbnd roots, as
+    # the reference does.
+    if guard_bands is None:
+        guard_bands = MIXED_GUARD_BANDS if (precision == "mixed"
+                                            and system.occupations == "smearing") else 0
+    guard_bands = max(0, int(guard_bands))
     if precision not in ("f64", "mixed"):
         raise ValueError("precision must be 'f64' or 'mixed'")
     device = require_cuda()
@@ -499,6 +514,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     bases = make_bases(reciprocal, system.kpoints, system.ecutwfc)
     if min(len(b) for b in bases) < system.nbnd:
         raise ValueError("nbnd exceeds the smallest plane-wave basis")
+    nsolve = min(system.nbnd + guard_bands, min(len(b) for b in bases))
     shape = fft_shape(bases, reciprocal, system.ecutrho, fft_factors(system.operations))
     grid = ChargeGrid(shape, reciprocal, system.ecutrho)
     tables = {label: SpeciesTables(p, volume) for label, p in system.pseudos.items()}
@@ -572,7 +588,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             if k not in local_k:
                 if state.vectors is None and iteration == 1 and not random_drawn[k]:
                     # keep the shared random stream in step with one rank
-                    rng.pairs(len(state.basis), system.nbnd)
+                    rng.pairs(len(state.basis), nsolve)
                     random_drawn[k] = True
                 continue
             ws = state.workspace(current_precision)
@@ -588,7 +604,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             initial_eigs = None
             if state.vectors is None:
                 start_vectors, initial_eigs, initial_applied = random_starting_subspace(
-                    ham, state.basis, rng, system.nbnd)
+                    ham, state.basis, rng, nsolve)
                 random_drawn[k] = True
             else:
                 start_vectors = state.vectors.to(ham.dtype).T.contiguous().T
@@ -600,7 +616,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             hams[k] = ham
             solves[k] = _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied,
                                        tol, occ_roots, iteration == 1, timers,
-                                       lock=lock_converged)
+                                       lock=lock_converged, nroots=nsolve)
         k_order = sorted(solves)
         if batch_kpoints and len(k_order) > 1:
             # chosen form: the k points' Davidson solves advance together and
@@ -614,7 +630,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             state = states[k]
             its.append(total_its)
             state.vectors = sol.eigenvectors.to(torch.complex128).T.contiguous().T
-            state.eigenvalues = np.asarray(sol.eigenvalues)
+            state.eigenvalues = np.asarray(sol.eigenvalues)[:system.nbnd]
             local_eigenvalues[k] = state.eigenvalues
         david_its.append(float(np.mean(its)))
         if pools is not None:
