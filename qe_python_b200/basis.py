@@ -222,6 +222,21 @@ def make_bases(reciprocal, k_crystal, ecut_ry: float, *, mpi=None) -> list[Plane
     ]
 
 
+def _charge_extent(reciprocal: np.ndarray, ecut_ry: float) -> np.ndarray:
+    """Largest |Miller index| per axis over the k = 0 sphere 1/2 |G|^2 <=
+    ecut + 1e-12: the rows make_bases would select at k = 0, without their
+    (order-only) energy sort."""
+    ecut_ha = 0.5 * float(ecut_ry)
+    sigma_min = float(np.linalg.svd(reciprocal, compute_uv=False)[-1])
+    bound = int(_search_bound(reciprocal, np.zeros(3), ecut_ha, sigma_min))
+    cube = _miller_cube(bound)
+    g = cube @ reciprocal
+    inside = 0.5 * np.einsum("ij,ij->i", g, g) <= ecut_ha + _CUTOFF_SLACK
+    if not inside.any():
+        raise ValueError("ecutrho produces an empty charge sphere")
+    return np.max(np.abs(cube[inside]), axis=0)
+
+
 def make_basis(reciprocal, k_crystal, ecut_ry: float) -> PlaneWaveBasis:
     return make_bases(reciprocal, k_crystal, ecut_ry)[0]
 
@@ -239,8 +254,7 @@ def fft_shape(bases, reciprocal=None, ecutrho_ry=None, fft_factors=(1, 1, 1)) ->
     if (reciprocal is None) != (ecutrho_ry is None):
         raise ValueError("reciprocal and ecutrho_ry must be supplied together")
     if reciprocal is not None:
-        charge = make_basis(np.asarray(reciprocal, dtype=float), np.zeros(3), float(ecutrho_ry))
-        extent = np.max(np.abs(charge.indices), axis=0)
+        extent = _charge_extent(np.asarray(reciprocal, dtype=float), float(ecutrho_ry))
         shape = []
         for n, factor in zip(extent, fft_factors):
             length = int(2 * n + 1)

@@ -22,6 +22,7 @@ from scipy.special import erfc
 
 from . import kernels as K
 from .device import empty_f, to_device_f
+from .pseudo_tables import _real_space_blocks
 
 
 def ewald_forces(lattice, positions, charges, ecutrho_ry, g_vectors) -> np.ndarray:
@@ -44,22 +45,27 @@ def ewald_forces(lattice, positions, charges, ecutrho_ry, g_vectors) -> np.ndarr
     weight = 2.0 * np.pi / volume * np.exp(-g2 / (4.0 * alpha)) / g2
     forces = _ewald_reciprocal_forces(positions, charges, g, weight)
     radius = 4.0 / np.sqrt(alpha)
-    lmin = float(np.linalg.svd(lattice, compute_uv=False)[-1])
-    ra = np.sqrt(alpha)
-    for i, (left, qi) in enumerate(zip(positions, charges)):
-        d0 = left - positions
-        nb = int(np.ceil((radius + np.linalg.norm(d0, axis=1).max()) / lmin)) + 1
-        rng = np.arange(-nb, nb + 1)
-        images = np.stack(np.meshgrid(rng, rng, rng, indexing="ij"), -1).reshape(-1, 3) @ lattice
-        d = d0[:, None, :] + images[None, :, :]
-        dist = np.linalg.norm(d, axis=2)
+    ra = float(np.sqrt(alpha))
+    q = None
+    total_grad = None
+    for first, d in _real_space_blocks(lattice, positions, radius):
+        # d: (block atoms i, nat j, images, 3) separations i - j + image (torch)
+        if q is None:
+            q = torch.as_tensor(charges, dtype=torch.float64, device=d.device)
+            total_grad = torch.zeros((len(positions), 3), dtype=torch.float64, device=d.device)
+        dist = torch.linalg.vector_norm(d, dim=3)
         mask = (dist >= 1.0e-14) & (dist <= radius)
-        safe = np.where(mask, dist, 1.0)
-        radial = -erfc(ra * safe) / safe**2 - 2.0 * ra / np.sqrt(np.pi) * np.exp(-alpha * safe**2) / safe
-        grad = 0.25 * qi * charges[:, None, None] * (radial / safe)[:, :, None] * d
-        grad = np.where(mask[:, :, None], grad, 0.0).sum(axis=1)  # (nat, 3), one per right atom
-        forces[i] -= grad.sum(axis=0)
-        forces += grad
+        safe = torch.where(mask, dist, torch.ones_like(dist))
+        radial = (-torch.special.erfc(ra * safe) / safe**2
+                  - 2.0 * ra / np.sqrt(np.pi) * torch.exp(-alpha * safe**2) / safe)
+        qi = q[first:first + d.shape[0]]
+        grad = (0.25 * qi[:, None, None, None] * q[None, :, None, None]
+                * (radial / safe)[:, :, :, None] * d)
+        grad = torch.where(mask[:, :, :, None], grad, torch.zeros_like(grad)).sum(dim=2)
+        total_grad[first:first + d.shape[0]] -= grad.sum(dim=1)
+        total_grad += grad.sum(dim=0)
+    if total_grad is not None:
+        forces = forces + total_grad.cpu().numpy()
     return forces
 
 
@@ -142,8 +148,13 @@ def nonlocal_forces(system, states, tables, occupations, weights=None) -> np.nda
             if not atom_index or table.channels == 0:
                 continue
             species, coupling1 = table.projectors(vectors)
-            angle = vectors @ system.positions[atom_index].T
-            phases = to_device_f(np.cos(angle) - 1j * np.sin(angle), torch.complex128, device)
+            # structure phases exp(-i (k+G).tau) on the device
+            tau = torch.as_tensor(np.ascontiguousarray(system.positions[atom_index].T),
+                                  dtype=torch.float64, device=device)
+            angle = kg @ tau
+            phases = to_device_f(torch.polar(torch.ones_like(angle), -angle), torch.complex128,
+                                 device)
+            del angle
             species = to_device_f(species, torch.complex128, device)
             natoms, c = phases.shape[1], species.shape[1]
             beta = empty_f(len(basis), natoms * c, torch.complex128, device)

@@ -19,6 +19,7 @@ from __future__ import annotations
 import math
 
 import numpy as np
+import torch
 from scipy.special import erf, erfc
 
 DQ = 0.01
@@ -249,21 +250,41 @@ def ewald_energy(lattice: np.ndarray, positions: np.ndarray, charges: np.ndarray
     recip_sum -= float(np.sum(charges**2) * 2.0 * np.sqrt(alpha / np.pi))
     # real-space sum within 4/sqrt(alpha)
     radius = 4.0 / np.sqrt(alpha)
-    lmin = float(np.linalg.svd(lattice, compute_uv=False)[-1])
     real_sum = 0.0
-    sqa = np.sqrt(alpha)
-    for a, qa in zip(positions, charges):
-        d0 = a - positions  # (nat, 3)
-        reach = np.linalg.norm(d0, axis=1)
-        nb = int(np.ceil((radius + reach.max()) / lmin)) + 1
-        rng = np.arange(-nb, nb + 1)
-        images = np.stack(np.meshgrid(rng, rng, rng, indexing="ij"), -1).reshape(-1, 3) @ lattice
-        d = d0[:, None, :] + images[None, :, :]
-        dist = np.linalg.norm(d, axis=2)
+    sqa = float(np.sqrt(alpha))
+    q = None
+    for first, d in _real_space_blocks(lattice, positions, radius):
+        # d: (block atoms, nat, images, 3) separations a - b + image (torch)
+        if q is None:
+            q = torch.as_tensor(charges, dtype=torch.float64, device=d.device)
+        dist = torch.linalg.vector_norm(d, dim=3)
         mask = (dist >= 1.0e-14) & (dist <= radius)
-        contrib = np.where(mask, erfc(sqa * np.where(mask, dist, 1.0)) / np.where(mask, dist, 1.0), 0.0)
-        real_sum += qa * float(np.sum(charges * contrib.sum(axis=1)))
+        safe = torch.where(mask, dist, torch.ones_like(dist))
+        contrib = torch.where(mask, torch.special.erfc(sqa * safe) / safe, torch.zeros_like(dist))
+        block_q = q[first:first + d.shape[0]]
+        real_sum += float(torch.sum(block_q * (contrib.sum(dim=2) @ q)))
     return 0.5 * (recip_sum + 0.5 * real_sum)
+
+
+def _real_space_blocks(lattice: np.ndarray, positions: np.ndarray, radius: float, block: int = 16):
+    """(first atom, separations) for blocks of atoms a: the vectors
+    a - b + R (float64 torch tensors, on the GPU when there is one) over all
+    atoms b and the lattice translations R of one common image cube, large
+    enough that every pair within ``radius`` is in it for every a (images
+    beyond ``radius`` are masked by the callers)."""
+    device = torch.device("cuda", torch.cuda.current_device()) if torch.cuda.is_available() \
+        else torch.device("cpu")
+    lmin = float(np.linalg.svd(lattice, compute_uv=False)[-1])
+    reach = max(float(np.max(np.linalg.norm(a - positions, axis=1))) for a in positions)
+    nb = int(np.ceil((radius + reach) / lmin)) + 1
+    rng = np.arange(-nb, nb + 1)
+    images = torch.as_tensor(
+        np.stack(np.meshgrid(rng, rng, rng, indexing="ij"), -1).reshape(-1, 3) @ lattice,
+        dtype=torch.float64, device=device)
+    pos = torch.as_tensor(np.ascontiguousarray(positions), dtype=torch.float64, device=device)
+    for first in range(0, len(positions), block):
+        d0 = pos[first:first + block, None, :] - pos[None, :, :]
+        yield first, d0[:, :, None, :] + images[None, None, :, :]
 
 
 def pz81(rho: np.ndarray) -> tuple[np.ndarray, np.ndarray]:

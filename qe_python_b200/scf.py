@@ -381,8 +381,16 @@ def random_starting_subspace(ham: PlaneWaveHamiltonian, basis, rng: QERandom, nb
     Rayleigh-Ritz step in their span (qepy_pw/pw/scf.py:853-870, 923-953).
     Returns (vectors, eigenvalues, H vectors) in the Hamiltonian's dtype."""
     amp, phase = rng.pairs(len(basis), nbnd)
-    trials = amp * np.exp(2j * np.pi * phase) / (1.0 + 2.0 * basis.kinetic[:, None])
-    trials_dev = to_device_f(trials, ham.dtype, ham.device)
+    # the trial vectors are formed on the device (480 bands x 80 725 plane
+    # waves took a second as host complex exponentials)
+    device = ham.device
+    amp_d = torch.from_numpy(amp).to(device)
+    phase_d = torch.from_numpy(phase).to(device)
+    denominator = 1.0 + 2.0 * torch.from_numpy(np.asarray(basis.kinetic, dtype=float)).to(device)
+    trials = torch.polar(amp_d, (2.0 * np.pi) * phase_d) / denominator[:, None]
+    del amp_d, phase_d
+    trials_dev = to_device_f(trials, ham.dtype, device)
+    del trials
     applied = ham.apply(trials_dev)
     t128, a128 = _as128(trials_dev), _as128(applied)
     proj = K.gemm(K.OP_C, t128, a128)
