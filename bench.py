@@ -438,7 +438,7 @@ def run_b200(args) -> None:
     # public HostStreamedHpsi: 64-band chunks, copies overlapped with compute
     from qe_python_b200.diagonalization import HostStreamedHpsi
 
-    streamed = HostStreamedHpsi(forms["mixed"][1], nb, chunk=32, buffers=4)
+    streamed = HostStreamedHpsi(forms["mixed"][1], nb, chunk=64, buffers=4)
     host_in_storage, host_out_storage = streamed.host_buffers()
     host_in_storage[:, :npw] = torch.from_numpy(work.psi.T.astype(np.complex64))
     e2e_times = []

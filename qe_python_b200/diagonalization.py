@@ -35,10 +35,11 @@ from .device import (
 
 @dataclass(frozen=True)
 class FactorizedProjectorTerm:
-    """Species beta functions plus per-atom phase columns (diagonalization.py:21-28)."""
+    """Species beta functions plus per-atom phase columns (diagonalization.py:21-28);
+    ``phases`` may be a host array or a device tensor."""
 
     beta: np.ndarray
-    phases: np.ndarray
+    phases: "np.ndarray | torch.Tensor"
     coupling: np.ndarray
 
 

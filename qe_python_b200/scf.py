@@ -417,8 +417,17 @@ def projector_terms(system: System, tables: dict, basis) -> tuple:
         if not len(pos) or table.channels == 0:
             continue
         beta, coupling = table.projectors(vectors)
-        angle = vectors @ pos.T
-        phases = np.asfortranarray(np.cos(angle) - 1j * np.sin(angle))
+        if torch.cuda.is_available():
+            # exp(-i (k+G).tau) for every atom, formed on the device
+            device = torch.device("cuda", torch.cuda.current_device())
+            angle = torch.from_numpy(np.ascontiguousarray(vectors)).to(device) @ \
+                torch.from_numpy(np.ascontiguousarray(pos.T)).to(device)
+            phases = to_device_f(torch.polar(torch.ones_like(angle), -angle), torch.complex128,
+                                 device)
+            del angle
+        else:
+            angle = vectors @ pos.T
+            phases = np.asfortranarray(np.cos(angle) - 1j * np.sin(angle))
         terms.append(FactorizedProjectorTerm(beta, phases, coupling))
     return tuple(terms)
 
