@@ -67,10 +67,20 @@ struct GroupIds {
   }
 };
 
+// Line stride of the z passes.  Each line doubles as its own four-step
+// exchange buffer (its values are in registers by then), so it holds
+// F::scratch values; the stride is odd so that the transposed copies between
+// the lines and the stick buffer hit distinct banks.  Without a separate
+// exchange buffer a block needs about half the shared memory, and eight
+// blocks fit on an SM instead of six.
+template <class F>
+constexpr int line_stride() {
+  return (F::scratch > F::n ? F::scratch : F::n) | 1;
+}
+
 template <typename T, class F>
-constexpr size_t ac_smem(int nz_pad) {
-  return sizeof(C2<T>) * ((size_t)kSticksPerBlock * nz_pad + F::n +
-                          (size_t)kWarps * F::per_warp * F::scratch);
+constexpr size_t ac_smem() {
+  return sizeof(C2<T>) * ((size_t)kSticksPerBlock * line_stride<F>() + F::n);
 }
 
 template <typename T, class F>
@@ -83,15 +93,15 @@ size_t b_smem(const qeb_local_plan* p) {
 // ---------------------------------------------------------------------------
 template <typename T, class F>
 __device__ __forceinline__ void pass_a_body(
-    const C2<T>* __restrict__ psi, int64_t ld, int nst, int nz_pad,
+    const C2<T>* __restrict__ psi, int64_t ld, int nst,
     const int32_t* __restrict__ entry_g, const int32_t* __restrict__ entry_z,
     const int32_t* __restrict__ entry_stick, const int32_t* __restrict__ stick_off,
     const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks, int block_x, int64_t band) {
   constexpr int nz = F::n;
+  constexpr int nz_pad = line_stride<F>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2<T>* lines = reinterpret_cast<C2<T>*>(smem_raw);
   C2<T>* tw = lines + kSticksPerBlock * nz_pad;
-  C2<T>* xbuf = tw + nz;
   const int s0 = block_x * kSticksPerBlock;
   const int nsl = min(kSticksPerBlock, nst - s0);
   for (int i = threadIdx.x; i < nz; i += kThreads) tw[i] = tw_z[i];
@@ -104,7 +114,6 @@ __device__ __forceinline__ void pass_a_body(
   __syncthreads();
   const GroupIds<F> g;
   if (g.valid) {
-    C2<T>* x = xbuf + g.gid * F::scratch;
     for (int s = g.gid; s < nsl; s += g.ngroups) {
       C2<T>* line = lines + s * nz_pad;
       C2<T> v[F::R];
@@ -112,7 +121,8 @@ __device__ __forceinline__ void pass_a_body(
 #pragma unroll
         for (int i = 0; i < F::N1; ++i) v[i] = line[g.lig + F::N2 * i];
       }
-      qeb::four_inverse<T, F>(v, g.lig, x, tw, g.mask);
+      __syncwarp(g.mask);  // the line becomes the exchange buffer
+      qeb::four_inverse<T, F>(v, g.lig, line, tw, g.mask);
       if (g.lig < F::N1) {
 #pragma unroll
         for (int p = 0; p < F::N2; ++p) line[g.lig + F::N1 * p] = v[p];
@@ -130,16 +140,16 @@ __device__ __forceinline__ void pass_a_body(
 
 template <typename T, class F>
 __device__ __forceinline__ void pass_c_body(
-    const C2<T>* __restrict__ sticks, int nst, int nz_pad, const int32_t* __restrict__ entry_g,
+    const C2<T>* __restrict__ sticks, int nst, const int32_t* __restrict__ entry_g,
     const int32_t* __restrict__ entry_z, const int32_t* __restrict__ entry_stick,
     const int32_t* __restrict__ stick_off, const C2<T>* __restrict__ tw_z,
     const C2<T>* __restrict__ psi, int64_t ld, const T* __restrict__ kinetic, T inv_n,
     C2<T>* __restrict__ out, int64_t ldo, int block_x, int64_t band) {
   constexpr int nz = F::n;
+  constexpr int nz_pad = line_stride<F>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2<T>* lines = reinterpret_cast<C2<T>*>(smem_raw);
   C2<T>* tw = lines + kSticksPerBlock * nz_pad;
-  C2<T>* xbuf = tw + nz;
   const int s0 = block_x * kSticksPerBlock;
   const int nsl = min(kSticksPerBlock, nst - s0);
   for (int i = threadIdx.x; i < nz; i += kThreads) tw[i] = tw_z[i];
@@ -151,7 +161,6 @@ __device__ __forceinline__ void pass_c_body(
   __syncthreads();
   const GroupIds<F> g;
   if (g.valid) {
-    C2<T>* x = xbuf + g.gid * F::scratch;
     for (int s = g.gid; s < nsl; s += g.ngroups) {
       C2<T>* line = lines + s * nz_pad;
       C2<T> v[F::R];
@@ -159,7 +168,8 @@ __device__ __forceinline__ void pass_c_body(
 #pragma unroll
         for (int p = 0; p < F::N2; ++p) v[p] = line[g.lig + F::N1 * p];
       }
-      qeb::four_forward<T, F>(v, g.lig, x, tw, g.mask);
+      __syncwarp(g.mask);  // the line becomes the exchange buffer
+      qeb::four_forward<T, F>(v, g.lig, line, tw, g.mask);
       if (g.lig < F::N2) {
 #pragma unroll
         for (int i = 0; i < F::N1; ++i) line[g.lig + F::N2 * i] = v[i];
@@ -299,22 +309,22 @@ __device__ __forceinline__ void pass_b_body(
 
 template <typename T, class F>
 __global__ void __launch_bounds__(kThreads) four_pass_a(
-    const C2<T>* __restrict__ psi, int64_t ld, int nst, int nz_pad,
+    const C2<T>* __restrict__ psi, int64_t ld, int nst,
     const int32_t* __restrict__ entry_g, const int32_t* __restrict__ entry_z,
     const int32_t* __restrict__ entry_stick, const int32_t* __restrict__ stick_off,
     const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks) {
-  pass_a_body<T, F>(psi, ld, nst, nz_pad, entry_g, entry_z, entry_stick, stick_off, tw_z, sticks,
+  pass_a_body<T, F>(psi, ld, nst, entry_g, entry_z, entry_stick, stick_off, tw_z, sticks,
                     blockIdx.x, blockIdx.y);
 }
 
 template <typename T, class F>
 __global__ void __launch_bounds__(kThreads) four_pass_c(
-    const C2<T>* __restrict__ sticks, int nst, int nz_pad, const int32_t* __restrict__ entry_g,
+    const C2<T>* __restrict__ sticks, int nst, const int32_t* __restrict__ entry_g,
     const int32_t* __restrict__ entry_z, const int32_t* __restrict__ entry_stick,
     const int32_t* __restrict__ stick_off, const C2<T>* __restrict__ tw_z,
     const C2<T>* __restrict__ psi, int64_t ld, const T* __restrict__ kinetic, T inv_n,
     C2<T>* __restrict__ out, int64_t ldo) {
-  pass_c_body<T, F>(sticks, nst, nz_pad, entry_g, entry_z, entry_stick, stick_off, tw_z, psi, ld,
+  pass_c_body<T, F>(sticks, nst, entry_g, entry_z, entry_stick, stick_off, tw_z, psi, ld,
                     kinetic, inv_n, out, ldo, blockIdx.x, blockIdx.y);
 }
 
@@ -351,10 +361,10 @@ struct KBatch {
 
 template <typename T, class F>
 __global__ void __launch_bounds__(kThreads) four_pass_a_multi(const __grid_constant__ KBatch<T> kb,
-                                                              int nz_pad, const C2<T>* tw_z) {
+                                                              const C2<T>* tw_z) {
   const KDesc<T>& d = kb.k[blockIdx.z];
   if ((int)blockIdx.x * kSticksPerBlock >= d.nst || (int)blockIdx.y >= d.nb) return;
-  pass_a_body<T, F>(d.psi, d.ld, d.nst, nz_pad, d.entry_g, d.entry_z, d.entry_stick, d.stick_off,
+  pass_a_body<T, F>(d.psi, d.ld, d.nst, d.entry_g, d.entry_z, d.entry_stick, d.stick_off,
                     tw_z, d.sticks, blockIdx.x, blockIdx.y);
 }
 
@@ -371,11 +381,10 @@ __global__ void __launch_bounds__(kThreads) four_pass_b_multi(const __grid_const
 
 template <typename T, class F>
 __global__ void __launch_bounds__(kThreads) four_pass_c_multi(const __grid_constant__ KBatch<T> kb,
-                                                              int nz_pad, const C2<T>* tw_z,
-                                                              T inv_n) {
+                                                              const C2<T>* tw_z, T inv_n) {
   const KDesc<T>& d = kb.k[blockIdx.z];
   if ((int)blockIdx.x * kSticksPerBlock >= d.nst || (int)blockIdx.y >= d.nb) return;
-  pass_c_body<T, F>(d.sticks, d.nst, nz_pad, d.entry_g, d.entry_z, d.entry_stick, d.stick_off,
+  pass_c_body<T, F>(d.sticks, d.nst, d.entry_g, d.entry_z, d.entry_stick, d.stick_off,
                     tw_z, d.psi, d.ld, d.kinetic, inv_n, d.out, d.ldo, blockIdx.x, blockIdx.y);
 }
 
@@ -405,7 +414,7 @@ struct SetLimits {
   int operator()() const {
     cudaError_t err = cudaSuccess;
     if (p->fast_z >= 0 && F::n == p->nz) {
-      const int s = (int)ac_smem<T, F>(p->nz_pad);
+      const int s = (int)ac_smem<T, F>();
       err = qeb::raise_smem_limit(four_pass_a<T, F>, s);
       if (err == cudaSuccess)
         err = qeb::raise_smem_limit(four_pass_c<T, F>, s);
@@ -436,8 +445,8 @@ struct PassA {
   template <class F>
   int operator()() const {
     const dim3 grid((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
-    four_pass_a<T, F><<<grid, kThreads, ac_smem<T, F>(p->nz_pad), s>>>(
-        psi, ld, p->nst, p->nz_pad, p->entry_g, p->entry_z, p->entry_stick, p->stick_off,
+    four_pass_a<T, F><<<grid, kThreads, ac_smem<T, F>(), s>>>(
+        psi, ld, p->nst, p->entry_g, p->entry_z, p->entry_stick, p->stick_off,
         tw_at<T>(p, 2), sticks);
     return QEB_OK;
   }
@@ -451,8 +460,8 @@ struct PassC {
   int operator()() const {
     const dim3 grid((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
     const T inv_n = T(1.0 / ((double)p->nx * p->ny * p->nz));
-    four_pass_c<T, F><<<grid, kThreads, ac_smem<T, F>(p->nz_pad), s>>>(
-        sticks, p->nst, p->nz_pad, p->entry_g, p->entry_z, p->entry_stick, p->stick_off,
+    four_pass_c<T, F><<<grid, kThreads, ac_smem<T, F>(), s>>>(
+        sticks, p->nst, p->entry_g, p->entry_z, p->entry_stick, p->stick_off,
         tw_at<T>(p, 2), psi, ld, kinetic, inv_n, out, ldo);
     return QEB_OK;
   }
@@ -478,7 +487,7 @@ struct PassAMulti {
   template <class F>
   int operator()() const {
     const dim3 grid(sblocks, (unsigned)nb, (unsigned)nk);
-    four_pass_a_multi<T, F><<<grid, kThreads, ac_smem<T, F>(p0->nz_pad), s>>>(*kb, p0->nz_pad,
+    four_pass_a_multi<T, F><<<grid, kThreads, ac_smem<T, F>(), s>>>(*kb,
                                                                              tw_at<T>(p0, 2));
     return QEB_OK;
   }
@@ -504,8 +513,8 @@ struct PassCMulti {
   int operator()() const {
     const dim3 grid(sblocks, (unsigned)nb, (unsigned)nk);
     const T inv_n = T(1.0 / ((double)p0->nx * p0->ny * p0->nz));
-    four_pass_c_multi<T, F><<<grid, kThreads, ac_smem<T, F>(p0->nz_pad), s>>>(
-        *kb, p0->nz_pad, tw_at<T>(p0, 2), inv_n);
+    four_pass_c_multi<T, F><<<grid, kThreads, ac_smem<T, F>(), s>>>(
+        *kb, tw_at<T>(p0, 2), inv_n);
     return QEB_OK;
   }
 };
