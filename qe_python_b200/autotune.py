@@ -59,7 +59,7 @@ class Autotuner:
                 torch.cuda.is_current_stream_capturing():
             return candidates[0]
         with self._lock:
-            stream = torch.cuda.current_stream()
+            stream = torch.cuda.current_stream(torch.cuda.current_device())
             for c in candidates:  # warm-up: first-use allocations, caches
                 run(c)
             samples = {c: [] for c in candidates}

@@ -58,6 +58,7 @@ def _check_matrix(name: str, t: torch.Tensor) -> None:
 TENSOR_MIN_MACS = 1 << 21
 
 
+TUNE_MIN_FLOP = 2.0e9  # split-TF32 products below this are not worth timing (~20 us)
 SKINNY_MAX = 16  # narrow output side at or below which qeb_zgemm/qeb_cgemm stream the wide operand
 
 
@@ -246,7 +247,8 @@ def cgemm_tf32x3(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | 
     (qeb_cgemm_tf32x3_ex).  Returns None, touching nothing, when a or b lacks
     16-byte aligned columns (odd leading dimension); callers then use the
     packed path.  ``splits``: CTAs per output tile along K; None lets the
-    autotuner pick among the built-in choice, half and twice it."""
+    autotuner pick among the built-in choice, half, twice and four times it
+    (each K slice at least four 32-wide K tiles deep)."""
     _check_matrix("a", a)
     _check_matrix("b", b)
     if a.dtype != torch.complex64 or b.dtype != torch.complex64:
@@ -282,9 +284,14 @@ def cgemm_tf32x3(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | 
         if default == 1 and not 148 < tiles < 296:
             # enough output tiles for full waves: the K split stays off
             candidates = [1]
+        elif 8 * m * n * k < TUNE_MIN_FLOP:
+            # a few microseconds of work: timing candidates costs more than
+            # a better split could save
+            candidates = [default]
         else:
             candidates = sorted({default, max(1, default // 2),
-                                 min(2 * default, max(1, kblocks // 4))})
+                                 min(2 * default, max(1, kblocks // 4)),
+                                 min(4 * default, max(1, kblocks // 4))})
             candidates.remove(default)
             candidates.insert(0, default)
         key = f"cgemm_tf32x3/{op_a}/{bucket(m)}/{bucket(n)}/{bucket(k)}"
