@@ -157,10 +157,16 @@ __device__ __forceinline__ bool drain_accumulator(float (&acc)[BN], uint64_t* ac
   return true;
 }
 
-template <int OP>
+template <int OP, bool TAIL = false>
 __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
     const __grid_constant__ Maps maps, int M, int N, int kb_per_split, int kb_total, float2 alpha,
-    float2 beta, float2* C, int64_t ldc, float2* split, int* error) {
+    float2 beta, float2* C, int64_t ldc, float2* split, int* error, int skip_m, int skip_n,
+    int m_off, int n_off, int tail_tiles) {
+  // TAIL == false: grid (M tiles, N tiles, K slices); the tiles of column
+  // skip_n from row skip_m on belong to a tail launch and return at once.
+  // TAIL: grid (tail tiles, 1, K slices) over rows m_off + x of column
+  // n_off; the K slices go to compact BM x BN partial tiles.
+  if (!TAIL && (int)blockIdx.y == skip_n && (int)blockIdx.x >= skip_m) return;
   using S = Slots<OP>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(
@@ -176,7 +182,8 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
   volatile int* abort_v = abort_flag;
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-  const int m0 = blockIdx.x * BM, n0 = blockIdx.y * BN;
+  const int m0 = ((int)blockIdx.x + (TAIL ? m_off : 0)) * BM;
+  const int n0 = ((int)blockIdx.y + (TAIL ? n_off : 0)) * BN;
   const int kb0 = blockIdx.z * kb_per_split;
   const int nk = max(0, min(kb_total, kb0 + kb_per_split) - kb0);
 
@@ -307,12 +314,17 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
     if (!aborted && row < M) {
       const int cbase = n0 + half * (BN / 2);
       if (split != nullptr) {
+        // partial slice of this K range: full M x N slices, or compact
+        // BM x BN tiles for a tail launch
+        const int64_t cstride = TAIL ? BM : M;
+        float2* sbase = TAIL
+            ? split + ((int64_t)blockIdx.z * tail_tiles + blockIdx.x) * (BM * BN) + (row - m0) -
+                  (int64_t)n0 * BM
+            : split + (int64_t)blockIdx.z * M * N + row;
 #pragma unroll
         for (int j = 0; j < BN / 2; ++j) {
           const int col = cbase + j;
-          if (col < N)
-            split[(int64_t)blockIdx.z * M * N + row + (int64_t)col * M] =
-                make_float2(acc[j], acc[BN / 2 + j]);
+          if (col < N) sbase[(int64_t)col * cstride] = make_float2(acc[j], acc[BN / 2 + j]);
         }
       } else {
         const bool use_beta = beta.x != 0.0f || beta.y != 0.0f;
@@ -374,6 +386,38 @@ __global__ void reduce_slices(int M, int N, int splits, const float2* __restrict
   }
 }
 
+// C = alpha * sum_s P[s] + beta * C over the ntiles tail tiles (rows m_off ..
+// m_off + ntiles - 1 of tile column n_off): compact partial tiles
+// P[(s * ntiles + t) * BM * BN + r + c * BM], slices summed in ascending order.
+__global__ void reduce_tail(int M, int N, int splits, int m_off, int n_off, int ntiles,
+                            const float2* __restrict__ P, float2 alpha, float2 beta, float2* C,
+                            int64_t ldc) {
+  const int64_t per_tile = (int64_t)BM * BN;
+  const int64_t total = (int64_t)ntiles * per_tile;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < total;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int lt = (int)(i / per_tile);
+    const int64_t e = i - lt * per_tile;
+    const int m = (m_off + lt) * BM + (int)(e % BM);
+    const int n = n_off * BN + (int)(e / BM);
+    if (m >= M || n >= N) continue;
+    float2 s = make_float2(0.0f, 0.0f);
+    for (int k = 0; k < splits; ++k) {
+      const float2 p = P[((int64_t)k * ntiles + lt) * per_tile + e];
+      s.x += p.x;
+      s.y += p.y;
+    }
+    float2* c = C + m + (int64_t)n * ldc;
+    float2 v = make_float2(alpha.x * s.x - alpha.y * s.y, alpha.x * s.y + alpha.y * s.x);
+    if (beta.x != 0.0f || beta.y != 0.0f) {
+      const float2 o = *c;
+      v.x += beta.x * o.x - beta.y * o.y;
+      v.y += beta.x * o.y + beta.y * o.x;
+    }
+    *c = v;
+  }
+}
+
 int encode_map(qeb::EncodeTiled enc, CUtensorMap* map, const void* ptr, uint64_t inner,
                uint64_t outer, int64_t ld_bytes, uint32_t box_inner, uint32_t box_outer,
                bool swizzle) {
@@ -417,14 +461,58 @@ int choose_splits(int M, int N, int K) {
   return s < 1 ? 1 : s;
 }
 
+// Split of a partial last wave: an unsplit product of several waves whose
+// last wave holds rem <= sm/2 output tiles runs its full waves as usual and
+// the rem tail tiles with their K range split over about one wave of CTAs
+// (reduced afterwards), instead of leaving most SMs idle for a whole wave.
+// Returns the tail's slice count (0: no tail split) and its scratch bytes.
+int tail_splits(int M, int N, int K, int64_t* bytes) {
+  const int mt = (M + BM - 1) / BM;
+  const int tiles = mt * ((N + BN - 1) / BN);
+  const int sm = sm_count();
+  const int kblocks = (2 * K + BKF - 1) / BKF;
+  *bytes = 0;
+  if (tiles <= sm) return 0;
+  const int rem = tiles % sm;
+  if (rem == 0 || rem > sm / 2 || rem > mt) return 0;  // the tail: part of the last tile column
+  int ts = sm / rem;
+  if (ts > kblocks / 4) ts = kblocks / 4;
+  if (ts > 64) ts = 64;
+  if (ts < 2) return 0;
+  *bytes = (int64_t)ts * rem * BM * BN * (int64_t)sizeof(float2);
+  return ts;
+}
+
 template <int OP>
 int launch(const Maps& maps, int M, int N, int K, float2 al, float2 be, float2* C, int64_t ldc,
            void* scratch, int64_t scratch_bytes, int requested_splits, int* err, cudaStream_t s) {
   cudaError_t e = qeb::raise_smem_limit(cgemm_tf32x3_kernel<OP>, smem_bytes<OP>());
+  if (e == cudaSuccess) e = qeb::raise_smem_limit(cgemm_tf32x3_kernel<OP, true>, smem_bytes<OP>());
   if (e != cudaSuccess) return qeb::cuda_status(e, "cgemm_tf32x3 shared-memory limit");
   const int kblocks = (2 * K + BKF - 1) / BKF;
   int splits = requested_splits > 0 ? (requested_splits < kblocks ? requested_splits : kblocks)
                                     : choose_splits(M, N, K);
+  if (splits == 1) {
+    int64_t tail_bytes = 0;
+    int ts = tail_splits(M, N, K, &tail_bytes);
+    if (ts > 1 && scratch != nullptr && scratch_bytes >= tail_bytes) {
+      const int mt = (M + BM - 1) / BM, nt = (N + BN - 1) / BN;
+      const int rem = (mt * nt) % sm_count();
+      float2* part = static_cast<float2*>(scratch);
+      // every tile but the tail (the last rem rows of the last tile column), unsplit
+      cgemm_tf32x3_kernel<OP><<<dim3(mt, nt, 1), THREADS, smem_bytes<OP>(), s>>>(
+          maps, M, N, kblocks, kblocks, al, be, C, ldc, nullptr, err, mt - rem, nt - 1, 0, 0, 0);
+      const int per_t = (kblocks + ts - 1) / ts;
+      ts = (kblocks + per_t - 1) / per_t;
+      cgemm_tf32x3_kernel<OP, true><<<dim3(rem, 1, ts), THREADS, smem_bytes<OP>(), s>>>(
+          maps, M, N, per_t, kblocks, al, be, C, ldc, part, err, 0, -1, mt - rem, nt - 1, rem);
+      int blocks = (int)(((int64_t)rem * BM * BN + 255) / 256);
+      if (blocks > 4 * sm_count()) blocks = 4 * sm_count();
+      reduce_tail<<<blocks, 256, 0, s>>>(M, N, ts, mt - rem, nt - 1, rem, part, al, be, C, ldc);
+      qeb::count_launches(3);
+      return qeb::cuda_status(cudaGetLastError(), "cgemm_tf32x3 launch");
+    }
+  }
   const int64_t slice = (int64_t)M * N * 8;
   if (splits > 1 && (scratch == nullptr || scratch_bytes < splits * slice)) {
     const int64_t fit = scratch == nullptr ? 0 : scratch_bytes / slice;
@@ -435,7 +523,8 @@ int launch(const Maps& maps, int M, int N, int K, float2 al, float2 be, float2* 
   float2* part = splits > 1 ? static_cast<float2*>(scratch) : nullptr;
   const dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, splits);
   cgemm_tf32x3_kernel<OP><<<grid, THREADS, smem_bytes<OP>(), s>>>(maps, M, N, per, kblocks, al,
-                                                                  be, C, ldc, part, err);
+                                                                  be, C, ldc, part, err, 0, -1,
+                                                                  0, 0, 0);
   qeb::count_launches(1);
   if (splits > 1) {
     int blocks = (int)(((int64_t)M * N + 255) / 256);
@@ -458,7 +547,10 @@ extern "C" int64_t qeb_cgemm_tf32x3_scratch_bytes(int op_a, int M, int N, int K)
   (void)op_a;
   if (M <= 0 || N <= 0 || K <= 0) return 0;
   const int s = choose_splits(M, N, K);
-  return s > 1 ? (int64_t)s * M * N * 8 : 0;
+  if (s > 1) return (int64_t)s * M * N * 8;
+  int64_t tail_bytes = 0;
+  tail_splits(M, N, K, &tail_bytes);
+  return tail_bytes;
 }
 
 extern "C" int qeb_cgemm_tf32x3(int op_a, int M, int N, int K, const double* alpha, const void* A,

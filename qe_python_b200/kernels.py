@@ -313,7 +313,9 @@ def _cgemm_tf32x3_launch(lib, op_a, m, n, k, alpha, a, lda, b, ldb, beta, c, spl
     if splits and splits > 1:
         need = int(splits) * m * n * 8
     else:
-        need = 0 if splits == 1 else int(lib.qeb_cgemm_tf32x3_scratch_bytes(op_a, m, n, k))
+        # the default split, or for an unsplit product the K split of its
+        # partial last wave of output tiles
+        need = int(lib.qeb_cgemm_tf32x3_scratch_bytes(op_a, m, n, k))
     scratch = _SCRATCH.get(need, c.device) if need > 0 else None
     _lib.check("qeb_cgemm_tf32x3_ex", lib.qeb_cgemm_tf32x3_ex(
         op_a, m, n, k, al, a.data_ptr(), lda, b.data_ptr(), ldb, be, c.data_ptr(),

@@ -88,3 +88,26 @@ def test_gemm_routes_large_complex64_to_tensor_cores(cuda_device):
     simt = K.gemm(K.OP_C, _dev(a), _dev(b), tensor=False).cpu().numpy()
     assert np.max(np.abs(simt - exp)) <= _tol(3000, exp)
     assert torch.cuda.is_available()
+
+
+@pytest.mark.parametrize("op,m,n,k", [
+    (K.OP_N, 11019, 256, 512),   # 174 output tiles: one wave + a 26-tile tail
+    (K.OP_C, 20000, 130, 300),   # 314 tiles: two waves + an 18-tile tail
+    (K.OP_N, 19100, 260, 96),    # 450 tiles: three waves + a 6-tile tail, short K
+])
+def test_unsplit_product_with_tail_wave(cuda_device, op, m, n, k):
+    """An unsplit product (splits=1) whose last wave of output tiles is at most
+    half full runs that tail with its K range split and reduced apart from
+    the full waves; the result must be the same product."""
+    rng = np.random.default_rng(m + n + k)
+    shape_a = (k, m) if op == K.OP_C else (m, k)
+    a = rng.standard_normal(shape_a) + 1j * rng.standard_normal(shape_a)
+    b = rng.standard_normal((k, n)) + 1j * rng.standard_normal((k, n))
+    c0 = rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
+    alpha, beta = 0.75 + 0.5j, -0.5 + 1.0j
+    exp = _ref(op, a, b, c0, alpha, beta)
+    for _ in range(2):
+        got = K.cgemm_tf32x3(op, _dev(a), _dev(b), _dev(c0), alpha, beta, splits=1)
+        assert got is not None
+        assert np.max(np.abs(got.cpu().numpy() - exp)) <= _tol(k, exp)
+    assert K.tf32_error() == 0
