@@ -459,6 +459,22 @@ def run_b200(args) -> None:
         if i >= args.warmup:
             e2e_times.append(a.elapsed_time(b))
     e2e_ms = max_over_ranks(statistics.mean(e2e_times), world, device)
+    # the bare copies of one step's bytes, to tell the link's share of e2e
+    copy_dev = torch.empty_like(host_in_storage, device=device)
+    copy_ms = {}
+    for name, copy in (("h2d", lambda: copy_dev.copy_(host_in_storage, non_blocking=True)),
+                       ("d2h", lambda: host_out_storage.copy_(copy_dev, non_blocking=True))):
+        samples = []
+        for _ in range(5):
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            copy()
+            b.record(stream)
+            torch.cuda.synchronize()
+            samples.append(a.elapsed_time(b))
+        copy_ms[name] = statistics.median(samples)
+    del copy_dev
 
     # roofline of the dominant kernel in the headline (mixed) form
     names = ["pass_a", "pass_b", "pass_c", "calbec_gemm", "coupling_gemm", "add_gemm"]
@@ -548,7 +564,13 @@ def run_b200(args) -> None:
         "gpu_launches": int(launches),
         "e2e": {"value": world * nb / (e2e_ms / 1e3), "unit": "bands/s",
                 "h2d_bytes_per_step": host_in_storage.numel() * 8,
-                "d2h_bytes_per_step": host_out_storage.numel() * 8},
+                "d2h_bytes_per_step": host_out_storage.numel() * 8,
+                "ms_per_step": e2e_ms,
+                "bare_copy_ms": {k: round(v, 4) for k, v in copy_ms.items()},
+                "link_gbs": {k: round(host_in_storage.numel() * 8 / (v / 1e3) / 1e9, 1)
+                             for k, v in copy_ms.items()},
+                "note": "64-band chunks: input copy, graph replay and output copy on three "
+                        "streams; bounded by the host link, whose speed varies between boxes"},
         "clocks": graph_clocks.summary(),
         "clocks_staged": clocks.summary(),
     }
