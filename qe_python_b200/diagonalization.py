@@ -20,7 +20,7 @@ import numpy as np
 import torch
 
 from . import kernels as K
-from .basis import LocalPotentialWorkspace, PlaneWaveBasis, apply_local_multi
+from .basis import FFTScratchPool, LocalPotentialWorkspace, PlaneWaveBasis, apply_local_multi
 from .device import (
     COMPLEX_OF,
     REAL_OF,
@@ -333,7 +333,11 @@ class HpsiGraph:
     launch overhead.
     """
 
-    def __init__(self, ham: PlaneWaveHamiltonian, nbands: int) -> None:
+    def __init__(self, ham: PlaneWaveHamiltonian, nbands: int, private: bool = False) -> None:
+        """``private``: the graph gets its own stick scratch, side stream and
+        split-K scratch, so that it can replay concurrently with the other
+        private graphs of the same Hamiltonian (by default the graphs of one
+        Hamiltonian share them and must replay one after another)."""
         npw = len(ham.basis)
         self.ham = ham
         self.nbands = int(nbands)
@@ -346,17 +350,33 @@ class HpsiGraph:
         self.output_storage = self.output.T.as_strided(
             (self.nbands, leading_dimension(self.output)), (leading_dimension(self.output), 1))
         stream = torch.cuda.Stream(device=ham.device)
-        stream.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(stream):
-            # warm-up outside the capture: workspaces, attributes, scratch
-            for _ in range(2):
+        workspace = ham.local_workspace
+        shared_pool, shared_side = workspace.scratch_pool, getattr(ham, "_stream_side", None)
+        if private:
+            workspace.scratch_pool = FFTScratchPool()
+            ham._stream_side = torch.cuda.Stream(device=ham.device)
+        try:
+            stream.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(stream):
+                # warm-up outside the capture: workspaces, attributes, scratch
+                for _ in range(2):
+                    ham.apply_into(self.input, self.output)
+            torch.cuda.current_stream().wait_stream(stream)
+            torch.cuda.synchronize()
+            self.graph = torch.cuda.CUDAGraph()
+            # a private graph captures on its warm-up stream, whose split-K
+            # scratch is its own
+            with torch.cuda.graph(self.graph, stream=stream if private else None):
                 ham.apply_into(self.input, self.output)
-        torch.cuda.current_stream().wait_stream(stream)
-        torch.cuda.synchronize()
-        self.graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.graph):
-            ham.apply_into(self.input, self.output)
-        torch.cuda.synchronize()
+            torch.cuda.synchronize()
+        finally:
+            # the private scratch and side stream stay alive with the graph
+            self._scratch_pool, self._side = workspace.scratch_pool, ham._stream_side
+            workspace.scratch_pool = shared_pool
+            if shared_side is None:
+                del ham._stream_side
+            else:
+                ham._stream_side = shared_side
 
     def replay(self) -> torch.Tensor:
         self.graph.replay()
@@ -377,23 +397,28 @@ class HostStreamedHpsi:
     """H|psi> of host-resident band blocks with the PCIe copies overlapped.
 
     The bands are cut into chunks; chunk c is copied in on one stream, its
-    H|psi> replayed from a captured graph on the compute stream, and its
-    result copied out on a third stream, so chunk c's compute overlaps chunk
-    c+1's input and chunk c-1's output copies (H|psi> is independent per
-    band).  Host buffers are pinned, with the (nbands, ld) storage layout of
+    H|psi> replayed from a captured graph on one of the compute streams
+    (alternating, so chunk c's projector GEMMs can overlap chunk c+1's FFT
+    passes), and its result copied out on another stream, so chunk c's
+    compute overlaps chunk c+1's input and chunk c-1's output copies (H|psi>
+    is independent per band; each graph has its own scratch).  Host buffers are pinned, with the (nbands, ld) storage layout of
     the device buffers so that each copy is one contiguous DMA.
     """
 
     def __init__(self, ham: PlaneWaveHamiltonian, nbands: int, chunk: int = 64,
-                 buffers: int = 2) -> None:
+                 buffers: int = 2, compute_streams: int = 2) -> None:
         self.ham = ham
         self.nbands = int(nbands)
         self.chunk = max(1, min(int(chunk), self.nbands))
-        self.graphs = [HpsiGraph(ham, self.chunk) for _ in range(max(1, int(buffers)))]
+        # private graphs: consecutive chunks replay on alternating compute
+        # streams, so one chunk's projector GEMMs overlap the next one's FFTs
+        self.graphs = [HpsiGraph(ham, self.chunk, private=True)
+                       for _ in range(max(1, int(buffers)))]
         self.ld = self.graphs[0].input_storage.shape[1]
         self.copy_in = torch.cuda.Stream(device=ham.device)
         self.copy_out = torch.cuda.Stream(device=ham.device)
-        self.compute = torch.cuda.Stream(device=ham.device)
+        self.computes = [torch.cuda.Stream(device=ham.device)
+                         for _ in range(max(1, int(compute_streams)))]
 
     def host_buffers(self) -> tuple[torch.Tensor, torch.Tensor]:
         """Pinned (nbands, ld) input and output storage; band b's plane-wave
@@ -410,7 +435,7 @@ class HostStreamedHpsi:
         n = len(self.graphs)
         ready_in, done_compute, done_out = [], [], []
         current = torch.cuda.current_stream(self.ham.device)
-        for stream in (self.copy_in, self.copy_out, self.compute):
+        for stream in (self.copy_in, self.copy_out, *self.computes):
             stream.wait_stream(current)
         for index, start in enumerate(range(0, self.nbands, self.chunk)):
             stop = min(self.nbands, start + self.chunk)
@@ -423,11 +448,12 @@ class HostStreamedHpsi:
                     graph.input_storage[stop - start:].zero_()
                 ready_in.append(torch.cuda.Event())
                 ready_in[-1].record(self.copy_in)
-            with torch.cuda.stream(self.compute):
-                self.compute.wait_event(ready_in[-1])
+            compute = self.computes[index % len(self.computes)]
+            with torch.cuda.stream(compute):
+                compute.wait_event(ready_in[-1])
                 graph.replay()
                 done_compute.append(torch.cuda.Event())
-                done_compute[-1].record(self.compute)
+                done_compute[-1].record(compute)
             with torch.cuda.stream(self.copy_out):
                 self.copy_out.wait_event(done_compute[-1])
                 host_out[start:stop].copy_(graph.output_storage[:stop - start], non_blocking=True)

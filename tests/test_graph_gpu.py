@@ -52,16 +52,21 @@ def test_host_streamed_hpsi_equals_direct_apply(cuda_device):
     ham = PlaneWaveHamiltonian(basis, None, ((work.beta, work.coupling),), local_workspace=ws,
                                real_potential=torch.from_numpy(work.potential).cuda(),
                                potential_average=0.0)
-    streamed = HostStreamedHpsi(ham, 40, chunk=16)
-    host_in, host_out = streamed.host_buffers()
     npw = len(basis)
-    host_in[:, :npw] = torch.from_numpy(work.psi.T.astype(np.complex64))
-    streamed(host_in, host_out)
-    torch.cuda.synchronize()
-    for start in range(0, 40, 16):
-        stop = min(40, start + 16)
-        block = to_device_f(work.psi[:, start:stop], torch.complex64)
-        expected = ham.apply(block).cpu().T
-        got = host_out[start:stop, :npw]
-        scale = float(expected.abs().max())
-        assert float((got - expected).abs().max()) <= 1e-5 * scale
+    # graphs replay concurrently on two compute streams, each with its own
+    # scratch: every chunk must still match the direct application
+    for chunk, buffers in ((16, 2), (8, 4)):
+        streamed = HostStreamedHpsi(ham, 40, chunk=chunk, buffers=buffers)
+        host_in, host_out = streamed.host_buffers()
+        host_in[:, :npw] = torch.from_numpy(work.psi.T.astype(np.complex64))
+        for _ in range(2):
+            host_out.zero_()
+            streamed(host_in, host_out)
+            torch.cuda.synchronize()
+            for start in range(0, 40, chunk):
+                stop = min(40, start + chunk)
+                block = to_device_f(work.psi[:, start:stop], torch.complex64)
+                expected = ham.apply(block).cpu().T
+                got = host_out[start:stop, :npw]
+                scale = float(expected.abs().max())
+                assert float((got - expected).abs().max()) <= 1e-5 * scale
