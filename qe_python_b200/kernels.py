@@ -8,6 +8,7 @@ the current torch stream.  Matrices are column-major torch CUDA tensors
 from __future__ import annotations
 
 import ctypes
+import os
 
 import numpy as np
 import torch
@@ -59,6 +60,10 @@ TENSOR_MIN_MACS = 1 << 21
 
 
 TUNE_MIN_FLOP = 2.0e9  # split-TF32 products below this are not worth timing (~20 us)
+# Timing the K split on first use (QEB_TUNE_SPLITS=1).  Off by default: on every
+# shape of the benchmark cells the library's two-wave default was the tuned
+# choice (within 5 %), and the first-use timing cost about a second per SCF.
+TUNE_SPLITS = os.environ.get("QEB_TUNE_SPLITS") == "1"
 SKINNY_MAX = 16  # narrow output side at or below which qeb_zgemm/qeb_cgemm stream the wide operand
 
 
@@ -246,9 +251,10 @@ def cgemm_tf32x3(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | 
     """Split-TF32 c = alpha op(a) b + beta c reading complex64 a and b directly
     (qeb_cgemm_tf32x3_ex).  Returns None, touching nothing, when a or b lacks
     16-byte aligned columns (odd leading dimension); callers then use the
-    packed path.  ``splits``: CTAs per output tile along K; None lets the
-    autotuner pick among the built-in choice, half, twice and four times it
-    (each K slice at least four 32-wide K tiles deep)."""
+    packed path.  ``splits``: CTAs per output tile along K; None takes the
+    library's choice or, with QEB_TUNE_SPLITS=1, lets the autotuner pick among
+    it, half, twice and four times it (each K slice at least four 32-wide K
+    tiles deep)."""
     _check_matrix("a", a)
     _check_matrix("b", b)
     if a.dtype != torch.complex64 or b.dtype != torch.complex64:
@@ -277,6 +283,8 @@ def cgemm_tf32x3(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | 
     if k == 0:  # empty contraction: c = beta c
         return c.zero_() if complex(beta) == 0 else c.mul_(beta)
     lib = _lib.load()
+    if splits is None and not TUNE_SPLITS:
+        splits = 0  # the library's choice: two whole waves, or a split tail wave
     if splits is None:
         default = int(lib.qeb_cgemm_tf32x3_default_splits(op_a, m, n, k))
         kblocks = (2 * k + 31) // 32
