@@ -449,13 +449,15 @@ int sm_count() {
 }
 
 // K slices per output tile: as many as fill two whole waves of CTAs (one CTA
-// per SM); rounding up to one wave instead left a second wave of a few CTAs
+// per SM), or one whole wave when two would leave slices shorter than 64
+// K tiles; rounding up to one wave instead left a second wave of a few CTAs
 // (for 8 tiles, 152 CTAs on 148 SMs), and measured two-wave splits were
-// 25-30 % faster on the Davidson overlaps.
+// 25-30 % faster on the Davidson overlaps (K = 80 725).
 int choose_splits(int M, int N, int K) {
   const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
   const int kblocks = (2 * K + BKF - 1) / BKF;
   int s = (2 * sm_count()) / tiles;
+  if (s > 0 && kblocks / s < 64) s = sm_count() / tiles;
   if (s > kblocks / 4) s = kblocks / 4;  // at least four stages per slice
   if (s > 64) s = 64;
   return s < 1 ? 1 : s;
