@@ -83,3 +83,16 @@ def test_empty_basis_raises():
     with pytest.raises(ValueError):
         # |k+G| >= 50 for every G at k = (1/2, 1/2, 1/2): nothing below 1e-3 Ry
         make_bases(np.eye(3) * 100.0, np.array([0.5, 0.5, 0.5]), 1e-3)
+
+
+@pytest.mark.parametrize("length,ecutrho", [(10.26, 80.0), (15.8, 120.0), (7.3, 200.0)])
+def test_charge_extent_equals_sorted_sphere(length, ecutrho):
+    """fft_shape takes the extent of the k = 0 charge sphere without sorting
+    it; the extent must equal that of the QE-ordered sphere make_bases builds."""
+    from qe_python_b200.basis import _charge_extent, make_basis
+
+    lattice = length / 2.0 * np.array([[-1.0, 0.0, 1.0], [0.0, 1.0, 1.0], [-1.0, 1.0, 0.0]])
+    reciprocal = 2.0 * np.pi * np.linalg.inv(lattice).T
+    sphere = make_basis(reciprocal, np.zeros(3), ecutrho)
+    np.testing.assert_array_equal(_charge_extent(reciprocal, ecutrho),
+                                  np.max(np.abs(sphere.indices), axis=0))
