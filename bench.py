@@ -28,7 +28,6 @@ all host threads) on the same workload, a bounded band sample per step.
 from __future__ import annotations
 
 import argparse
-import gc
 import json
 import os
 import statistics
@@ -98,7 +97,6 @@ def scf_times(name: str) -> dict:
         walls = []
         for _ in range(2):
             system = benchmark_system(name)
-            gc.collect()
             torch.cuda.synchronize()
             started = time.perf_counter()
             result = run_scf(system, precision=precision, **options)
@@ -172,10 +170,12 @@ def barrier(world: int) -> None:
 # clocks sampled during the timed region
 
 class ClockSampler:
-    """SM clocks and slowdown reasons of one GPU during a timed region
-    (read only).  NVML is polled from a thread every 10 ms, with one sample
-    at entry and one at exit, so a region of a few milliseconds still has
-    samples; without NVML, ``nvidia-smi -lms 200`` is read instead."""
+    """SM clocks and slowdown reasons of one GPU around a timed region (read
+    only), from ``nvidia-smi -lms 200``.  Entry waits (at most 3 s) until
+    the sampler has printed its first line, so the samples of the region
+    are not lost to its start-up; exit waits (at most 1 s) for one more
+    line, so a region shorter than the 200 ms period still has the sample
+    taken as it ends."""
 
     QUERY = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
@@ -184,47 +184,16 @@ class ClockSampler:
     def __init__(self, index: int) -> None:
         self.index = index
         self.samples: list[list[str]] = []
+        self._lines: list[list[str]] = []
         self._proc = None
         self._thread = None
-        self._nvml = None
-        self._handle = None
-        self._stop = threading.Event()
+        self._arrived = threading.Condition()
 
-    def _nvml_handle(self):
-        import pynvml
-        import torch
-
-        pynvml.nvmlInit()
-        self._nvml = pynvml
-        try:
-            bus = torch.cuda.get_device_properties(self.index).pci_bus_id
-            return pynvml.nvmlDeviceGetHandleByPciBusId(bus)
-        except Exception:  # noqa: BLE001 - fall back to the ordinal
-            return pynvml.nvmlDeviceGetHandleByIndex(self.index)
-
-    def _nvml_sample(self):
-        nv, h = self._nvml, self._handle
-        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-        flags = [nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
-                 nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap]
-        self.samples.append([str(sm), str(smax)]
-                            + ["Active" if bits & f else "Not Active" for f in flags])
-
-    def _poll(self):
-        while not self._stop.wait(0.01):
-            self._nvml_sample()
+    def _wait_for(self, count: int, seconds: float) -> None:
+        with self._arrived:
+            self._arrived.wait_for(lambda: len(self._lines) >= count, timeout=seconds)
 
     def __enter__(self):
-        try:
-            self._handle = self._nvml_handle()
-            self._nvml_sample()
-            self._thread = threading.Thread(target=self._poll, daemon=True)
-            self._thread.start()
-            return self
-        except Exception:  # noqa: BLE001 - no NVML: use nvidia-smi
-            self._nvml = self._handle = None
         try:
             self._proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
@@ -232,28 +201,28 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._thread = threading.Thread(target=self._read, daemon=True)
             self._thread.start()
+            self._wait_for(1, 3.0)
         except (OSError, ValueError):
             self._proc = None
+        self._first = len(self._lines)
         return self
 
     def _read(self):
         for line in self._proc.stdout:
-            self.samples.append([v.strip() for v in line.split(",")])
+            with self._arrived:
+                self._lines.append([v.strip() for v in line.split(",")])
+                self._arrived.notify_all()
 
     def __exit__(self, *exc):
-        if self._handle is not None:
-            self._stop.set()
-            self._thread.join(timeout=5)
-            try:
-                self._nvml_sample()
-            finally:
-                self._nvml.nvmlShutdown()
         if self._proc is not None:
+            self._wait_for(len(self._lines) + 1, 1.0)
             self._proc.terminate()
             try:
                 self._proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self._proc.kill()
+        # the samples from the last one before the region to the end
+        self.samples = self._lines[max(0, self._first - 1):]
         return False
 
     def summary(self) -> dict:
