@@ -1,7 +1,8 @@
-"""The bench's clock sampler (host logic, CPU): a stand-in ``nvidia-smi`` on
-PATH prints the query lines; a timed region shorter than the 200 ms
-sampling period must still come back with samples, and slowdown reasons
-that are active in any sample must be reported."""
+"""Host logic of bench.py (CPU).  The clock sampler: a stand-in
+``nvidia-smi`` on PATH prints the query lines; a timed region shorter than
+the 200 ms sampling period must still come back with samples, and slowdown
+reasons active in any sample must be reported.  The FFT-convention rate
+reported beside the dominant FFT pass's roofline."""
 
 from __future__ import annotations
 
@@ -50,3 +51,15 @@ def test_missing_tool_gives_no_samples(tmp_path, monkeypatch):
     with bench.ClockSampler(0) as clocks:
         pass
     assert clocks.summary() == {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+
+def test_plane_fft_rate_convention():
+    """64^3 grid, 256 bands in 0.28 ms: 2 x 5 N log2 N + 2 N flops per
+    (plane, band) with N = 64 x 64."""
+    import json
+
+    rate = bench.plane_fft_rate((64, 64, 64), 256, 0.28e-3)
+    flops = (2 * 5 * 4096 * 12 + 2 * 4096) * 64 * 256
+    assert abs(rate["achieved"] - flops / 0.28e-3 / 1e12) < 1e-9
+    assert abs(rate["frac"] - rate["achieved"] / rate["peak"]) < 1e-12
+    json.dumps(rate)
