@@ -252,8 +252,8 @@ def plane_fft_rate(shape, bands: int, seconds: float) -> dict:
     per complex transform of a full nx x ny plane, two transforms (inverse
     and forward) and the real potential product (2 flops a point) for each
     (z plane, band), against the nominal FP32 FMA peak of the 148 SMs at
-    1.965 GHz.  The kernel skips the y transforms of empty x columns, so
-    the convention counts more than it executes."""
+    1.965 GHz.  The kernel skips the x transforms of rows that hold no
+    stick, so the convention counts more than it executes."""
     nx, ny, nz = (int(v) for v in shape)
     points = nx * ny
     per_plane = 2 * 5.0 * points * np.log2(points) + 2.0 * points
