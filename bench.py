@@ -624,7 +624,9 @@ def run_b200(args) -> None:
         "clocks": graph_clocks.summary(),
         "clocks_staged": clocks.summary(),
     }
-    if args.scf and args.scf != "none":
+    # the SCF legs are single-GPU runs: under torchrun (N > 1) every rank
+    # would only repeat them, so they run at N = 1 alone
+    if args.scf and args.scf != "none" and world == 1:
         legs = [scf_times(name) for name in args.scf.split(",") if name]
         line["scf"] = legs[0] if len(legs) == 1 else legs
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
