@@ -64,7 +64,8 @@ def parse_args():
     p.add_argument("--scf", default="scf-dia216,scf-dia64",
                    help="comma-separated benchmark cells whose SCF-to-1e-8 Ry times (plain "
                         "and mixed) are reported beside the H|psi> rate (scf-fcc2, "
-                        "scf-fcc2-smear, scf-dia8-disp, scf-dia64, scf-dia216, or none)")
+                        "scf-fcc2-smear, scf-dia8-disp, scf-dia64, scf-dia216, or none); "
+                        "run at N = 1 only")
     return p.parse_args()
 
 
