@@ -10,8 +10,9 @@ synthetic inputs (qe_python_b200/workloads.py).
              projector GEMMs), inputs resident in HBM; L2 is flushed before
              every timed step (a 256 MiB write).
   fp64       the same for the plain FP64 form.
-  e2e        bands/s through the public PlaneWaveHamiltonian.apply call with
-             pinned host buffers: H2D of psi and D2H of H psi in the timed region.
+  e2e        bands/s through the public HostStreamedHpsi call (the Hamiltonian
+             applied to host-resident bands in 64-band chunks) with pinned host
+             buffers: H2D of psi and D2H of H psi in the timed region.
   roofline   the dominant kernel's algorithmic bytes (FFT passes) or flops
              (GEMMs) per launch over its CUDA-event duration.
   cpu_baseline  the oracle (NumPy/SciPy restatement of the reference's
@@ -75,6 +76,33 @@ def parse_args():
 PASS_B_NCU_TRAFFIC = {("pass_b", 256): 100.64e6}
 
 
+# How the SCF benchmark cells differ from the configurations they stand for:
+# with the synthetic pseudopotential the diamond supercells are semimetals,
+# which fixed filling and plain Broyden do not converge (qe_python_b200/configs.py).
+SCF_CELL_CHANGES = {
+    "scf-dia64": ["Gaussian smearing, degauss 0.02 Ry (configuration: fixed occupations)",
+                  "Thomas-Fermi Broyden mixing (configuration: default plain Broyden)",
+                  "unshifted 2x2x2 k mesh, 4 irreducible points (the shifted mesh reduces "
+                  "to one point under the cubic group)"],
+    "scf-dia216": ["Gaussian smearing, degauss 0.02 Ry (configuration: fixed occupations)",
+                   "Thomas-Fermi Broyden mixing (configuration: default plain Broyden)"],
+}
+
+
+def scf_cell_config(name: str) -> dict:
+    """The SCF cell's settings as run, with its changes from the named
+    benchmark configuration."""
+    from qe_python_b200.scf import benchmark_system
+
+    system = benchmark_system(name)
+    return {"atoms": len(system.positions), "ecutwfc_ry": system.ecutwfc,
+            "ecutrho_ry": system.ecutrho, "nbnd": system.nbnd,
+            "kpoints": int(len(system.kpoints)), "occupations": system.occupations,
+            "smearing": system.smearing if system.occupations == "smearing" else None,
+            "degauss_ry": system.degauss, "mixing_mode": system.mixing_mode,
+            "mixing_beta": system.mixing_beta, "changes": SCF_CELL_CHANGES.get(name, [])}
+
+
 def scf_times(name: str) -> dict:
     """Wall time of the GPU SCF to conv_thr = 1e-8 Ry, plain FP64 and mixed,
     with the mixed form's energy, eigenvalue and force differences from the
@@ -90,7 +118,7 @@ def scf_times(name: str) -> dict:
 
     from qe_python_b200.scf import MIXED_GUARD_BANDS, benchmark_system, run_scf
 
-    out = {"cell": name, "conv_thr_ry": 1.0e-8}
+    out = {"cell": name, "conv_thr_ry": 1.0e-8, "config": scf_cell_config(name)}
     results = {}
     runs = (("f64", "f64", {}), ("mixed", "mixed", {}),
             ("f64_guard_bands", "f64", {"guard_bands": MIXED_GUARD_BANDS}))
@@ -170,9 +198,21 @@ def barrier(world: int) -> None:
 # ---------------------------------------------------------------------------
 # clocks sampled during the timed region
 
+def smi_device_id(local: int) -> str:
+    """The PCI bus id (domain:bus:device.function, hex) of torch device
+    ``local``.  nvidia-smi numbers GPUs in its own (PCI) order and ignores
+    CUDA_VISIBLE_DEVICES, so a torch index can name another GPU there; the
+    bus id names the same physical device in both."""
+    import torch
+
+    props = torch.cuda.get_device_properties(local)
+    return f"{props.pci_domain_id:08X}:{props.pci_bus_id:02X}:{props.pci_device_id:02X}.0"
+
+
 class ClockSampler:
     """SM clocks and slowdown reasons of one GPU around a timed region (read
-    only), from ``nvidia-smi -lms 200``.  Entry waits (at most 3 s) until
+    only), from ``nvidia-smi -lms 200``; ``device_id`` is what nvidia-smi's
+    ``--id`` takes (the PCI bus id from ``smi_device_id``).  Entry waits (at most 3 s) until
     the sampler has printed its first line, so the samples of the region
     are not lost to its start-up; exit waits (at most 1 s) for one more
     line, so a region shorter than the 200 ms period still has the sample
@@ -182,8 +222,8 @@ class ClockSampler:
              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
              "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int) -> None:
-        self.index = index
+    def __init__(self, device_id) -> None:
+        self.device_id = str(device_id)
         self.samples: list[list[str]] = []
         self._lines: list[list[str]] = []
         self._proc = None
@@ -197,7 +237,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self._proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                ["nvidia-smi", f"--id={self.device_id}", f"--query-gpu={self.QUERY}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._thread = threading.Thread(target=self._read, daemon=True)
@@ -433,7 +473,7 @@ def run_b200(args) -> None:
         return times, stages, launches
 
     # timed region of the headline value
-    with ClockSampler(local) as clocks:
+    with ClockSampler(smi_device_id(local)) as clocks:
         barrier(world)
         torch.cuda.synchronize()
         times, stages, launches = timed_loop("mixed", args.steps, args.warmup, profile=True)
@@ -469,7 +509,7 @@ def run_b200(args) -> None:
         # library's launch counter only sees launches made through its API
         return max_over_ranks(statistics.mean(samples), world, device), graph
 
-    with ClockSampler(local) as graph_clocks:
+    with ClockSampler(smi_device_id(local)) as graph_clocks:
         step_ms, mixed_graph = graph_loop("mixed")
     fp64_graph_ms, fp64_graph = graph_loop("fp64")
     del fp64_graph
@@ -630,6 +670,7 @@ def run_b200(args) -> None:
     if args.scf and args.scf != "none" and world == 1:
         legs = [scf_times(name) for name in args.scf.split(",") if name]
         line["scf"] = legs[0] if len(legs) == 1 else legs
+        line["config"]["scf_cells"] = {leg["cell"]: leg["config"] for leg in legs}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         sample = 16

@@ -143,7 +143,11 @@ int qeb_cgemm(int opa, int M, int N, int K, const double* alpha, const void* A, 
  * allocates nothing.  It rejects M*N > capacity/32 (two complex128 partial
  * slices must fit) with QEB_STATUS_EUNSUPPORTED.  The first call on a device
  * looks up the array's device address (cudaGetSymbolAddress) with that
- * device current; make that first call before any stream capture.  All
+ * device current; make that first call before any stream capture.  The
+ * address is cached per device index for the life of the process, so it
+ * assumes the runtime's primary context throughout: after cudaDeviceReset,
+ * or with another context made current, the cached address is stale and
+ * this entry point must not be called.  All
  * calls share the one array and each call overwrites every partial entry it
  * reads, so nothing needs clearing between calls; calls that overlap on the
  * GPU (different streams, or different host threads) race on the array and

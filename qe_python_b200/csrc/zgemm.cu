@@ -557,7 +557,9 @@ void* g_static_address[kMaxDevices] = {nullptr};
 
 // Device address of g_static_partials on the current device.  The host-side
 // symbol is only a stand-in, so the address is looked up once per device
-// (with that device current) and cached.
+// (with that device current) and cached for the life of the process; the
+// cache assumes the primary context of each device throughout (a
+// cudaDeviceReset or another current context leaves it stale).
 int static_partials(void** out) {
   int device = 0;
   cudaError_t err = cudaGetDevice(&device);

@@ -294,6 +294,171 @@ def mixer_tables() -> None:
     print("broyden: plain and TF sequences")
 
 
+class _Captured(Exception):
+    """Raised by the capturing Davidson stand-in once every k point's
+    first-iteration Hamiltonian has been built."""
+
+
+def _c_order_potential(ham) -> np.ndarray:
+    """The reference Hamiltonian's real V_eff(r) as a C-order (nx, ny, nz) grid."""
+    v = np.asarray(ham.real_potential, dtype=np.float64)
+    shape = tuple(int(s) for s in ham.local_workspace.shape)
+    if ham.native_potential_layout:  # (nz, nx, ny) native layout
+        v = v.reshape(shape[2], shape[0], shape[1]).transpose(1, 2, 0)
+    return np.ascontiguousarray(v.reshape(shape))
+
+
+def potential_checksums(v: np.ndarray, seed: int) -> dict:
+    """Size-independent fingerprints of a real grid: sum, sum of squares and
+    the dot product with a seeded uniform field."""
+    field = np.random.default_rng(seed).uniform(-1.0, 1.0, v.shape)
+    return {"sum": float(np.sum(v)), "sum_sq": float(np.sum(v * v)),
+            "probe": float(np.sum(v * field))}
+
+
+def probe_vectors(npw: int, count: int, seed: int, kinetic: np.ndarray) -> np.ndarray:
+    """Seeded complex Gaussian columns scaled by exp(-T_G/10) (the test
+    draws the same columns with the same generator)."""
+    rng = np.random.default_rng(seed)
+    psi = rng.standard_normal((npw, count)) + 1j * rng.standard_normal((npw, count))
+    return np.asfortranarray(psi * np.exp(-np.asarray(kinetic) / 10.0)[:, None])
+
+
+def first_iteration(name: str, workdir: Path, filename: str, roots: int) -> None:
+    """The reference's first-SCF-iteration Hamiltonian of every k point of a
+    benchmark cell (starting V_eff from the uniform density, the reference's
+    own projector construction qepy_pw/pw/scf.py:596-718, its
+    PlaneWaveHamiltonian qepy_pw/diagonalization.py:124-368), captured at
+    its Davidson call site (qepy_pw/pw/scf.py:3510) and then:
+      * fingerprints of V_eff(r) and of the preconditioner diagonal,
+      * <psi|H|psi> and <w|H|psi> of seeded probe columns,
+      * the lowest ``roots`` eigenvalues by the reference's davidson from a
+        seeded start, converged to 1e-10 Ha (tight, so path independent).
+    The run stops once every k point's operator is captured; the starting
+    subspace and rotate_wfc are skipped (they play no part here)."""
+    import qepy_pw.pw.scf as ref_scf
+    from qepy_pw.diagonalization import DavidsonResult, davidson
+    from qepy_pw.scf import run_scf
+
+    pw = read_config(name, workdir)
+    nk = len(pw.kpoints)
+    captured = []
+
+    def capture(operator, diagonal, number, **options):
+        captured.append(operator.__self__)
+        if len(captured) == nk:
+            raise _Captured
+        start = options["initial_vectors"]
+        return DavidsonResult(np.zeros(number), np.asfortranarray(start[:, :number]),
+                              np.zeros(number), 1, True, 0, 0)
+
+    def cheap_orbitals(pw_, pseudos, basis, bands, **_kw):
+        out = np.zeros((len(basis), bands), dtype=np.complex128, order="F")
+        out[np.arange(bands), np.arange(bands)] = 1.0
+        return out
+
+    def no_rotation(operator, trials, bands, mpi=None):
+        return np.asfortranarray(trials[:, :bands]), np.zeros(bands), None
+
+    saved = (ref_scf.davidson, ref_scf._atomic_starting_orbitals,
+             ref_scf._rotate_starting_subspace)
+    ref_scf.davidson = capture
+    ref_scf._atomic_starting_orbitals = cheap_orbitals
+    ref_scf._rotate_starting_subspace = no_rotation
+    started = time.perf_counter()
+    try:
+        run_scf(pw)
+    except _Captured:
+        pass
+    finally:
+        (ref_scf.davidson, ref_scf._atomic_starting_orbitals,
+         ref_scf._rotate_starting_subspace) = saved
+    print(f"{name}: captured {len(captured)} operators in {time.perf_counter() - started:.1f} s")
+    record = {"config": name, "roots": roots, "davidson_tolerance_ha": 1.0e-10,
+              "probe_seed": 20261203, "probe_columns": 4, "kpoints": []}
+    for k, ham in enumerate(captured):
+        basis = ham.basis
+        v = _c_order_potential(ham)
+        diagonal = np.asarray(ham.diagonal)
+        psi = probe_vectors(len(basis), 4, 20261203 + k, basis.kinetic)
+        probes = probe_vectors(len(basis), 4, 20261303 + k, np.zeros(len(basis)))
+        hpsi = ham.apply(psi)
+        quad = psi.conj().T @ hpsi
+        cross = probes.conj().T @ hpsi
+        t0 = time.perf_counter()
+        start = probe_vectors(len(basis), roots, 20261403 + k, basis.kinetic)
+        solution = davidson(ham.apply, diagonal, roots, initial_vectors=start,
+                            tolerance=1.0e-10, max_iterations=400, subspace_multiplier=4,
+                            residual_factor=None, operator_into=ham.apply_into)
+        print(f"  k {k}: npw {len(basis)} davidson {solution.iterations} its "
+              f"converged {solution.converged} in {time.perf_counter() - t0:.1f} s; "
+              f"lowest {solution.eigenvalues[:3]}")
+        record["kpoints"].append({
+            "npw": len(basis),
+            "miller_sha256": sha(basis.indices),
+            "potential": potential_checksums(v, 7),
+            "potential_average": float(ham.potential_average),
+            "diagonal": {"sum": float(np.sum(diagonal)),
+                         "sum_sq": float(np.sum(diagonal * diagonal)),
+                         "max": float(np.max(diagonal))},
+            "hpsi_norms": np.linalg.norm(hpsi, axis=0).tolist(),
+            "psi_h_psi": {"re": quad.real.tolist(), "im": quad.imag.tolist()},
+            "probe_h_psi": {"re": cross.real.tolist(), "im": cross.imag.tolist()},
+            "eigenvalues_ha": np.asarray(solution.eigenvalues).tolist(),
+            "davidson_converged": bool(solution.converged),
+            "davidson_iterations": float(solution.iterations),
+        })
+    record["reference_wall_seconds"] = time.perf_counter() - started
+    record["reference_runner"] = "reference Python + NumPy oracle native module, 1 process"
+    (HERE / filename).write_text(json.dumps(record, indent=1))
+
+
+def displaced_energies(workdir: Path, filename: str, coordinates, step: float) -> None:
+    """Reference total energies of scf-dia8-disp with one atom coordinate
+    moved by +-``step`` bohr (central differences of E_tot give the force
+    on that coordinate), conv_thr tightened to 1e-10 Ry so the energy error
+    stays well below step x 1e-4 Ry/bohr."""
+    from qepy_pw.pw.input import read_pw_input
+    from qepy_pw.scf import run_scf
+
+    from qe_python_b200.configs import config_input
+    from qe_python_b200.pseudo import write_synthetic_upf
+
+    write_synthetic_upf(workdir / "X.upf")
+    base = config_input("scf-dia8-disp", str(workdir))
+    record = {"config": "scf-dia8-disp", "step_bohr": step, "conv_thr_ry": 1.0e-10,
+              "entries": []}
+    for atom, axis in coordinates:
+        energies = {}
+        for sign in (+1, -1):
+            text = _displace(base, atom, axis, sign * step)
+            text = text.replace("conv_thr = 1e-08", "conv_thr = 1e-10")
+            path = workdir / f"disp_{atom}_{axis}_{sign}.in"
+            path.write_text(text)
+            pw = read_pw_input(path)
+            t0 = time.perf_counter()
+            result = run_scf(pw)
+            energies[sign] = 2.0 * float(result.iterations[-1].total_energy_ha)
+            print(f"atom {atom} axis {axis} sign {sign:+d}: E = {energies[sign]:.10f} Ry "
+                  f"({len(result.iterations)} its, {time.perf_counter() - t0:.1f} s)")
+        record["entries"].append({
+            "atom": atom, "axis": axis, "energy_plus_ry": energies[+1],
+            "energy_minus_ry": energies[-1],
+            "force_ry_per_bohr": -(energies[+1] - energies[-1]) / (2.0 * step)})
+        (HERE / filename).write_text(json.dumps(record, indent=1))
+
+
+def _displace(text: str, atom: int, axis: int, delta: float) -> str:
+    """Move one atom of a pw.x input's ATOMIC_POSITIONS (bohr) block."""
+    lines = text.splitlines()
+    start = next(i for i, line in enumerate(lines) if line.startswith("ATOMIC_POSITIONS"))
+    fields = lines[start + 1 + atom].split()
+    values = [float(v) for v in fields[1:4]]
+    values[axis] += delta
+    lines[start + 1 + atom] = f"  {fields[0]} {values[0]:.12f} {values[1]:.12f} {values[2]:.12f}"
+    return "\n".join(lines) + "\n"
+
+
 def si_regression() -> None:
     path = REFERENCE_ROOT / "tests/qe_reference/reference/pw_scf/scf.in.out"
     text = path.read_text()
@@ -311,8 +476,25 @@ def si_regression() -> None:
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--skip-scf", action="store_true")
+    parser.add_argument("--only", default=None,
+                        help="comma-separated subset: first-iteration-dia64, "
+                             "first-iteration-dia216, fd-forces")
     args = parser.parse_args()
     load_reference()
+    if args.only:
+        with tempfile.TemporaryDirectory() as tmp:
+            workdir = Path(tmp)
+            for part in args.only.split(","):
+                if part == "first-iteration-dia64":
+                    first_iteration("scf-dia64", workdir, "first_iteration_dia64.json", 32)
+                elif part == "first-iteration-dia216":
+                    first_iteration("scf-dia216", workdir, "first_iteration_dia216.json", 32)
+                elif part == "fd-forces":
+                    displaced_energies(workdir, "fd_forces_dia8.json",
+                                       [(0, 0), (3, 1), (5, 2), (6, 0)], 1.0e-3)
+                else:
+                    raise SystemExit(f"unknown part {part!r}")
+        return
     with tempfile.TemporaryDirectory() as tmp:
         workdir = Path(tmp)
         index_maps(workdir)

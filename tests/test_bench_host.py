@@ -63,3 +63,31 @@ def test_plane_fft_rate_convention():
     assert abs(rate["achieved"] - flops / 0.28e-3 / 1e12) < 1e-9
     assert abs(rate["frac"] - rate["achieved"] / rate["peak"]) < 1e-12
     json.dumps(rate)
+
+
+def test_sampler_passes_the_device_id(tmp_path, monkeypatch):
+    """nvidia-smi gets the id it was given (a PCI bus id), not a torch index."""
+    record = tmp_path / "args.txt"
+    script = tmp_path / "nvidia-smi"
+    script.write_text("#!/bin/bash\n"
+                      f"echo \"$@\" > {record}\n"
+                      "while true; do echo \"1965, 1965, Not Active, Not Active, Not Active, "
+                      "Not Active\"; sleep 0.2; done\n")
+    script.chmod(script.stat().st_mode | stat.S_IEXEC)
+    monkeypatch.setenv("PATH", f"{tmp_path}{os.pathsep}{os.environ['PATH']}")
+    with bench.ClockSampler("00000000:1B:00.0") as clocks:
+        time.sleep(0.01)
+    assert clocks.summary()["samples"] >= 1
+    args = record.read_text().split()
+    assert "--id=00000000:1B:00.0" in args
+
+
+def test_smi_device_id_format(monkeypatch):
+    """domain:bus:device.function in upper-case hex, as nvidia-smi prints it."""
+    import types
+
+    import torch
+
+    props = types.SimpleNamespace(pci_domain_id=0, pci_bus_id=0x1B, pci_device_id=0)
+    monkeypatch.setattr(torch.cuda, "get_device_properties", lambda index: props)
+    assert bench.smi_device_id(3) == "00000000:1B:00.0"

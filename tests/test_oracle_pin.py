@@ -20,6 +20,7 @@ import pytest
 
 from oracle import native_fft as oracle
 from qe_python_b200.basis import grid_slots, potential_matrix
+from tests.golden import reference_env
 
 GOLDEN = Path(__file__).resolve().parent / "golden"
 
@@ -97,7 +98,7 @@ def test_qe_random_stream_is_deterministic():
     assert np.all((a1 >= 0) & (a1 < 1))
 
 
-@pytest.mark.skipif(not (Path("/root/reference") / "qepy_pw").is_dir(),
+@pytest.mark.skipif(not reference_env.reference_available(),
                     reason="the reference tree is only present in the build container")
 def test_oracle_reproduces_reference_si_regression():
     from tests.golden.reference_env import REFERENCE_ROOT, load_reference

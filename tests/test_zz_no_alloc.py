@@ -3,9 +3,13 @@
 ``qeb_zgemm_static_scratch`` serves callers that cannot allocate device
 memory (for example code running inside a memory pool it does not own): its
 split-K partial tiles live in a fixed array inside the library instead of in
-caller scratch.  This test calls it through the C ABI twice in a row, with
-different operands, and checks each result against ``qeb_zgemm`` with
-caller-provided scratch at the GEMM tolerance used elsewhere (1e-13 relative).
+caller scratch.  This test calls it through the C ABI several times in a
+row, with different operands, and checks each result against an
+independent complex128 product on the host (NumPy) and against
+``qeb_zgemm`` with caller-provided scratch, at the GEMM tolerance used
+elsewhere (1e-13 relative, scaled by sqrt(K)).  The shapes cover the tiled
+split-K path and both skinny split-K paths (a narrow output of at most 16
+columns on either side).
 It is collected last so that a failure here leaves every other test already
 run; it passes on its own in a fresh process as well.
 """
@@ -41,8 +45,10 @@ def test_static_scratch_gemm_matches_regular_entry(cuda_device):
     lib = _lib.load()
     stream = torch.cuda.current_stream().cuda_stream
     rng = np.random.default_rng(20261203)
-    # Shapes whose long K makes both entry points split K across blocks.
-    cases = [(96, 80, 20000, 0.75 - 0.25j, 0.0), (40, 33, 11019, 1.0, 0.5 + 1.0j)]
+    # Shapes whose long K makes both entry points split K across blocks: two
+    # tiled products, then a narrow M (swapped skinny plan) and a narrow N.
+    cases = [(96, 80, 20000, 0.75 - 0.25j, 0.0), (40, 33, 11019, 1.0, 0.5 + 1.0j),
+             (8, 300, 20000, 1.0, 0.0), (300, 12, 20000, -0.5 + 0.5j, 1.0)]
     for m, n, k, alpha, beta in cases:
         a, b, c0 = _operands(rng, m, n, k, torch)
         expected = c0.clone()
@@ -61,9 +67,11 @@ def test_static_scratch_gemm_matches_regular_entry(cuda_device):
                                               stream)
         _lib.check("qeb_zgemm_static_scratch", status)
         torch.cuda.synchronize()
-        exp = expected.cpu().numpy()
-        err = np.max(np.abs(got.cpu().numpy() - exp))
-        assert err <= RTOL * max(1.0, np.sqrt(k)) * np.max(np.abs(exp))
+        host = alpha * (a.cpu().numpy().conj().T @ b.cpu().numpy()) + beta * c0.cpu().numpy()
+        bound = RTOL * max(1.0, np.sqrt(k)) * np.max(np.abs(host))
+        result = got.cpu().numpy()
+        assert np.max(np.abs(result - host)) <= bound, (m, n, k)
+        assert np.max(np.abs(result - expected.cpu().numpy())) <= bound, (m, n, k)
 
 
 def test_static_scratch_gemm_rejects_oversized_output(cuda_device):
