@@ -908,6 +908,208 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
                           completed, False, unconverged_count, applications)
 
 
+def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
+                           tolerance: float = 1.0e-8, max_iterations: int = 20,
+                           subspace_multiplier: int = 2, occupied_roots: int | None = None,
+                           timers=None):
+    """Chosen-form Davidson: an FP64 Ritz block with FP32 corrections.
+
+    A generator like ``davidson_steps``; it yields ``(vectors, destination)``
+    for destination = H vectors, with complex128 vectors when it needs the
+    FP64 Hamiltonian and complex64 vectors for the chosen form's (FP32 FFT
+    passes, split-TF32 projector GEMMs).  Same criteria as the reference's
+    Davidson (qepy_pw/diagonalization.py:527-880): the lowest roots of the
+    reduced problem, converged when |e - e_previous| is below the root's
+    threshold (occupied roots ``tolerance``, the others max(5 tol, 5e-6)),
+    restart when the subspace is full, results as DavidsonResult with
+    complex128 eigenvectors.
+
+    How FP64 accuracy comes out of FP32 work.  The block X (the roots'
+    vectors, complex128) is first made a Ritz block of the FP64 Hamiltonian:
+    one FP64 H application, X^H H X and X^H X in FP64, the FP64 reduced
+    eigensolve and the rotation, so that X^H H X = diag(lam) and X^H X = 1
+    to FP64 round-off and R = H X - X lam is an FP64 residual.  The
+    subspace is then [X, D_1, D_2, ...] with FP32 correction blocks D_j and
+    their chosen-form products H D_j.  Its reduced matrices take
+      * the X-X block as diag(lam) and 1 exactly;
+      * the D-X blocks as S_DX = D^H X32 and H_DX = S_DX lam + D^H R32
+        (X^H H D = (H X)^H D = lam X^H D + R^H D), both from the same
+        FP32-accurate S_DX: an error in S_DX is an exact Rayleigh-Ritz step
+        on [X, D + X dS^H], which spans the same space, so it does not
+        reach the Ritz values;
+      * the D-D blocks from FP32 products, whose errors enter the Ritz
+        values through the squared correction coefficients only.
+    The residuals of unconverged roots, sum of X (lam - e) c_X + R c_X +
+    (H D_j - e D_j) c_j, are formed in FP32 from terms that shrink as the
+    roots converge.  At a restart and at the end the vectors X c_X + D c_D
+    are formed with the X part in FP64.  FP64 work per solve: one FP64 H
+    application of the block and four FP64 GEMMs (npw x n x n) at the start
+    and at each restart, one FP64 GEMM at the end."""
+    device = require_cuda()
+    diag = to_device_f(diagonal, torch.float64, device).reshape(-1)
+    npw = diag.numel()
+    n = int(number_of_roots)
+    if not 1 <= n <= npw:
+        raise ValueError("number_of_roots must be between 1 and the matrix size")
+    if tolerance <= 0.0:
+        raise ValueError("Davidson tolerance must be positive")
+    if max_iterations < 1:
+        raise ValueError("Davidson max_iterations must be at least 1")
+    if subspace_multiplier < 2:
+        raise ValueError("diago_david_ndim must be at least 2")
+    if occupied_roots is None:
+        occupied_roots = n
+    if not 0 <= occupied_roots <= n:
+        raise ValueError("occupied_roots must be between zero and number_of_roots")
+    root_tolerances = np.full(n, max(5.0 * tolerance, 5.0e-6))
+    root_tolerances[:occupied_roots] = tolerance
+    trial = to_device_f(initial_vectors, torch.complex128, device)
+    if trial.dim() != 2 or trial.shape[0] != npw or trial.shape[1] < n:
+        raise ValueError("initial_vectors must have shape (matrix size, at least number_of_roots)")
+    maximum_subspace = min(npw, max(2 * n, subspace_multiplier * n))
+    if maximum_subspace <= n:
+        raise ValueError("the subspace has no room for corrections")
+    f32 = torch.complex64
+    basis32 = empty_f(npw, maximum_subspace, f32, device)
+    applied32 = empty_f(npw, maximum_subspace, f32, device)
+    projected = torch.zeros((maximum_subspace, maximum_subspace), dtype=torch.complex128,
+                            device=device)
+    overlap = torch.zeros_like(projected)
+    eye = torch.eye(n, dtype=torch.complex128, device=device)
+    x = empty_f(npw, n, torch.complex128, device)
+    x.copy_(trial[:, :n])
+    del trial
+    hx = empty_f(npw, n, torch.complex128, device)
+    state = {"applications": 0}
+
+    def ritz_block(vectors):
+        """FP64 Rayleigh-Ritz of ``vectors``: returns (X, lam, R) with X the
+        Ritz vectors, lam their values and R = H X - X lam."""
+        yield vectors, hx
+        state["applications"] += n
+        with _timer(timers, "cegterg:over"):
+            a = _hermitize(K.gemm(K.OP_C, vectors, hx))
+            s = _hermitize(K.gemm(K.OP_C, vectors, vectors))
+        with _timer(timers, "cdiaghg"):
+            lam, rot = lowest_generalized_eigh(a, s, n)
+        with _timer(timers, "cegterg:upda"):
+            rot = rot.T.contiguous().T
+            ritz = K.gemm(K.OP_N, vectors, rot)
+            residual = K.gemm(K.OP_N, hx, rot)
+            K.subtract_band_energies(residual, ritz, lam)
+        return ritz, lam, residual
+
+    def start_block(ritz, lam, residual):
+        basis32[:, :n].copy_(ritz)
+        applied32[:, :n].copy_(residual)
+        projected[:n, :n] = torch.diag(lam.to(torch.complex128))
+        overlap[:n, :n] = eye
+
+    def update_projected(first_new: int, active: int, lam_dev) -> None:
+        with _timer(timers, "cegterg:over"):
+            new = basis32[:, first_new:active]
+            h_rows = K.gemm(K.OP_C, new, applied32[:, :active]).to(torch.complex128)
+            s_rows = K.gemm(K.OP_C, new, basis32[:, :active]).to(torch.complex128)
+            h_rows[:, :n] += s_rows[:, :n] * lam_dev.to(torch.complex128)[None, :]
+            projected[first_new:active, :active] = h_rows
+            overlap[first_new:active, :active] = s_rows
+            projected[:first_new, first_new:active] = h_rows[:, :first_new].conj().T
+            overlap[:first_new, first_new:active] = s_rows[:, :first_new].conj().T
+            block = slice(first_new, active)
+            projected[block, block] = _hermitize(projected[block, block])
+            overlap[block, block] = _hermitize(overlap[block, block])
+
+    def composite_residuals(coefficients, roots, lam_dev, active):
+        """FP32 residuals H V c - e V c of the selected roots."""
+        with _timer(timers, "cegterg:upda"):
+            shift = torch.empty_like(coefficients)
+            shift[:n] = coefficients[:n] * (lam_dev[:, None] - roots[None, :])
+            shift[n:] = -coefficients[n:] * roots[None, :]
+            left = empty_f(active, coefficients.shape[1], f32, device)
+            left.copy_(shift)
+            right = empty_f(active, coefficients.shape[1], f32, device)
+            right.copy_(coefficients)
+            out = K.gemm(K.OP_N, basis32[:, :active], left)
+            K.gemm(K.OP_N, applied32[:, :active], right, out, beta=1.0)
+        return out
+
+    def vectors_of(xblock, coefficients, active):
+        """X c_X (FP64) + D c_D (FP32) of every root."""
+        with _timer(timers, "cegterg:last"):
+            c = coefficients[:, :n]
+            out = K.gemm(K.OP_N, xblock, c[:n].T.contiguous().T)
+            if active > n:
+                low = empty_f(active - n, n, f32, device)
+                low.copy_(c[n:active])
+                out += K.gemm(K.OP_N, basis32[:, n:active], low).to(torch.complex128)
+        return out
+
+    x, lam_dev, r = yield from ritz_block(x)
+    start_block(x, lam_dev, r)
+    active = n
+    values = lam_dev.cpu().numpy()
+    values_dev = lam_dev
+    coefficients = None
+    block = applied32[:, :n]
+    energies = lam_dev
+    unconverged = np.ones(n, dtype=bool)
+    completed = 0
+    for iteration in range(1, max_iterations + 1):
+        completed = iteration
+        previous = values
+        with _timer(timers, "g_psi"):
+            corrections = K.precondition(block, energies, diag)
+        norms2 = K.column_squared_norms(corrections)
+        norms_host = norms2.cpu().numpy()
+        scale = max(float(np.max(norms_host)), 1.0e-300) if len(norms_host) else 0.0
+        keep = np.flatnonzero(norms_host > (1.0e-14 ** 2) * scale) if scale else np.empty(0, int)
+        if keep.size == 0:
+            break
+        old = active
+        active += keep.size
+        selected = torch.as_tensor(keep.astype(np.int64), device=device)
+        K.normalize_columns(corrections, norms2, selected, basis32[:, old:active])
+        del corrections, block
+        yield basis32[:, old:active], applied32[:, old:active]
+        state["applications"] += keep.size
+        update_projected(old, active, lam_dev)
+        with _timer(timers, "cdiaghg"):
+            roots, coefficients = lowest_generalized_eigh(
+                projected[:active, :active], overlap[:active, :active], n)
+        values_dev = roots
+        values = roots.cpu().numpy()
+        converged = np.abs(values - previous) < root_tolerances
+        unconverged = ~converged
+        count = int(np.count_nonzero(unconverged))
+        if count == 0:
+            break
+        index = torch.as_tensor(np.flatnonzero(unconverged), device=device)
+        if active + count > maximum_subspace:
+            # restart on the Ritz vectors, made exact again in FP64
+            x = vectors_of(x, coefficients, active)
+            x, lam_dev, r = yield from ritz_block(x)
+            start_block(x, lam_dev, r)
+            active = n
+            coefficients = None
+            block = _select_columns(applied32[:, :n], index).T.contiguous().T
+            energies = lam_dev.index_select(0, index)
+            continue
+        energies = values_dev.index_select(0, index)
+        block = composite_residuals(coefficients.index_select(1, index), energies, lam_dev,
+                                    active)
+    if coefficients is None:
+        vectors, final_values = x, lam_dev.cpu().numpy()
+        norms = np.sqrt(np.maximum(K.column_squared_norms(r).cpu().numpy(), 0.0))
+    else:
+        vectors = vectors_of(x, coefficients, active)
+        final_values = values
+        residual = composite_residuals(coefficients, values_dev, lam_dev, active)
+        norms = np.sqrt(np.maximum(K.column_squared_norms(residual).cpu().numpy(), 0.0))
+    count = int(np.count_nonzero(unconverged))
+    return DavidsonResult(final_values, vectors, norms, completed, count == 0, count,
+                          state["applications"])
+
+
 def _select_columns(matrix: torch.Tensor, index: torch.Tensor) -> torch.Tensor:
     """Columns ``index`` of a column-major matrix, column-major."""
     return matrix.T.index_select(0, index).T

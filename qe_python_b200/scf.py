@@ -40,6 +40,7 @@ from .diagonalization import (
     davidson,
     davidson_steps,
     lowest_generalized_eigh,
+    refined_davidson_steps,
     run_lockstep,
 )
 from .pseudo import SyntheticPseudo, synthetic_pseudo
@@ -331,6 +332,10 @@ class SCFResult:
     timings: dict[str, float] = field(default_factory=dict)
     occupations: list[np.ndarray] = field(default_factory=list)
     fermi_energy_ha: float | None = None
+    # the last iteration's input V_eff(r) (device, C-order) and each local k
+    # point's eigenvectors (device, complex128, nbnd + guard columns)
+    potential: "torch.Tensor | None" = None
+    eigenvectors: list = field(default_factory=list)
 
     @property
     def total_energy_ry(self) -> float:
@@ -432,26 +437,103 @@ def projector_terms(system: System, tables: dict, basis) -> tuple:
     return tuple(terms)
 
 
+@dataclass
+class SCFSetup:
+    """Fixed-ion pieces of an SCF: bases, FFT grid, charge sphere, species
+    tables and the ionic local potential (qepy_pw/pw/scf.py:2193-2330)."""
+
+    bases: list
+    shape: tuple
+    grid: ChargeGrid
+    cgrid: DeviceChargeGrid
+    tables: dict
+    v_ion: torch.Tensor          # V_ion(r), C-order (nx, ny, nz) float64 on the device
+    v_ion_average: float         # its G = 0 component (QE v_of_0)
+
+
+def scf_setup(system: System, device) -> SCFSetup:
+    """Bases of every k point, the FFT grid by the reference's rule, the
+    charge sphere and V_ion(r) = sum_species V_loc(|G|) S(G)."""
+    reciprocal = system.reciprocal
+    bases = make_bases(reciprocal, system.kpoints, system.ecutwfc)
+    shape = fft_shape(bases, reciprocal, system.ecutrho, fft_factors(system.operations))
+    grid = ChargeGrid(shape, reciprocal, system.ecutrho)
+    tables = {label: SpeciesTables(p, system.volume) for label, p in system.pseudos.items()}
+    q = np.sqrt(grid.g2)
+    v_ion_g = np.zeros(len(grid.g2), dtype=np.complex128)
+    for label, table in tables.items():
+        pos = np.array([p for p, l in zip(system.positions, system.labels) if l == label])
+        structure = gpu_structure_factor(grid.vectors, pos, np.ones(len(pos)))
+        v_ion_g += table.vloc(q) * structure
+    cgrid = DeviceChargeGrid(grid, device)
+    v_ion = cgrid.to_r(torch.from_numpy(v_ion_g).to(device))
+    v_ion_average = float(np.real(np.sum(v_ion_g[grid.g2 < 1.0e-14])))
+    return SCFSetup(bases, tuple(shape), grid, cgrid, tables, v_ion, v_ion_average)
+
+
+def starting_density(system: System, setup: SCFSetup) -> torch.Tensor:
+    """Uniform starting density rho = nelec / Omega (no PP_RHOATOM,
+    qepy_pw/pw/scf.py:1004-1012)."""
+    return torch.full(setup.shape, system.nelec / system.volume, dtype=torch.float64,
+                      device=setup.v_ion.device)
+
+
+def hxc_potential(setup: SCFSetup, rho: torch.Tensor) -> torch.Tensor:
+    """V_H(r) + V_xc(r) of a density (Hartree 4 pi rho(G)/G^2, PZ81 LDA)."""
+    cgrid = setup.cgrid
+    vh = cgrid.to_r(cgrid.hartree(cgrid.to_g(rho)))
+    _eps, vxc = device_pz81(rho)
+    return vh + vxc
+
+
+def starting_hamiltonians(system: System, precision: str = "f64", setup: SCFSetup | None = None):
+    """The first SCF iteration's Hamiltonian of every k point: V_eff =
+    V_ion + V_H + V_xc of the uniform starting density and the projector
+    terms of the fixed ions (the operator the reference hands to Davidson at
+    qepy_pw/pw/scf.py:3396-3411, 3510 in its first iteration).  Returns
+    (hamiltonians, V_eff(r) on the device, setup)."""
+    device = require_cuda()
+    setup = setup if setup is not None else scf_setup(system, device)
+    v_eff = setup.v_ion + hxc_potential(setup, starting_density(system, setup))
+    hams = []
+    for basis in setup.bases:
+        state = KPointState(basis, setup.shape, device)
+        terms = projector_terms(system, setup.tables, state.basis)
+        hams.append(PlaneWaveHamiltonian(state.basis, None, terms,
+                                         local_workspace=state.workspace(precision),
+                                         real_potential=v_eff,
+                                         potential_average=setup.v_ion_average))
+    return hams, v_eff, setup
+
+
 MIN_FP64_ITERATIONS = 3  # mixed form: FP64 iterations before convergence is accepted
 MIXED_GUARD_BANDS = 24  # mixed form: extra Davidson roots beyond nbnd (run_scf guard_bands)
 
 
 def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, tol, occ_roots,
-                   is_ritz, timers, lock=False, nroots=None):
+                   is_ritz, timers, lock=False, nroots=None, refined=False):
     """One k point's diagonalisation as a generator of H applications: the
     Davidson of qepy_pw/pw/scf.py:3496-3556 (20 iterations), repeated up to
     five more times from its last vectors while more than five roots remain
-    unconverged.  Returns (DavidsonResult, Davidson iterations)."""
+    unconverged.  ``refined``: the chosen form's FP64-accurate Davidson
+    (``refined_davidson_steps``: FP64 Ritz block, FP32 corrections).
+    Returns (DavidsonResult, Davidson iterations)."""
     attempt, total_its = 0, 0.0
     vectors, eigs, applied = start_vectors, initial_eigs, initial_applied
     while True:
-        sol = yield from davidson_steps(
-            ham.diagonal, nroots or system.nbnd, initial_vectors=vectors, tolerance=tol,
-            max_iterations=20,
-            subspace_multiplier=system.diago_david_ndim, residual_factor=None,
-            residual_energy_scale=None, occupied_roots=occ_roots, initial_is_ritz=is_ritz,
-            initial_is_orthonormal=True, initial_eigenvalues=eigs, initial_applied=applied,
-            timers=timers, dtype=ham.dtype, lock_converged=lock)
+        if refined:
+            sol = yield from refined_davidson_steps(
+                ham.diagonal, nroots or system.nbnd, initial_vectors=vectors, tolerance=tol,
+                max_iterations=20, subspace_multiplier=system.diago_david_ndim,
+                occupied_roots=occ_roots, timers=timers)
+        else:
+            sol = yield from davidson_steps(
+                ham.diagonal, nroots or system.nbnd, initial_vectors=vectors, tolerance=tol,
+                max_iterations=20,
+                subspace_multiplier=system.diago_david_ndim, residual_factor=None,
+                residual_energy_scale=None, occupied_roots=occ_roots, initial_is_ritz=is_ritz,
+                initial_is_orthonormal=True, initial_eigenvalues=eigs, initial_applied=applied,
+                timers=timers, dtype=ham.dtype, lock_converged=lock)
         attempt += 1
         total_its += sol.iterations
         if sol.converged or sol.number_unconverged <= 5 or attempt >= 6:
@@ -459,21 +541,37 @@ def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, to
         vectors, eigs, applied = sol.eigenvectors, sol.eigenvalues, None
 
 
-def _drive(steps, ham):
-    """Run a generator of H applications with one Hamiltonian."""
+def _drive(steps, ham, ham32=None):
+    """Run a generator of H applications with one Hamiltonian (complex64
+    requests go to ``ham32`` when given: the refined Davidson's FP32
+    corrections)."""
     try:
         request = next(steps)
         while True:
-            ham.apply_into(*request)
+            target = ham32 if ham32 is not None and request[0].dtype == torch.complex64 else ham
+            target.apply_into(*request)
             request = steps.send(None)
     except StopIteration as done:
         return done.value
 
 
+def _apply_by_dtype(hams, hams32, requests) -> None:
+    """Batched H applications of a lockstep round: complex128 requests with
+    ``hams`` and complex64 ones with ``hams32`` (when given), each group in
+    one launch per FFT pass."""
+    groups: dict = {}
+    for request in requests:
+        groups.setdefault(request[1].dtype, []).append(request)
+    for dtype, group in groups.items():
+        table = hams32 if hams32 is not None and dtype == torch.complex64 else hams
+        apply_hamiltonians(table, group)
+
+
 def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             progress=None, timers=None, pools=None, fp32_floor: float = 5.0e-7,
             batch_kpoints: bool | None = None, lock_converged: bool | None = None,
-            guard_bands: int | None = None, restart_mixer_at_switch: bool = False) -> SCFResult:
+            guard_bands: int | None = None, restart_mixer_at_switch: bool = False,
+            fp64_phase: str = "refined", eigenvalue_change_ry: float = 1.0e-6) -> SCFResult:
     """Converge the Kohn-Sham density to ``system.conv_thr`` (Ry) on the GPU.
 
     ``timers``: optional object with a ``measure(name)`` context manager,
@@ -492,7 +590,14 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
 
     Mixed form: ``fp32_floor`` (Ha) bounds the Davidson threshold of the
     FP32 iterations from below; ``restart_mixer_at_switch`` drops the
-    Broyden history when H|psi> turns FP64.  Measured on the 216-atom Gamma
+    Broyden history when H|psi> turns FP64.  ``fp64_phase`` picks the
+    iterations after the switch: 'refined' (default) solves with
+    ``refined_davidson_steps`` (FP64 Ritz block, chosen-form H and GEMMs
+    for the corrections) and accepts convergence once 2 dr2 < conv_thr in a
+    refined iteration whose eigenvalues moved less than
+    ``eigenvalue_change_ry`` from the previous iteration's; 'f64' runs the
+    plain FP64 Davidson there and accepts convergence after
+    MIN_FP64_ITERATIONS such iterations.  Measured on the 216-atom Gamma
     cell and the 64-atom 4-k cell (SCF to 1e-8 Ry): a 5e-7 Ha floor with
     the history kept took 19 and 13 iterations (6.7 s, 4.0 s) where a
     2e-6 Ha floor with the restart took 20 and 17 (8.2-8.7 s, 4.6 s); the
@@ -516,6 +621,8 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     guard_bands = max(0, int(guard_bands))
     if precision not in ("f64", "mixed"):
         raise ValueError("precision must be 'f64' or 'mixed'")
+    if fp64_phase not in ("refined", "f64"):
+        raise ValueError("fp64_phase must be 'refined' or 'f64'")
     device = require_cuda()
     started = time.perf_counter()
     timings: dict[str, float] = {}
@@ -524,7 +631,6 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         timings[name] = timings.get(name, 0.0) + time.perf_counter() - t0
 
     t0 = time.perf_counter()
-    reciprocal = system.reciprocal
     volume = system.volume
     nelec = system.nelec
     occupied = int(round(nelec / 2.0))
@@ -538,27 +644,16 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     elif system.nbnd < occupied:
         raise ValueError("nbnd is smaller than the number of occupied states")
     fermi = None
-    bases = make_bases(reciprocal, system.kpoints, system.ecutwfc)
+    setup = scf_setup(system, device)
+    bases, shape, grid, cgrid = setup.bases, setup.shape, setup.grid, setup.cgrid
+    tables, v_ion, v_ion_average = setup.tables, setup.v_ion, setup.v_ion_average
     if min(len(b) for b in bases) < system.nbnd:
         raise ValueError("nbnd exceeds the smallest plane-wave basis")
     nsolve = min(system.nbnd + guard_bands, min(len(b) for b in bases))
-    shape = fft_shape(bases, reciprocal, system.ecutrho, fft_factors(system.operations))
-    grid = ChargeGrid(shape, reciprocal, system.ecutrho)
-    tables = {label: SpeciesTables(p, volume) for label, p in system.pseudos.items()}
-    q = np.sqrt(grid.g2)
-    v_ion_g = np.zeros(len(grid.g2), dtype=np.complex128)
-    for label, table in tables.items():
-        pos = np.array([p for p, l in zip(system.positions, system.labels) if l == label])
-        structure = gpu_structure_factor(grid.vectors, pos, np.ones(len(pos)))
-        v_ion_g += table.vloc(q) * structure
-    cgrid = DeviceChargeGrid(grid, device)
-    v_ion = cgrid.to_r(torch.from_numpy(v_ion_g).to(device))
-    v_ion_average = float(np.real(np.sum(v_ion_g[grid.g2 < 1.0e-14])))
     charges = np.array([system.pseudos[l].z_valence for l in system.labels])
     e_ion = ewald_energy(system.lattice, system.positions, charges, system.ecutrho,
                          structure=gpu_structure_factor)
-    # uniform starting density (no PP_RHOATOM): rho(G=0) = nelec / Omega
-    rho = torch.full(shape, nelec / volume, dtype=torch.float64, device=device)
+    rho = starting_density(system, setup)
     symmetrizer = DensitySymmetrizer(system.operations, shape) if len(system.operations) > 1 else None
     mixer = (DeviceLinearMixer(system.mixing_beta) if system.mixing_mode == "linear"
              else DeviceBroydenMixer(cgrid, system.mixing_beta, system.mixing_ndim,
@@ -573,6 +668,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     first_diagonalization = True
     input_hxc = None
     energies, accuracies, precision_log, david_its = [], [], [], []
+    previous_eigenvalues = None
     energy_terms: dict[str, float] = {}
     total = 0.0
     converged = False
@@ -583,9 +679,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     while iteration <= system.maxiter:
         t0 = time.perf_counter()
         if input_hxc is None:
-            vh = cgrid.to_r(cgrid.hartree(cgrid.to_g(rho)))
-            _eps, vxc = device_pz81(rho)
-            input_hxc = vh + vxc
+            input_hxc = hxc_potential(setup, rho)
         v_dev = v_ion + input_hxc
         if iteration > 1 and np.isfinite(previous_accuracy):
             if iteration == 2:
@@ -600,19 +694,20 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             # otherwise (their fixed point differs from the FP64 one by less
             # than the residual at the switch, and keeping them saved
             # iterations on both benchmark cells).
-            current_precision = "f64"
+            current_precision = fp64_phase
             if restart_mixer_at_switch and isinstance(mixer, DeviceBroydenMixer):
                 mixer.reset()
             davidson_tolerance = max(5.0e-14, 0.1 * previous_accuracy / max(1.0, nelec))
         # FP32 eigenvalues stall near 1e-7 relative: never ask more of them
         # than ``fp32_floor`` (Ha)
-        tol = davidson_tolerance if current_precision == "f64" else max(davidson_tolerance, fp32_floor)
+        tol = davidson_tolerance if current_precision != "f32" else max(davidson_tolerance, fp32_floor)
+        refined = current_precision == "refined"
         precision_log.append(current_precision)
         tick("v_of_rho", t0)
         t0 = time.perf_counter()
         local_eigenvalues = {}
         its = []
-        hams, solves = {}, {}
+        hams, hams32, solves = {}, {}, {}
         for k, state in enumerate(states):
             if k not in local_k:
                 if state.vectors is None and iteration == 1 and not random_drawn[k]:
@@ -620,15 +715,21 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
                     rng.pairs(len(state.basis), nsolve)
                     random_drawn[k] = True
                 continue
-            ws = state.workspace(current_precision)
             if state.terms is None:
                 state.terms = projector_terms(system, tables, state.basis)
-            ham = PlaneWaveHamiltonian(state.basis, None, state.terms, local_workspace=ws,
-                                       real_potential=v_dev, potential_average=v_ion_average,
-                                       timers=timers,
-                                       device_projectors=state.device_projectors.get(
-                                           current_precision))
-            state.device_projectors[current_precision] = ham.projectors
+
+            def hamiltonian(form):
+                made = PlaneWaveHamiltonian(state.basis, None, state.terms,
+                                            local_workspace=state.workspace(form),
+                                            real_potential=v_dev,
+                                            potential_average=v_ion_average, timers=timers,
+                                            device_projectors=state.device_projectors.get(form))
+                state.device_projectors[form] = made.projectors
+                return made
+
+            ham = hamiltonian("f64" if refined else current_precision)
+            if refined:
+                hams32[k] = hamiltonian("f32")
             initial_applied = None
             initial_eigs = None
             if state.vectors is None:
@@ -645,16 +746,17 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             hams[k] = ham
             solves[k] = _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied,
                                        tol, occ_roots, iteration == 1, timers,
-                                       lock=lock_converged, nroots=nsolve)
+                                       lock=lock_converged, nroots=nsolve, refined=refined)
         k_order = sorted(solves)
         if batch_kpoints and len(k_order) > 1:
             # chosen form: the k points' Davidson solves advance together and
             # each round's H applications share one launch per FFT pass
+            table = [hams[k] for k in k_order]
+            table32 = [hams32[k] for k in k_order] if refined else None
             outcomes = run_lockstep([solves[k] for k in k_order],
-                                    lambda requests: apply_hamiltonians(
-                                        [hams[k] for k in k_order], requests))
+                                    lambda requests: _apply_by_dtype(table, table32, requests))
         else:
-            outcomes = [_drive(solves[k], hams[k]) for k in k_order]
+            outcomes = [_drive(solves[k], hams[k], hams32.get(k)) for k in k_order]
         for k, (sol, total_its) in zip(k_order, outcomes):
             state = states[k]
             its.append(total_its)
@@ -715,8 +817,16 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         # which mixing removes only a factor (1 - beta) per iteration, while
         # V_xc passes it on to the eigenvalues.
         fp64_done = sum(1 for p in precision_log if p == "f64")
-        converged = 2.0 * accuracy < system.conv_thr and current_precision == "f64" and \
-            (precision == "f64" or fp64_done >= MIN_FP64_ITERATIONS)
+        if current_precision == "refined":
+            # measured criterion: the eigenvalues of this FP64-accurate
+            # iteration moved less than eigenvalue_change_ry from the last
+            change = max(float(np.max(np.abs(a - b))) for a, b in
+                         zip(eigenvalues, previous_eigenvalues)) if previous_eigenvalues else np.inf
+            converged = 2.0 * accuracy < system.conv_thr and 2.0 * change < eigenvalue_change_ry
+        else:
+            converged = 2.0 * accuracy < system.conv_thr and current_precision == "f64" and \
+                (precision == "f64" or fp64_done >= MIN_FP64_ITERATIONS)
+        previous_eigenvalues = [np.array(e, copy=True) for e in eigenvalues]
         if converged:
             rho_energy = rho_out
         elif isinstance(mixer, DeviceBroydenMixer):
@@ -758,4 +868,5 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     return SCFResult(converged, total, iteration, energies, accuracies,
                      [s.eigenvalues for s in states], energy_terms, rho, forces,
                      time.perf_counter() - started, precision_log, david_its, timings,
-                     [np.asarray(f) for f in band_occ], fermi)
+                     [np.asarray(f) for f in band_occ], fermi, v_dev,
+                     [states[k].vectors for k in local_k])

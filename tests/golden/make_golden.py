@@ -36,7 +36,7 @@ HERE = Path(__file__).resolve().parent
 REPO = HERE.parents[1]
 sys.path.insert(0, str(REPO))
 
-from tests.golden.reference_env import REFERENCE_ROOT, load_reference  # noqa: E402
+from tests.golden.reference_env import SOURCE_ROOT, load_reference  # noqa: E402
 
 
 def sha(array: np.ndarray) -> str:
@@ -332,8 +332,9 @@ def first_iteration(name: str, workdir: Path, filename: str, roots: int) -> None
     its Davidson call site (qepy_pw/pw/scf.py:3510) and then:
       * fingerprints of V_eff(r) and of the preconditioner diagonal,
       * <psi|H|psi> and <w|H|psi> of seeded probe columns,
-      * the lowest ``roots`` eigenvalues by the reference's davidson from a
-        seeded start, converged to 1e-10 Ha (tight, so path independent).
+      * the lowest ``roots`` eigenvalues by the reference's davidson from its
+        default start (unit vectors on the lowest plane waves), converged to
+        1e-9 Ha (tight, so path independent).
     The run stops once every k point's operator is captured; the starting
     subspace and rotate_wfc are skipped (they play no part here)."""
     import qepy_pw.pw.scf as ref_scf
@@ -374,7 +375,7 @@ def first_iteration(name: str, workdir: Path, filename: str, roots: int) -> None
         (ref_scf.davidson, ref_scf._atomic_starting_orbitals,
          ref_scf._rotate_starting_subspace) = saved
     print(f"{name}: captured {len(captured)} operators in {time.perf_counter() - started:.1f} s")
-    record = {"config": name, "roots": roots, "davidson_tolerance_ha": 1.0e-10,
+    record = {"config": name, "roots": roots, "davidson_tolerance_ha": 1.0e-9,
               "probe_seed": 20261203, "probe_columns": 4, "kpoints": []}
     for k, ham in enumerate(captured):
         basis = ham.basis
@@ -386,10 +387,9 @@ def first_iteration(name: str, workdir: Path, filename: str, roots: int) -> None
         quad = psi.conj().T @ hpsi
         cross = probes.conj().T @ hpsi
         t0 = time.perf_counter()
-        start = probe_vectors(len(basis), roots, 20261403 + k, basis.kinetic)
-        solution = davidson(ham.apply, diagonal, roots, initial_vectors=start,
-                            tolerance=1.0e-10, max_iterations=400, subspace_multiplier=4,
-                            residual_factor=None, operator_into=ham.apply_into)
+        solution = davidson(ham.apply, diagonal, roots, tolerance=1.0e-9, max_iterations=300,
+                            subspace_multiplier=4, residual_factor=None,
+                            operator_into=ham.apply_into)
         print(f"  k {k}: npw {len(basis)} davidson {solution.iterations} its "
               f"converged {solution.converged} in {time.perf_counter() - t0:.1f} s; "
               f"lowest {solution.eigenvalues[:3]}")
@@ -460,7 +460,7 @@ def _displace(text: str, atom: int, axis: int, delta: float) -> str:
 
 
 def si_regression() -> None:
-    path = REFERENCE_ROOT / "tests/qe_reference/reference/pw_scf/scf.in.out"
+    path = SOURCE_ROOT / "tests/qe_reference/reference/pw_scf/scf.in.out"
     text = path.read_text()
     energy = float(re.search(r"!\s+total energy\s+=\s+(-?\d+\.\d+)\s+Ry", text).group(1))
     blocks = re.findall(r"k =.*?bands \(ev\):\s*\n\s*\n(.*?)\n\s*\n", text, flags=re.S)
@@ -486,9 +486,9 @@ def main() -> None:
             workdir = Path(tmp)
             for part in args.only.split(","):
                 if part == "first-iteration-dia64":
-                    first_iteration("scf-dia64", workdir, "first_iteration_dia64.json", 32)
+                    first_iteration("scf-dia64", workdir, "first_iteration_dia64.json", 16)
                 elif part == "first-iteration-dia216":
-                    first_iteration("scf-dia216", workdir, "first_iteration_dia216.json", 32)
+                    first_iteration("scf-dia216", workdir, "first_iteration_dia216.json", 16)
                 elif part == "fd-forces":
                     displaced_energies(workdir, "fd_forces_dia8.json",
                                        [(0, 0), (3, 1), (5, 2), (6, 0)], 1.0e-3)

@@ -98,17 +98,17 @@ def test_qe_random_stream_is_deterministic():
     assert np.all((a1 >= 0) & (a1 < 1))
 
 
-@pytest.mark.skipif(not reference_env.reference_available(),
+@pytest.mark.skipif(not (reference_env.reference_available() and reference_env.source_available()),
                     reason="the reference tree is only present in the build container")
 def test_oracle_reproduces_reference_si_regression():
-    from tests.golden.reference_env import REFERENCE_ROOT, load_reference
+    from tests.golden.reference_env import SOURCE_ROOT, load_reference
 
     load_reference()
     from qepy_pw.input import read_pw_input
     from qepy_pw.scf import run_scf
 
     record = json.loads((GOLDEN / "si_regression.json").read_text())
-    upstream = REFERENCE_ROOT / "tests/qe_reference/upstream"
+    upstream = SOURCE_ROOT / "tests/qe_reference/upstream"
     pw = read_pw_input(upstream / "pw_scf" / "scf.in")
     pw.control["pseudo_dir"] = str(upstream / "pseudo")
     pw.control["disk_io"] = "none"
