@@ -105,6 +105,34 @@ def scf_cell_config(name: str) -> dict:
             "mixing_beta": system.mixing_beta, "changes": SCF_CELL_CHANGES.get(name, [])}
 
 
+def fixed_potential_error(name: str, result) -> float:
+    """Max |e_mixed - e_FP64| (Ry) over the nbnd bands of every k point: a
+    plain FP64 Davidson to 1e-10 Ha on the mixed SCF's last potential,
+    started from its eigenvectors."""
+    from qe_python_b200.basis import LocalPotentialWorkspace
+    from qe_python_b200.diagonalization import PlaneWaveHamiltonian, davidson
+    from qe_python_b200.scf import benchmark_system, projector_terms, scf_setup
+
+    system = benchmark_system(name)
+    setup = scf_setup(system, result.potential.device)
+    worst = 0.0
+    for k, basis in enumerate(setup.bases):
+        ws = LocalPotentialWorkspace(basis, setup.shape, precision="f64")
+        ham = PlaneWaveHamiltonian(basis, None, projector_terms(system, setup.tables, basis),
+                                   local_workspace=ws, real_potential=result.potential,
+                                   potential_average=setup.v_ion_average)
+        vectors = result.eigenvectors[k]
+        check = davidson(ham.apply, ham.diagonal, vectors.shape[1], initial_vectors=vectors,
+                         tolerance=1.0e-10, max_iterations=200,
+                         subspace_multiplier=system.diago_david_ndim, residual_factor=None,
+                         occupied_roots=system.nbnd, initial_is_orthonormal=True,
+                         operator_into=ham.apply_into)
+        diff = np.abs(np.asarray(check.eigenvalues)[:system.nbnd]
+                      - np.asarray(result.eigenvalues_ha[k])[:system.nbnd])
+        worst = max(worst, 2.0 * float(np.max(diff)))
+    return worst
+
+
 def scf_times(name: str) -> dict:
     """Wall time of the GPU SCF to conv_thr = 1e-8 Ry, plain FP64 and mixed,
     with the mixed form's energy, eigenvalue and force differences from the
@@ -156,6 +184,14 @@ def scf_times(name: str) -> dict:
     out["max_eigenvalue_difference_ry"] = max(
         float(np.max(np.abs(2.0 * (np.asarray(x) - np.asarray(y)))))
         for x, y in zip(a.eigenvalues_ha, b.eigenvalues_ha))
+    # the same difference between the two FP64 runs (no guard bands / with):
+    # two converged SCFs along different mixing paths, no FP32 arithmetic
+    out["max_eigenvalue_difference_f64_paths_ry"] = max(
+        float(np.max(np.abs(2.0 * (np.asarray(x) - np.asarray(y)))))
+        for x, y in zip(results["f64_guard_bands"].eigenvalues_ha, b.eigenvalues_ha))
+    # the chosen form's arithmetic error alone: its eigenvalues against a
+    # tight plain-FP64 Davidson on its own final potential
+    out["max_eigenvalue_error_at_fixed_potential_ry"] = fixed_potential_error(name, a)
     if a.forces_ha_per_bohr is not None and b.forces_ha_per_bohr is not None:
         out["max_force_difference_ry_per_bohr"] = float(
             np.max(np.abs(2.0 * (a.forces_ha_per_bohr - b.forces_ha_per_bohr))))

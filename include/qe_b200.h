@@ -157,6 +157,30 @@ int qeb_zgemm_static_scratch(int M, int N, int K, const double* alpha, const voi
                              int64_t lda, const void* B, int64_t ldb, const double* beta,
                              void* C, int64_t ldc, void* stream);
 
+/* Species projector columns beta[g + c ldb] = (-i)^l Y_lm(k+G) beta_l(|k+G|)
+ * (complex128, column-major) for npw plane waves: kg is (npw, 3) float64
+ * column-major (k+G in bohr^-1), table is (rows, columns) float64 row-major
+ * with row r at q = r dq; channel c uses table column channel_radial[c],
+ * angular momentum channel_l[c] <= 2 and QE ylmr2 index channel_m[c].
+ * All pointers but the channel arrays (host) are device pointers.
+ * Replaces qe_cubic_interpolate + low_l_real_harmonics +
+ * assemble_low_l_projectors (qepy_pw/_native_fft.pyx:1556-1600, 1603-1661,
+ * 1702-1791) as called by projector_basis (qepy_pw/upf.py:483-556). */
+int qeb_projector_basis(int64_t npw, const void* kg, const void* table, int64_t rows,
+                        int columns, double dq, int channels, const int* channel_radial,
+                        const int* channel_l, const int* channel_m, void* beta, int64_t ldb,
+                        void* stream);
+
+/* density_out[p] = (1/nops) sum_op density_in[op(p)] on an (nx, ny, nz)
+ * C-order float64 grid (device pointers, in != out): op maps grid point
+ * (i0, i1, i2) to ((offsets[3 op + b] + sum_a coefficients[9 op + 3 a + b]
+ * i_a) mod n_b)_b, summed in operation order.  Host arrays offsets (nops x
+ * 3) and coefficients (nops x 3 x 3); nops <= 96.  Replaces
+ * DensitySymmetrizer.apply (qepy_pw/symmetry.py:28-238). */
+int qeb_symmetrize_density(int nx, int ny, int nz, int nops, const int* offsets,
+                           const int* coefficients, const void* density_in, void* density_out,
+                           void* stream);
+
 /* out = D becp for a block-diagonal D (P x P): block k covers rows/columns
  * [start[k], start[k] + size[k]) with its size x size entries row-major at
  * values + offset[k]; row_block[p] is the block of row p.  All arrays are

@@ -46,6 +46,8 @@ SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_zgemm_scratch_bytes", _L, [_I, _I, _I, _I, _I]),
     ("qeb_zgemm", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
     ("qeb_cgemm", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
+    ("qeb_projector_basis", _I, [_L, _P, _P, _L, _I, _D, _I, _P, _P, _P, _P, _L, _P]),
+    ("qeb_symmetrize_density", _I, [_I, _I, _I, _I, _P, _P, _P, _P, _P]),
     ("qeb_zgemm_static_scratch_capacity", _L, []),
     ("qeb_zgemm_static_scratch", _I, [_I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P]),
     ("qeb_block_coupling", _I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _L, _P, _L, _P]),

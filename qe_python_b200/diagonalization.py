@@ -911,40 +911,56 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
 def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
                            tolerance: float = 1.0e-8, max_iterations: int = 20,
                            subspace_multiplier: int = 2, occupied_roots: int | None = None,
-                           timers=None):
-    """Chosen-form Davidson: an FP64 Ritz block with FP32 corrections.
+                           timers=None, initial_state=None, state_out: dict | None = None,
+                           refresh_above: float = 1.0e-3):
+    """Chosen-form Davidson: an FP64 block of vectors with FP32 corrections.
 
     A generator like ``davidson_steps``; it yields ``(vectors, destination)``
     for destination = H vectors, with complex128 vectors when it needs the
-    FP64 Hamiltonian and complex64 vectors for the chosen form's (FP32 FFT
-    passes, split-TF32 projector GEMMs).  Same criteria as the reference's
-    Davidson (qepy_pw/diagonalization.py:527-880): the lowest roots of the
-    reduced problem, converged when |e - e_previous| is below the root's
-    threshold (occupied roots ``tolerance``, the others max(5 tol, 5e-6)),
-    restart when the subspace is full, results as DavidsonResult with
-    complex128 eigenvectors.
+    FP64 Hamiltonian (only to start without ``initial_state``) and complex64
+    vectors for the chosen form's (FP32 FFT passes, split-TF32 projector
+    GEMMs).  Same criteria as the reference's Davidson
+    (qepy_pw/diagonalization.py:527-880): the lowest roots of the reduced
+    problem, converged when |e - e_previous| is below the root's threshold
+    (occupied roots ``tolerance``, the others max(5 tol, 5e-6)), restart when
+    the subspace is full; returns a DavidsonResult with complex128
+    eigenvectors.
 
-    How FP64 accuracy comes out of FP32 work.  The block X (the roots'
-    vectors, complex128) is first made a Ritz block of the FP64 Hamiltonian:
-    one FP64 H application, X^H H X and X^H X in FP64, the FP64 reduced
-    eigensolve and the rotation, so that X^H H X = diag(lam) and X^H X = 1
-    to FP64 round-off and R = H X - X lam is an FP64 residual.  The
-    subspace is then [X, D_1, D_2, ...] with FP32 correction blocks D_j and
-    their chosen-form products H D_j.  Its reduced matrices take
-      * the X-X block as diag(lam) and 1 exactly;
-      * the D-X blocks as S_DX = D^H X32 and H_DX = S_DX lam + D^H R32
-        (X^H H D = (H X)^H D = lam X^H D + R^H D), both from the same
-        FP32-accurate S_DX: an error in S_DX is an exact Rayleigh-Ritz step
-        on [X, D + X dS^H], which spans the same space, so it does not
-        reach the Ritz values;
+    How FP64 accuracy comes out of FP32 work.  The block X (complex128,
+    orthonormal) comes with values lam and R = H X - X lam, so that
+    H X = X lam + R exactly.  R is small once X is near the eigenvectors
+    and is kept in FP32.  The subspace is [X, D_1, D_2, ...] with FP32
+    correction blocks D_j and their chosen-form products H D_j; the reduced
+    matrices take
+      * the X-X block as diag(lam) + X^H R (the second term, small, from an
+        FP32 product) and the overlap as 1;
+      * the D-X blocks as S_DX = D^H X32 and H_DX = S_DX lam + D^H R, both
+        from the same FP32-accurate S_DX: an error in S_DX is an exact
+        Rayleigh-Ritz step on [X, D + X dS^H], which spans the same space,
+        so it does not reach the Ritz values;
       * the D-D blocks from FP32 products, whose errors enter the Ritz
         values through the squared correction coefficients only.
-    The residuals of unconverged roots, sum of X (lam - e) c_X + R c_X +
-    (H D_j - e D_j) c_j, are formed in FP32 from terms that shrink as the
-    roots converge.  At a restart and at the end the vectors X c_X + D c_D
-    are formed with the X part in FP64.  FP64 work per solve: one FP64 H
-    application of the block and four FP64 GEMMs (npw x n x n) at the start
-    and at each restart, one FP64 GEMM at the end."""
+    Residuals of the roots, X (lam - e) c_X + R c_X + (H D_j - e D_j) c_j,
+    are formed in FP32 from terms that shrink as the roots converge; at a
+    restart and at the end the vectors X c_X + D c_D are formed with the X
+    part in FP64 and R of the new block is that residual.  That R carries
+    the FP32 rounding of the H D_j c_j terms, which enters the next X-X
+    block at first order, so it is kept only while every root's correction
+    coefficients |c_D| stay at or below ``refresh_above``; a restart with
+    larger ones redoes the FP64 Rayleigh-Ritz step below, and an end with
+    larger ones leaves no state to carry (the next solve starts with that
+    step).  Near convergence (the SCF's later iterations) the corrections
+    are small, no FP64 Hamiltonian application is needed after the start,
+    and the FP64 work of a restart or of the end is one GEMM (npw x n x n).
+
+    Start: ``initial_state = (lam, R)`` (an FP64 tensor of n values and a
+    complex64 (npw, n) residual) gives H X = X lam + R for ``initial_vectors``
+    X; the SCF carries it from the previous iteration's end, adding
+    (V_new - V_old) X for the change of the local potential.  Without it
+    the start is an FP64 Rayleigh-Ritz step: one FP64 H application of the
+    block, X^H H X and X^H X in FP64, the FP64 reduced eigensolve and the
+    rotation.  ``state_out`` (a dict) receives the final ``lam`` and ``R``
+    under those keys."""
     device = require_cuda()
     diag = to_device_f(diagonal, torch.float64, device).reshape(-1)
     npw = diag.numel()
@@ -979,14 +995,14 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
     x = empty_f(npw, n, torch.complex128, device)
     x.copy_(trial[:, :n])
     del trial
-    hx = empty_f(npw, n, torch.complex128, device)
-    state = {"applications": 0}
+    counts = {"applications": 0}
 
     def ritz_block(vectors):
         """FP64 Rayleigh-Ritz of ``vectors``: returns (X, lam, R) with X the
         Ritz vectors, lam their values and R = H X - X lam."""
+        hx = empty_f(npw, n, torch.complex128, device)
         yield vectors, hx
-        state["applications"] += n
+        counts["applications"] += n
         with _timer(timers, "cegterg:over"):
             a = _hermitize(K.gemm(K.OP_C, vectors, hx))
             s = _hermitize(K.gemm(K.OP_C, vectors, vectors))
@@ -999,10 +1015,14 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
             K.subtract_band_energies(residual, ritz, lam)
         return ritz, lam, residual
 
-    def start_block(ritz, lam, residual):
-        basis32[:, :n].copy_(ritz)
+    def start_block(lam, residual) -> None:
+        """X block of the basis: X32, R, and the X-X blocks of the reduced
+        matrices, diag(lam) + X^H R and 1."""
+        basis32[:, :n].copy_(x)
         applied32[:, :n].copy_(residual)
-        projected[:n, :n] = torch.diag(lam.to(torch.complex128))
+        with _timer(timers, "cegterg:over"):
+            xr = K.gemm(K.OP_C, basis32[:, :n], applied32[:, :n]).to(torch.complex128)
+        projected[:n, :n] = _hermitize(xr) + torch.diag(lam.to(torch.complex128))
         overlap[:n, :n] = eye
 
     def update_projected(first_new: int, active: int, lam_dev) -> None:
@@ -1033,25 +1053,43 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
             K.gemm(K.OP_N, applied32[:, :active], right, out, beta=1.0)
         return out
 
-    def vectors_of(xblock, coefficients, active):
+    def vectors_of(coefficients, active):
         """X c_X (FP64) + D c_D (FP32) of every root."""
         with _timer(timers, "cegterg:last"):
-            c = coefficients[:, :n]
-            out = K.gemm(K.OP_N, xblock, c[:n].T.contiguous().T)
+            out = K.gemm(K.OP_N, x, coefficients[:n].T.contiguous().T)
             if active > n:
-                low = empty_f(active - n, n, f32, device)
-                low.copy_(c[n:active])
+                low = empty_f(active - n, coefficients.shape[1], f32, device)
+                low.copy_(coefficients[n:active])
                 out += K.gemm(K.OP_N, basis32[:, n:active], low).to(torch.complex128)
         return out
 
-    x, lam_dev, r = yield from ritz_block(x)
-    start_block(x, lam_dev, r)
+    def correction_size(coefficients, active) -> float:
+        """Largest norm over the roots of their correction coefficients."""
+        if active <= n:
+            return 0.0
+        return float(torch.linalg.vector_norm(coefficients[n:active], dim=0).max())
+
+    def reduced_solve(active):
+        with _timer(timers, "cdiaghg"):
+            return lowest_generalized_eigh(projected[:active, :active],
+                                           overlap[:active, :active], n)
+
+    if initial_state is None:
+        x, lam_dev, r = yield from ritz_block(x)
+    else:
+        lam_dev = torch.as_tensor(initial_state[0], dtype=torch.float64, device=device)
+        r = initial_state[1]
+        if tuple(r.shape) != (npw, n) or lam_dev.numel() != n:
+            raise ValueError("initial_state does not match the initial block")
+    start_block(lam_dev, r)
+    del r
     active = n
-    values = lam_dev.cpu().numpy()
-    values_dev = lam_dev
-    coefficients = None
-    block = applied32[:, :n]
-    energies = lam_dev
+    # Ritz values and residuals of the starting block (the reference's first
+    # reduced solve, :699-724)
+    values_dev, coefficients = reduced_solve(active)
+    values = values_dev.cpu().numpy()
+    block = composite_residuals(coefficients, values_dev, lam_dev, active)
+    energies = values_dev
     unconverged = np.ones(n, dtype=bool)
     completed = 0
     for iteration in range(1, max_iterations + 1):
@@ -1065,49 +1103,49 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
         keep = np.flatnonzero(norms_host > (1.0e-14 ** 2) * scale) if scale else np.empty(0, int)
         if keep.size == 0:
             break
+        if active + keep.size > maximum_subspace:
+            # restart on the current Ritz vectors (:843-868): X c_X + D c_D
+            # in FP64 for the X part, R the FP32 residual of every root, or
+            # a fresh FP64 Rayleigh-Ritz step while corrections are large
+            x_new = vectors_of(coefficients, active)
+            if correction_size(coefficients, active) > refresh_above:
+                x, lam_dev, r = yield from ritz_block(x_new)
+            else:
+                r = composite_residuals(coefficients, values_dev, lam_dev, active)
+                x, lam_dev = x_new, values_dev
+            start_block(lam_dev, r)
+            del r, x_new
+            active = n
+            coefficients = torch.eye(n, dtype=torch.complex128, device=device)
         old = active
         active += keep.size
         selected = torch.as_tensor(keep.astype(np.int64), device=device)
         K.normalize_columns(corrections, norms2, selected, basis32[:, old:active])
         del corrections, block
         yield basis32[:, old:active], applied32[:, old:active]
-        state["applications"] += keep.size
+        counts["applications"] += keep.size
         update_projected(old, active, lam_dev)
-        with _timer(timers, "cdiaghg"):
-            roots, coefficients = lowest_generalized_eigh(
-                projected[:active, :active], overlap[:active, :active], n)
-        values_dev = roots
-        values = roots.cpu().numpy()
+        values_dev, coefficients = reduced_solve(active)
+        values = values_dev.cpu().numpy()
         converged = np.abs(values - previous) < root_tolerances
         unconverged = ~converged
         count = int(np.count_nonzero(unconverged))
         if count == 0:
             break
         index = torch.as_tensor(np.flatnonzero(unconverged), device=device)
-        if active + count > maximum_subspace:
-            # restart on the Ritz vectors, made exact again in FP64
-            x = vectors_of(x, coefficients, active)
-            x, lam_dev, r = yield from ritz_block(x)
-            start_block(x, lam_dev, r)
-            active = n
-            coefficients = None
-            block = _select_columns(applied32[:, :n], index).T.contiguous().T
-            energies = lam_dev.index_select(0, index)
-            continue
         energies = values_dev.index_select(0, index)
         block = composite_residuals(coefficients.index_select(1, index), energies, lam_dev,
                                     active)
-    if coefficients is None:
-        vectors, final_values = x, lam_dev.cpu().numpy()
-        norms = np.sqrt(np.maximum(K.column_squared_norms(r).cpu().numpy(), 0.0))
-    else:
-        vectors = vectors_of(x, coefficients, active)
-        final_values = values
-        residual = composite_residuals(coefficients, values_dev, lam_dev, active)
-        norms = np.sqrt(np.maximum(K.column_squared_norms(residual).cpu().numpy(), 0.0))
+    vectors = vectors_of(coefficients, active)
+    residual = composite_residuals(coefficients, values_dev, lam_dev, active)
+    norms = np.sqrt(np.maximum(K.column_squared_norms(residual).cpu().numpy(), 0.0))
+    if state_out is not None:
+        carry = correction_size(coefficients, active) <= refresh_above
+        state_out["lam"] = values_dev
+        state_out["residual"] = residual if carry else None
     count = int(np.count_nonzero(unconverged))
-    return DavidsonResult(final_values, vectors, norms, completed, count == 0, count,
-                          state["applications"])
+    return DavidsonResult(values, vectors, norms, completed, count == 0, count,
+                          counts["applications"])
 
 
 def _select_columns(matrix: torch.Tensor, index: torch.Tensor) -> torch.Tensor:

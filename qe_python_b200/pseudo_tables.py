@@ -199,6 +199,47 @@ class SpeciesTables:
         return beta, coupling
 
 
+def channel_list(angular_momenta) -> list[tuple[int, int, int]]:
+    """(radial column, l, m) of every projector channel in QE's order."""
+    return [(index, l, m) for index, l in enumerate(angular_momenta) for m in range(2 * l + 1)]
+
+
+def device_projectors(tables: "SpeciesTables", kg) -> tuple:
+    """``SpeciesTables.projectors`` on the GPU: the radial table (host, once
+    per species and cell) interpolated and combined with the real harmonics
+    by qeb_projector_basis for every plane wave.  ``kg`` is the (npw, 3)
+    k+G array (host or device); returns (beta, coupling) with beta a
+    column-major complex128 CUDA tensor."""
+    from . import _lib
+    from .device import empty_f, leading_dimension, require_cuda, stream_handle
+
+    device = require_cuda()
+    p = tables.pseudo
+    if any(l > 2 for l in p.angular_momenta):
+        raise ValueError("only l <= 2 projectors are supported")
+    kg_dev = kg if isinstance(kg, torch.Tensor) else torch.from_numpy(np.asarray(kg, dtype=float))
+    kg_dev = kg_dev.to(device=device, dtype=torch.float64)
+    npw = kg_dev.shape[0]
+    kg_cols = kg_dev.T.contiguous()  # (3, npw): column-major (npw, 3)
+    qmax = float(torch.sqrt((kg_dev * kg_dev).sum(dim=1)).max()) if npw else 0.0
+    table = torch.from_numpy(np.ascontiguousarray(tables._beta_table(qmax))).to(device)
+    channels = channel_list(p.angular_momenta)
+    radial = np.array([c[0] for c in channels], dtype=np.int32)
+    ls = np.array([c[1] for c in channels], dtype=np.int32)
+    ms = np.array([c[2] for c in channels], dtype=np.int32)
+    beta = empty_f(npw, len(channels), torch.complex128, device)
+    _lib.check("qeb_projector_basis", _lib.load().qeb_projector_basis(
+        npw, kg_cols.data_ptr(), table.data_ptr(), table.shape[0], table.shape[1], DQ,
+        len(channels), radial.ctypes.data, ls.ctypes.data, ms.ctypes.data, beta.data_ptr(),
+        leading_dimension(beta), stream_handle()))
+    coupling = np.zeros((len(channels), len(channels)))
+    for i, (ri, li, mi) in enumerate(channels):
+        for j, (rj, lj, mj) in enumerate(channels):
+            if li == lj and mi == mj:
+                coupling[i, j] = 0.5 * p.dij_ry[ri, rj]
+    return beta, coupling
+
+
 def structure_factor(vectors: np.ndarray, positions: np.ndarray, weights: np.ndarray) -> np.ndarray:
     """S(G) = sum_a w_a exp(-i G.tau_a), chunked over atoms (host)."""
     out = np.zeros(len(vectors), dtype=np.complex128)

@@ -47,7 +47,7 @@ from .pseudo import SyntheticPseudo, synthetic_pseudo
 from .charge import DeviceBroydenMixer, DeviceChargeGrid, DeviceLinearMixer
 from .charge import pz81 as device_pz81
 from .occupations import fixed_occupations, smeared_occupations, smearing_order
-from .pseudo_tables import SpeciesTables, ewald_energy, pz81
+from .pseudo_tables import SpeciesTables, device_projectors, ewald_energy, pz81
 from .symmetry import (
     DensitySymmetrizer,
     Operation,
@@ -355,6 +355,8 @@ class KPointState:
         self.terms = None
         # projector operands on the device per precision (fixed ions)
         self.device_projectors: dict = {}
+        # refined Davidson: (lam, R, V) with H(V) X = X lam + R for X = vectors
+        self.refined = None
 
     def workspace(self, precision: str) -> LocalPotentialWorkspace:
         if precision not in self.workspaces:
@@ -421,18 +423,15 @@ def projector_terms(system: System, tables: dict, basis) -> tuple:
         pos = np.array([p for p, l in zip(system.positions, system.labels) if l == label])
         if not len(pos) or table.channels == 0:
             continue
-        beta, coupling = table.projectors(vectors)
-        if torch.cuda.is_available():
-            # exp(-i (k+G).tau) for every atom, formed on the device
-            device = torch.device("cuda", torch.cuda.current_device())
-            angle = torch.from_numpy(np.ascontiguousarray(vectors)).to(device) @ \
-                torch.from_numpy(np.ascontiguousarray(pos.T)).to(device)
-            phases = to_device_f(torch.polar(torch.ones_like(angle), -angle), torch.complex128,
-                                 device)
-            del angle
-        else:
-            angle = vectors @ pos.T
-            phases = np.asfortranarray(np.cos(angle) - 1j * np.sin(angle))
+        # init_us_2 on the device: radial interpolation, Y_lm and (-i)^l
+        # (qeb_projector_basis), then exp(-i (k+G).tau) for every atom
+        device = require_cuda()
+        vectors_dev = torch.from_numpy(np.ascontiguousarray(vectors)).to(device)
+        beta, coupling = device_projectors(table, vectors_dev)
+        angle = vectors_dev @ torch.from_numpy(np.ascontiguousarray(pos.T)).to(device)
+        phases = to_device_f(torch.polar(torch.ones_like(angle), -angle), torch.complex128,
+                             device)
+        del angle, vectors_dev
         terms.append(FactorizedProjectorTerm(beta, phases, coupling))
     return tuple(terms)
 
@@ -511,21 +510,27 @@ MIXED_GUARD_BANDS = 24  # mixed form: extra Davidson roots beyond nbnd (run_scf 
 
 
 def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, tol, occ_roots,
-                   is_ritz, timers, lock=False, nroots=None, refined=False):
+                   is_ritz, timers, lock=False, nroots=None, refined=False, carried=None):
     """One k point's diagonalisation as a generator of H applications: the
     Davidson of qepy_pw/pw/scf.py:3496-3556 (20 iterations), repeated up to
     five more times from its last vectors while more than five roots remain
     unconverged.  ``refined``: the chosen form's FP64-accurate Davidson
-    (``refined_davidson_steps``: FP64 Ritz block, FP32 corrections).
-    Returns (DavidsonResult, Davidson iterations)."""
+    (``refined_davidson_steps``: FP64 block, FP32 corrections), started
+    from ``carried`` = (lam, R) when given; the final (lam, R) are left in
+    ``carried_out``.  Returns (DavidsonResult, Davidson iterations,
+    carried_out)."""
     attempt, total_its = 0, 0.0
     vectors, eigs, applied = start_vectors, initial_eigs, initial_applied
+    carried_out: dict = {}
     while True:
         if refined:
             sol = yield from refined_davidson_steps(
                 ham.diagonal, nroots or system.nbnd, initial_vectors=vectors, tolerance=tol,
                 max_iterations=20, subspace_multiplier=system.diago_david_ndim,
-                occupied_roots=occ_roots, timers=timers)
+                occupied_roots=occ_roots, timers=timers, initial_state=carried,
+                state_out=carried_out)
+            carried = (None if carried_out["residual"] is None
+                       else (carried_out["lam"], carried_out["residual"]))
         else:
             sol = yield from davidson_steps(
                 ham.diagonal, nroots or system.nbnd, initial_vectors=vectors, tolerance=tol,
@@ -537,7 +542,7 @@ def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, to
         attempt += 1
         total_its += sol.iterations
         if sol.converged or sol.number_unconverged <= 5 or attempt >= 6:
-            return sol, total_its
+            return sol, total_its, carried_out
         vectors, eigs, applied = sol.eigenvectors, sol.eigenvalues, None
 
 
@@ -728,8 +733,19 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
                 return made
 
             ham = hamiltonian("f64" if refined else current_precision)
+            carried = None
             if refined:
                 hams32[k] = hamiltonian("f32")
+                if state.refined is not None and state.vectors is not None and \
+                        state.vectors.shape[1] == nsolve:
+                    # H X = X lam + R for the previous potential; the new one
+                    # adds (V_new - V_old) X, an FP32 local apply of the
+                    # (small) potential change
+                    lam_prev, r_prev, v_prev = state.refined
+                    x32 = to_device_f(state.vectors, torch.complex64, device)
+                    dvx = hams32[k].local_workspace.apply(v_dev - v_prev, x32)
+                    carried = (lam_prev, r_prev + dvx)
+                    del x32, dvx
             initial_applied = None
             initial_eigs = None
             if state.vectors is None:
@@ -746,7 +762,8 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             hams[k] = ham
             solves[k] = _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied,
                                        tol, occ_roots, iteration == 1, timers,
-                                       lock=lock_converged, nroots=nsolve, refined=refined)
+                                       lock=lock_converged, nroots=nsolve, refined=refined,
+                                       carried=carried)
         k_order = sorted(solves)
         if batch_kpoints and len(k_order) > 1:
             # chosen form: the k points' Davidson solves advance together and
@@ -757,10 +774,12 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
                                     lambda requests: _apply_by_dtype(table, table32, requests))
         else:
             outcomes = [_drive(solves[k], hams[k], hams32.get(k)) for k in k_order]
-        for k, (sol, total_its) in zip(k_order, outcomes):
+        for k, (sol, total_its, carried_out) in zip(k_order, outcomes):
             state = states[k]
             its.append(total_its)
             state.vectors = sol.eigenvectors.to(torch.complex128).T.contiguous().T
+            state.refined = ((carried_out["lam"], carried_out["residual"], v_dev)
+                             if refined and carried_out.get("residual") is not None else None)
             state.eigenvalues = np.asarray(sol.eigenvalues)[:system.nbnd]
             local_eigenvalues[k] = state.eigenvalues
         david_its.append(float(np.mean(its)))
@@ -795,9 +814,9 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             pools.sum_(rho_device)
         rho_out = rho_device * (nelec * grid.size / (float(torch.sum(rho_device)) * volume))
         if symmetrizer is not None:
-            sym = symmetrizer.apply(rho_out.cpu().numpy())
-            sym *= nelec * grid.size / (float(np.sum(sym)) * volume)
-            rho_out = torch.from_numpy(sym).to(device)
+            # on the device (qeb_symmetrize_density), then renormalised
+            sym = symmetrizer.apply_device(rho_out)
+            rho_out = sym * (nelec * grid.size / (float(torch.sum(sym)) * volume))
         band_energy = sum(w * float(np.sum(e * f)) for w, e, f in zip(system.weights, eigenvalues, band_occ))
         scale = volume / grid.size
         deband = -scale * float(torch.sum(rho_out * input_hxc))

@@ -166,14 +166,38 @@ def reduce_kpoints(points: np.ndarray, weights: np.ndarray, ops: list[Operation]
 
 
 class DensitySymmetrizer:
-    """Average a real-space density over the space-group operations."""
+    """Average a real-space density over the space-group operations.
+
+    ``apply`` (host, NumPy) is the CPU restatement; ``apply_device`` runs the
+    same average on the GPU (qeb_symmetrize_density, operations summed in
+    the reference's order: qepy_pw/symmetry.py:178-238)."""
 
     def __init__(self, ops: list[Operation], shape) -> None:
         self.shape = tuple(int(v) for v in shape)
         n = np.array(self.shape)
+        self.operations = list(ops)
+        # integer terms of the transformed coordinates: axis b of op(i) is
+        # (offset_b + sum_a coeff_ab i_a) mod n_b
+        self.offsets = np.zeros((len(ops), 3), dtype=np.int32)
+        self.coefficients = np.zeros((len(ops), 3, 3), dtype=np.int32)
+        for index, op in enumerate(ops):
+            offset = np.asarray(op.translation, dtype=float) * n
+            scaled = np.asarray(op.matrix, dtype=float) * n[None, :] / n[:, None]
+            if np.max(np.abs(offset - np.rint(offset))) > 1.0e-7 or \
+                    np.max(np.abs(scaled - np.rint(scaled))) > 1.0e-7:
+                raise ValueError("operation is not commensurate with the FFT grid")
+            self.offsets[index] = np.rint(offset).astype(np.int32)
+            self.coefficients[index] = np.rint(scaled).astype(np.int32)
+        self.maps = None
+        self.count = len(ops) if len(ops) > 1 else 1
+
+    def _host_maps(self) -> list:
+        if self.maps is not None:
+            return self.maps
+        n = np.array(self.shape)
         grid = np.indices(self.shape).reshape(3, -1).T  # integer grid coordinates
         self.maps = []
-        for op in ops:
+        for op in self.operations:
             if np.array_equal(op.matrix, np.eye(3, dtype=int)) and not np.any(op.translation):
                 continue
             # x = i / n ; x' = x M + t ; i' = n * x'
@@ -184,13 +208,39 @@ class DensitySymmetrizer:
                 raise ValueError("operation is not commensurate with the FFT grid")
             rounded = np.mod(rounded.astype(np.int64), n)
             self.maps.append(np.ravel_multi_index(rounded.T, self.shape))
-        self.count = len(self.maps) + 1
+        return self.maps
 
     def apply(self, density: np.ndarray) -> np.ndarray:
+        """Host restatement: the identity adds the density itself, every
+        other operation its permuted copy, in the operations' order."""
         if self.count == 1:
             return density
-        flat = density.reshape(-1)
-        total = flat.copy()
-        for index in self.maps:
-            total += flat[index]
+        flat = np.asarray(density, dtype=float).reshape(-1)
+        total = np.zeros_like(flat)
+        maps = iter(self._host_maps())
+        for op in self.operations:
+            if np.array_equal(op.matrix, np.eye(3, dtype=int)) and not np.any(op.translation):
+                total += flat
+            else:
+                total += flat[next(maps)]
         return (total / self.count).reshape(self.shape)
+
+    def apply_device(self, density):
+        """The same average of a float64 CUDA tensor (C-order grid) on the GPU."""
+        import torch
+
+        from . import _lib
+        from .device import stream_handle
+
+        if self.count == 1:
+            return density
+        if tuple(density.shape) != self.shape or density.dtype != torch.float64:
+            raise ValueError("density must be a float64 grid of the symmetrizer's shape")
+        source = density.contiguous()
+        out = torch.empty_like(source)
+        offsets = np.ascontiguousarray(self.offsets)
+        coefficients = np.ascontiguousarray(self.coefficients)
+        _lib.check("qeb_symmetrize_density", _lib.load().qeb_symmetrize_density(
+            *self.shape, len(self.operations), offsets.ctypes.data, coefficients.ctypes.data,
+            source.data_ptr(), out.data_ptr(), stream_handle()))
+        return out
