@@ -561,11 +561,15 @@ def apply_local_potential(vg: np.ndarray, indices: np.ndarray, coefficients: np.
 _MULTI_SCRATCH = FFTScratchPool()
 
 
-def apply_local_multi(workspaces, potential: torch.Tensor, vectors, kinetics, targets) -> None:
+def apply_local_multi(workspaces, potential: torch.Tensor, vectors, kinetics, targets,
+                      scratch_pool: FFTScratchPool | None = None) -> None:
     """targets[k] = (T_k + V) vectors[k] for several k points on one grid, one
     launch per FFT pass (qeb_apply_local_multi; at most 16 k points per call,
     more are taken 16 at a time).  ``potential`` is the native (nz, nx, ny)
-    grid in the workspaces' precision; ``kinetics[k]`` may be None."""
+    grid in the workspaces' precision; ``kinetics[k]`` may be None.
+    ``scratch_pool``: the stick scratch (default: one pool shared by all
+    calls; a captured graph passes its own)."""
+    pool = _MULTI_SCRATCH if scratch_pool is None else scratch_pool
     nk_all = len(workspaces)
     if not (len(vectors) == len(kinetics) == len(targets) == nk_all):
         raise ValueError("one vector block, kinetic term and target per workspace")
@@ -579,7 +583,7 @@ def apply_local_multi(workspaces, potential: torch.Tensor, vectors, kinetics, ta
         need = int(lib.qeb_local_multi_scratch_bytes(nk, plans, nbands))
         if need < 0:
             raise ValueError("invalid plans or band counts")
-        scratch = _MULTI_SCRATCH.buffer("sticks", max(need, 256), workspaces[start].device)
+        scratch = pool.buffer("sticks", max(need, 256), workspaces[start].device)
         psi = (ctypes.c_void_p * nk)(*[vectors[k].data_ptr() for k in part])
         ld_psi = (ctypes.c_int64 * nk)(*[leading_dimension(vectors[k]) for k in part])
         kin = (ctypes.c_void_p * nk)(*[0 if kinetics[k] is None else kinetics[k].data_ptr()

@@ -569,10 +569,13 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
         return done.value
 
 
-def apply_hamiltonians(hamiltonians, requests) -> None:
+def apply_hamiltonians(hamiltonians, requests, scratch_pool: FFTScratchPool | None = None,
+                       potential: torch.Tensor | None = None) -> None:
     """destination = H_index vectors for every (index, vectors, destination)
     request: the local parts of all k points in one launch per FFT pass
-    (basis.apply_local_multi), then each k point's projector products."""
+    (basis.apply_local_multi, stick scratch from ``scratch_pool``, the
+    native potential ``potential`` or the first Hamiltonian's), then each
+    k point's projector products."""
     if not requests:
         return
     hams = [hamiltonians[index] for index, _, _ in requests]
@@ -588,11 +591,130 @@ def apply_hamiltonians(hamiltonians, requests) -> None:
     vectors = [to_device_f(v, first.dtype, first.device) for _, v, _ in requests]
     with _timer(first.timers, "h_psi"):
         with _timer(first.timers, "vloc_psi"):
-            apply_local_multi([h.local_workspace for h in hams], first._potential, vectors,
+            apply_local_multi([h.local_workspace for h in hams],
+                              first._potential if potential is None else potential, vectors,
                               [h._kinetic_kernel for h in hams],
-                              [destination for _, _, destination in requests])
+                              [destination for _, _, destination in requests],
+                              scratch_pool=scratch_pool)
         for v, (_, _, destination), ham in zip(vectors, requests, hams):
             ham.add_nonlocal(v, destination)
+
+
+class RoundGraphs:
+    """The H applications of lockstep Davidson rounds as CUDA graphs.
+
+    A round applies each k point's Hamiltonian to its pending block of
+    vectors (``apply_hamiltonians``: one launch per FFT pass for all k
+    points, then each k point's projector GEMMs).  The graph of a round is
+    keyed by every requesting k point's block width rounded up to a bucket
+    (16 up to 16 columns, else a multiple of ``bucket``), so that a few
+    graphs cover all the rounds of an SCF.  A new key runs eagerly once
+    (its results serve the round) and is then captured; later rounds with
+    that key replay it.  Inputs and outputs live in per-k static buffers of
+    the largest width (``max_width``), the local potential in a static
+    buffer that ``set_potential`` refreshes each SCF iteration (the kinetic
+    terms and projectors of the k points do not change).  Padded columns
+    carry stale values whose results are discarded: every operation acts on
+    each column on its own.  Scratch is private and sized for
+    ``max_width`` before the first capture, so that no captured graph ever
+    sees its scratch reallocated: the stick scratch in its own pool, the
+    split-K partial tiles as the scratch of the graphs' own stream."""
+
+    def __init__(self, hamiltonians, max_width: int, bucket: int = 32, max_graphs: int = 48):
+        from . import _lib
+
+        self.hams = list(hamiltonians)
+        self.bucket = int(bucket)
+        self.max_width = -(-int(max_width) // self.bucket) * self.bucket
+        self.max_graphs = int(max_graphs)
+        first = self.hams[0]
+        self.device = first.device
+        self.stream = torch.cuda.Stream(device=self.device)
+        self.pool = FFTScratchPool()
+        self.potential = first._potential.clone()
+        self.inputs = [zeros_f(len(h.basis), self.max_width, h.dtype, self.device)
+                       for h in self.hams]
+        self.outputs = [zeros_f(len(h.basis), self.max_width, h.dtype, self.device)
+                        for h in self.hams]
+        self.graphs: dict = {}
+        self.captures = self.replays = self.eager = 0
+        lib = _lib.load()
+        import ctypes
+
+        for start in range(0, len(self.hams), 16):
+            part = self.hams[start:start + 16]
+            plans = (ctypes.c_void_p * len(part))(*[h.local_workspace._plan.value for h in part])
+            bands = (ctypes.c_int64 * len(part))(*([self.max_width] * len(part)))
+            need = int(lib.qeb_local_multi_scratch_bytes(len(part), plans, bands))
+            self.pool.buffer("sticks", max(need, 256), self.device)
+        need = 0
+        for h in self.hams:
+            p = h.projectors.beta.shape[1] if h.projectors.beta is not None else 0
+            npw = len(h.basis)
+            for width in [16] + list(range(self.bucket, self.max_width + 1, self.bucket)):
+                if p == 0:
+                    continue
+                if h.dtype == torch.complex64:
+                    need = max(need, int(lib.qeb_cgemm_tf32x3_scratch_bytes(K.OP_C, p, width, npw)),
+                               int(lib.qeb_cgemm_tf32x3_scratch_bytes(K.OP_N, npw, width, p)))
+                prec = _lib.QEB_F32 if h.dtype == torch.complex64 else _lib.QEB_F64
+                need = max(need, int(lib.qeb_zgemm_scratch_bytes(K.OP_C, p, width, npw, prec)))
+        with torch.cuda.stream(self.stream):
+            if need > 0:
+                K._SCRATCH.get(need, self.device)
+
+    def set_potential(self, potential: torch.Tensor) -> None:
+        """The local potential of the current SCF iteration (native layout,
+        the Hamiltonians' precision)."""
+        self.potential.copy_(potential)
+
+    def width(self, n: int) -> int:
+        if n <= 16:
+            return 16
+        return min(self.max_width, -(-n // self.bucket) * self.bucket)
+
+    def _requests(self, key):
+        return [(i, self.inputs[i][:, :w], self.outputs[i][:, :w]) for i, w in key]
+
+    def _apply(self, key) -> None:
+        apply_hamiltonians(self.hams, self._requests(key), scratch_pool=self.pool,
+                           potential=self.potential)
+
+    def run_key(self, key) -> None:
+        """H of the static inputs of ``key`` into the static outputs: the
+        graph's replay, or for a new key an eager run and then its capture."""
+        current = torch.cuda.current_stream(self.device)
+        self.stream.wait_stream(current)
+        graph = self.graphs.get(key)
+        with torch.cuda.stream(self.stream):
+            if graph is not None:
+                graph.replay()
+                self.replays += 1
+            else:
+                self._apply(key)
+                self.eager += 1
+        current.wait_stream(self.stream)
+        if graph is None and len(self.graphs) < self.max_graphs:
+            torch.cuda.synchronize(self.device)
+            graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(graph, stream=self.stream):
+                self._apply(key)
+            torch.cuda.synchronize(self.device)
+            self.graphs[key] = graph
+            self.captures += 1
+
+    def __call__(self, requests) -> None:
+        """destination = H_index vectors for every (index, vectors,
+        destination) request, as ``apply_hamiltonians`` computes it."""
+        if any(v.shape[1] > self.max_width or v.dtype != self.hams[i].dtype
+               for i, v, _ in requests):
+            raise ValueError("a request exceeds the graphs' width or precision")
+        key = tuple(sorted((index, self.width(v.shape[1])) for index, v, _ in requests))
+        for index, vectors, _ in requests:
+            self.inputs[index][:, :vectors.shape[1]].copy_(vectors)
+        self.run_key(key)
+        for index, vectors, destination in requests:
+            destination.copy_(self.outputs[index][:, :vectors.shape[1]])
 
 
 def run_lockstep(problems, apply_batch) -> list:

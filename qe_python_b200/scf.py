@@ -42,6 +42,7 @@ from .diagonalization import (
     lowest_generalized_eigh,
     refined_davidson_steps,
     run_lockstep,
+    RoundGraphs,
 )
 from .pseudo import SyntheticPseudo, synthetic_pseudo
 from .charge import DeviceBroydenMixer, DeviceChargeGrid, DeviceLinearMixer
@@ -506,6 +507,7 @@ def starting_hamiltonians(system: System, precision: str = "f64", setup: SCFSetu
 
 
 MIN_FP64_ITERATIONS = 3  # mixed form: FP64 iterations before convergence is accepted
+GRAPH_ROUNDS_DEFAULT = False  # mixed form: batched k-point rounds from CUDA graphs
 MIXED_GUARD_BANDS = 24  # mixed form: extra Davidson roots beyond nbnd (run_scf guard_bands)
 
 
@@ -560,14 +562,18 @@ def _drive(steps, ham, ham32=None):
         return done.value
 
 
-def _apply_by_dtype(hams, hams32, requests) -> None:
+def _apply_by_dtype(hams, hams32, requests, graphs=None) -> None:
     """Batched H applications of a lockstep round: complex128 requests with
     ``hams`` and complex64 ones with ``hams32`` (when given), each group in
-    one launch per FFT pass."""
+    one launch per FFT pass; the complex64 group through ``graphs`` (a
+    RoundGraphs) when given."""
     groups: dict = {}
     for request in requests:
         groups.setdefault(request[1].dtype, []).append(request)
     for dtype, group in groups.items():
+        if graphs is not None and dtype == torch.complex64:
+            graphs(group)
+            continue
         table = hams32 if hams32 is not None and dtype == torch.complex64 else hams
         apply_hamiltonians(table, group)
 
@@ -576,7 +582,8 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             progress=None, timers=None, pools=None, fp32_floor: float = 5.0e-7,
             batch_kpoints: bool | None = None, lock_converged: bool | None = None,
             guard_bands: int | None = None, restart_mixer_at_switch: bool = False,
-            fp64_phase: str = "refined", eigenvalue_change_ry: float = 1.0e-6) -> SCFResult:
+            fp64_phase: str = "refined", eigenvalue_change_ry: float = 1.0e-6,
+            graph_rounds: bool | None = None) -> SCFResult:
     """Converge the Kohn-Sham density to ``system.conv_thr`` (Ry) on the GPU.
 
     ``timers``: optional object with a ``measure(name)`` context manager,
@@ -602,7 +609,10 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     refined iteration whose eigenvalues moved less than
     ``eigenvalue_change_ry`` from the previous iteration's; 'f64' runs the
     plain FP64 Davidson there and accepts convergence after
-    MIN_FP64_ITERATIONS such iterations.  Measured on the 216-atom Gamma
+    MIN_FP64_ITERATIONS such iterations.  ``graph_rounds`` replays the
+    chosen-form H applications of the batched k-point rounds from CUDA
+    graphs (diagonalization.RoundGraphs; off when ``timers`` are given, as
+    their synchronisation cannot be captured).  Measured on the 216-atom Gamma
     cell and the 64-atom 4-k cell (SCF to 1e-8 Ry): a 5e-7 Ha floor with
     the history kept took 19 and 13 iterations (6.7 s, 4.0 s) where a
     2e-6 Ha floor with the restart took 20 and 17 (8.2-8.7 s, 4.6 s); the
@@ -611,6 +621,10 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     on the 216-atom cell."""
     if batch_kpoints is None:
         batch_kpoints = precision == "mixed"
+    if graph_rounds is None:
+        graph_rounds = GRAPH_ROUNDS_DEFAULT and precision == "mixed"
+    graph_rounds = bool(graph_rounds) and timers is None
+    round_graphs = None
     lock_converged = bool(lock_converged)
     # ``guard_bands`` (chosen form): Davidson solves nbnd + guard roots, the
     # guard roots at the loose threshold of empty bands; only the nbnd
@@ -770,8 +784,16 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             # each round's H applications share one launch per FFT pass
             table = [hams[k] for k in k_order]
             table32 = [hams32[k] for k in k_order] if refined else None
+            chosen = table32 if refined else (table if current_precision == "f32" else None)
+            graphs = None
+            if graph_rounds and chosen is not None:
+                if round_graphs is None:
+                    round_graphs = RoundGraphs(chosen, max_width=nsolve)
+                round_graphs.set_potential(chosen[0]._potential)
+                graphs = round_graphs
             outcomes = run_lockstep([solves[k] for k in k_order],
-                                    lambda requests: _apply_by_dtype(table, table32, requests))
+                                    lambda requests: _apply_by_dtype(table, table32, requests,
+                                                                     graphs))
         else:
             outcomes = [_drive(solves[k], hams[k], hams32.get(k)) for k in k_order]
         for k, (sol, total_its, carried_out) in zip(k_order, outcomes):

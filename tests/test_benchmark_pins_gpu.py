@@ -11,8 +11,9 @@
   operators (tests/golden/first_iteration_*.json, made by
   tests/golden/make_golden.py from the reference's run_scf): fingerprints
   of V_eff(r) and of the preconditioner diagonal, <psi|H|psi> and <w|H|psi>
-  of seeded probe columns, and the lowest 12 of 16 eigenvalues of a tight
-  Davidson solve from the reference's default start (1e-9 Ha): the plain
+  of seeded probe columns, and the lowest 12 eigenvalues of a tight Davidson
+  solve (16 roots at 1e-9 Ha for the 64-atom cell, 20 roots at 1e-8 Ha for
+  the 216-atom cell) from the reference's default start: the plain
   FP64 Davidson and the chosen form's refined Davidson within 1e-7 Ry, a
   Davidson wholly in FP32 (the chosen form's early SCF iterations) within
   3e-6 Ry.
@@ -145,7 +146,10 @@ def _first_iteration_case(name, filename, cuda_device):
         # in FP32 stalls near 1e-7 relative in its eigenvalues (the chosen
         # form runs it only in early SCF iterations, above a 5e-7 Ha floor)
         # and is held to 3e-6 Ry
-        compare = roots - 4  # the roots below the last (possibly split) multiplet
+        # the lowest 12: below the last multiplet of the solve and below the
+        # roots whose slow convergence the reference's criterion (a change
+        # under the tolerance between iterations) may have stopped early
+        compare = min(12, roots - 4)
         plain = davidson(ham.apply, ham.diagonal, roots, tolerance=1.0e-9, max_iterations=300,
                          subspace_multiplier=4, residual_factor=None,
                          operator_into=ham.apply_into)
