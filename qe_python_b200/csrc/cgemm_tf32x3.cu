@@ -18,20 +18,13 @@
 // Two-level accumulation: the tensor cores add each MMA's products into the
 // FP32 accumulator with an error that grows with the number of additions
 // (measured: 7e-6 relative after 384 MMAs into one accumulator, 2e-4 after
-// 12 000), so every stage (6 MMAs per accumulator) starts a fresh
-// tensor-memory accumulator (two buffers of Re and Im, 512 columns) and the
-// worker warps add it into FP32 registers with round-to-nearest.  The result
-// is as accurate as an FP32 FMA GEMM.
-//
-// Stages are 8 complex values deep along K (64-byte K-major rows, 64-byte
-// swizzle), so that four of them fit in shared memory: the producer runs
-// up to three stages ahead of the tensor cores, which hides the TMA latency
-// behind the MMAs of the stages in between (with two 16-deep stages the
-// latency of every load was exposed: the tensor pipe was busy ~40 % of the
-// time).
+// 12 000), so each stage's 12 MMAs per accumulator start a fresh tensor-memory
+// accumulator (two buffers of Re and Im, 512 columns) and the worker warps add
+// it into FP32 registers with round-to-nearest.  The result is as accurate
+// as an FP32 FMA GEMM.
 //
 // One CTA = 320 threads computes a 128 x 128 output tile over a K range:
-//   warp 0 lane 0 : TMA producer, four stages
+//   warp 0 lane 0 : TMA producer, two stages
 //   warp 1 lane 0 : MMA issuer; warp 1 owns the tensor-memory allocation
 //   warps 2-9     : workers: split the next stage, drain the previous
 //                   stage's accumulator into registers, then store C
@@ -57,10 +50,9 @@ namespace {
 using namespace qeb::tc;
 
 constexpr int BM = 128, BN = 128;
-constexpr int BKF = 16;      // FP32 words along K per stage (8 complex values)
-constexpr int TILE = 8192;   // bytes of one 128-row x 16-word tile
-constexpr int STAGES = 4;
-constexpr int ROW_BYTES = BKF * 4;  // one K-major tile row: 64 bytes
+constexpr int BKF = 32;      // FP32 words along K per stage (16 complex values)
+constexpr int TILE = 16384;  // bytes of one 128-row x 32-word tile
+constexpr int STAGES = 2;
 constexpr int WORKERS = 8;                 // worker warps (2 .. 9)
 constexpr int WORKER_THREADS = 32 * WORKERS;
 constexpr int THREADS = 64 + WORKER_THREADS;
@@ -69,7 +61,7 @@ constexpr int TMEM_COLS = 2 * ACC_COLS;    // two buffers
 constexpr uint32_t kIdesc = idesc_tf32(BM, BN);
 
 // Tile slots of one stage.  OP_C: 0 A (raw, then hi), 1 A lo, 2 B (raw, then
-// hi), 3 B lo, 4 B1 hi, 5 B1 lo.  OP_N: 0 A raw (8 x 256 words, row-major,
+// hi), 3 B lo, 4 B1 hi, 5 B1 lo.  OP_N: 0 A raw (16 x 256 words, row-major,
 // unswizzled), 1 B (raw, then hi), 2 B lo, 3 A0 hi, 4 A0 lo, 5 A1 hi, 6 A1 lo.
 template <int OP>
 struct Slots {
@@ -101,7 +93,7 @@ __device__ __forceinline__ float4 lo4(float4 v, float4 h) {
 }
 
 // Split one K-major tile in place (hi) with its lo part into another slot.
-// The split is elementwise, so the swizzle needs no attention.
+// The split is elementwise, so the 128-byte swizzle needs no attention.
 __device__ __forceinline__ void split_tile(unsigned char* tile, unsigned char* lo, int ct,
                                            unsigned char* swap_hi, unsigned char* swap_lo) {
   float4* t = reinterpret_cast<float4*>(tile);
@@ -119,22 +111,21 @@ __device__ __forceinline__ void split_tile(unsigned char* tile, unsigned char* l
   }
 }
 
-// OP_N: transpose the raw M-major slab of A (8 K rows x 128 complex) into
+// OP_N: transpose the raw M-major slab of A (16 K rows x 128 complex) into
 // the K-major swizzled tiles A0 = [re, -im] and A1 = [im, re], hi and lo.
-// 64-byte swizzle: the 16-byte chunk c of row m sits at chunk c ^ ((m/2) % 4).
 __device__ __forceinline__ void transpose_a(const unsigned char* raw, unsigned char* a0h,
                                             unsigned char* a0l, unsigned char* a1h,
                                             unsigned char* a1l, int ct) {
   const float2* x = reinterpret_cast<const float2*>(raw);
 #pragma unroll 2
-  for (int it = ct; it < BM * (BKF / 4); it += WORKER_THREADS) {
+  for (int it = ct; it < BM * 8; it += WORKER_THREADS) {
     const int m = it & (BM - 1), kp = it >> 7;  // kp: pair of K values 2kp, 2kp+1
     const float2 x0 = x[(2 * kp) * BM + m];
     const float2 x1 = x[(2 * kp + 1) * BM + m];
     const float4 r0 = make_float4(x0.x, -x0.y, x1.x, -x1.y);
     const float4 r1 = make_float4(x0.y, x0.x, x1.y, x1.x);
     const float4 h0 = hi4(r0), h1 = hi4(r1);
-    const int off = m * ROW_BYTES + ((kp ^ ((m >> 1) & 3)) << 4);
+    const int off = m * 128 + ((kp ^ (m & 7)) << 4);
     *reinterpret_cast<float4*>(a0h + off) = h0;
     *reinterpret_cast<float4*>(a0l + off) = lo4(r0, h0);
     *reinterpret_cast<float4*>(a1h + off) = h1;
@@ -260,14 +251,14 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
         for (int kk = 0; kk < BKF / 8; ++kk) {
           const uint32_t off = kk * 32;  // 8 tf32 words along K
           const uint32_t acc = kk > 0 ? 1u : 0u;
-          const uint64_t arh = smem_desc_sw64(st + S::a_re_hi * TILE + off);
-          const uint64_t arl = smem_desc_sw64(st + S::a_re_lo * TILE + off);
-          const uint64_t aih = smem_desc_sw64(st + S::a_im_hi * TILE + off);
-          const uint64_t ail = smem_desc_sw64(st + S::a_im_lo * TILE + off);
-          const uint64_t brh = smem_desc_sw64(st + S::b_re_hi * TILE + off);
-          const uint64_t brl = smem_desc_sw64(st + S::b_re_lo * TILE + off);
-          const uint64_t bih = smem_desc_sw64(st + S::b_im_hi * TILE + off);
-          const uint64_t bil = smem_desc_sw64(st + S::b_im_lo * TILE + off);
+          const uint64_t arh = smem_desc_sw128(st + S::a_re_hi * TILE + off);
+          const uint64_t arl = smem_desc_sw128(st + S::a_re_lo * TILE + off);
+          const uint64_t aih = smem_desc_sw128(st + S::a_im_hi * TILE + off);
+          const uint64_t ail = smem_desc_sw128(st + S::a_im_lo * TILE + off);
+          const uint64_t brh = smem_desc_sw128(st + S::b_re_hi * TILE + off);
+          const uint64_t brl = smem_desc_sw128(st + S::b_re_lo * TILE + off);
+          const uint64_t bih = smem_desc_sw128(st + S::b_im_hi * TILE + off);
+          const uint64_t bil = smem_desc_sw128(st + S::b_im_lo * TILE + off);
           mma_tf32(t_re, arh, brh, kIdesc, acc);
           mma_tf32(t_re, arh, brl, kIdesc, 1u);
           mma_tf32(t_re, arl, brh, kIdesc, 1u);
@@ -436,7 +427,7 @@ int encode_map(qeb::EncodeTiled enc, CUtensorMap* map, const void* ptr, uint64_t
   const cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(ptr), dims, strides,
                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   swizzle ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                   swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     qeb::set_error("cgemm_tf32x3: cuTensorMapEncodeTiled failed (%d) for %llu x %llu words",

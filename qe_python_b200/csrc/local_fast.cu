@@ -194,28 +194,6 @@ __device__ __forceinline__ void pass_c_body(
   }
 }
 
-// Spacing, in lines, between the rows (or columns) that the line groups of
-// one warp transform at the same time in pass B.  Consecutive rows of the
-// plane start 2 (FP32) or 4 (FP64) banks apart (row stride nx_pad odd), so
-// the groups of one warp reading rows r, r+1, ... pile up on the same banks:
-// for 64-point FP32 lines four groups read 4 x 16 words that cover only
-// 22 banks.  With the rows s apart the groups' words fall on disjoint
-// banks; s comes from a count of bank wavefronts of the row reads, row
-// writes and column reads of every four-step length (s must divide the 8
-// warps of a block).
-template <typename T, class F>
-constexpr int plane_spread() {
-  constexpr int n = F::n;
-  if (sizeof(T) == 4)
-    return (n == 32 || n == 48 || n == 64) ? 4
-           : (n == 96 || n == 128)         ? 8
-           : (n == 16 || n == 36 || n == 90) ? 2
-                                           : 1;
-  return (n == 24 || n == 32 || n == 48) ? 2
-         : (n == 96 || n == 108 || n == 144 || n == 180) ? 4
-                                                           : 1;
-}
-
 // MODE 0: local potential; MODE 1: density accumulation.
 template <typename T, class F, int MODE>
 __device__ __forceinline__ void pass_b_body(
@@ -242,16 +220,9 @@ __device__ __forceinline__ void pass_b_body(
   C2<T>* x = xbuf + g.gid * F::scratch;
   qeb::LaneTwiddles<T, F> lw;
   lw.load(g.lig, tw);
-  // the first row / column of this group: a permutation of the group ids
-  // that puts the groups of one warp plane_spread lines apart
-  constexpr int spread = plane_spread<T, F>();
-  static_assert(kWarps % spread == 0, "the spread must divide the warps of a block");
-  const int warp = threadIdx.x / 32;
-  const int first = (warp / spread) * (spread * F::per_warp) +
-                    (g.gid - warp * F::per_warp) * spread + warp % spread;
   // inverse transforms along x of the active rows (D1 in, D2 out, in place)
   if (g.valid) {
-    for (int r = first; r < nay; r += g.ngroups) {
+    for (int r = g.gid; r < nay; r += g.ngroups) {
       C2<T>* row = plane + r * nx_pad;
       C2<T> v[F::R];
       if (g.lig < F::N2) {
@@ -271,7 +242,7 @@ __device__ __forceinline__ void pass_b_body(
   double w = 0.0;
   if (MODE == 1) w = weights[band];
   if (g.valid) {
-    for (int col = first; col < n; col += g.ngroups) {
+    for (int col = g.gid; col < n; col += g.ngroups) {
       C2<T> v[F::R];
       if (g.lig < F::N2) {
 #pragma unroll
@@ -312,7 +283,7 @@ __device__ __forceinline__ void pass_b_body(
   __syncthreads();
   // forward transforms along x of the active rows (D2 in, D1 out, in place)
   if (g.valid) {
-    for (int r = first; r < nay; r += g.ngroups) {
+    for (int r = g.gid; r < nay; r += g.ngroups) {
       C2<T>* row = plane + r * nx_pad;
       C2<T> v[F::R];
       if (g.lig < F::N1) {

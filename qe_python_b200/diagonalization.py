@@ -570,17 +570,20 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
 
 
 def apply_hamiltonians(hamiltonians, requests, scratch_pool: FFTScratchPool | None = None,
-                       potential: torch.Tensor | None = None) -> None:
+                       potential: torch.Tensor | None = None, always_batched: bool = False) -> None:
     """destination = H_index vectors for every (index, vectors, destination)
     request: the local parts of all k points in one launch per FFT pass
     (basis.apply_local_multi, stick scratch from ``scratch_pool``, the
     native potential ``potential`` or the first Hamiltonian's), then each
-    k point's projector products."""
+    k point's projector products.  A single request goes through the
+    Hamiltonian's own apply unless ``always_batched`` (which a captured
+    graph needs: the batched path alone uses the given scratch and
+    potential, and nothing in it synchronises or times launches)."""
     if not requests:
         return
     hams = [hamiltonians[index] for index, _, _ in requests]
     first = hams[0]
-    batched = len(requests) > 1 and all(
+    batched = (len(requests) > 1 or always_batched) and all(
         h.local_workspace.precision == first.local_workspace.precision and
         h.local_workspace.shape == first.local_workspace.shape and
         h.dtype == first.dtype for h in hams)
@@ -624,6 +627,8 @@ class RoundGraphs:
         from . import _lib
 
         self.hams = list(hamiltonians)
+        if any(h.timers is not None for h in self.hams):
+            raise ValueError("timed Hamiltonians synchronise and cannot be captured")
         self.bucket = int(bucket)
         self.max_width = -(-int(max_width) // self.bucket) * self.bucket
         self.max_graphs = int(max_graphs)
@@ -678,7 +683,7 @@ class RoundGraphs:
 
     def _apply(self, key) -> None:
         apply_hamiltonians(self.hams, self._requests(key), scratch_pool=self.pool,
-                           potential=self.potential)
+                           potential=self.potential, always_batched=True)
 
     def run_key(self, key) -> None:
         """H of the static inputs of ``key`` into the static outputs: the
@@ -1030,11 +1035,20 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
                           completed, False, unconverged_count, applications)
 
 
+# Budget (Ha) of the FP32 rounding that the refined Davidson lets its
+# carried residual R accumulate (over restarts and SCF iterations) before it
+# redoes the FP64 Rayleigh-Ritz step (refined_davidson_steps ``budget``).
+REFINED_ERROR_BUDGET = 1.0e-8
+# relative rounding of an FP32 product-sum (a few units of 2^-24 for the
+# accumulation depths of the residual products)
+_FP32_ROUNDING = 2.4e-7
+
+
 def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
                            tolerance: float = 1.0e-8, max_iterations: int = 20,
                            subspace_multiplier: int = 2, occupied_roots: int | None = None,
                            timers=None, initial_state=None, state_out: dict | None = None,
-                           refresh_above: float = 1.0e-3):
+                           budget: float | None = None):
     """Chosen-form Davidson: an FP64 block of vectors with FP32 corrections.
 
     A generator like ``davidson_steps``; it yields ``(vectors, destination)``
@@ -1066,24 +1080,28 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
     are formed in FP32 from terms that shrink as the roots converge; at a
     restart and at the end the vectors X c_X + D c_D are formed with the X
     part in FP64 and R of the new block is that residual.  That R carries
-    the FP32 rounding of the H D_j c_j terms, which enters the next X-X
-    block at first order, so it is kept only while every root's correction
-    coefficients |c_D| stay at or below ``refresh_above``; a restart with
-    larger ones redoes the FP64 Rayleigh-Ritz step below, and an end with
-    larger ones leaves no state to carry (the next solve starts with that
-    step).  Near convergence (the SCF's later iterations) the corrections
-    are small, no FP64 Hamiltonian application is needed after the start,
-    and the FP64 work of a restart or of the end is one GEMM (npw x n x n).
+    the FP32 rounding of the H D_j c_j terms, about 2.4e-7 (sum_j |c_ji|^2
+    |H D_j|^2)^(1/2) for root i, which enters the next X-X block at first
+    order.  Its running total (carried with the state) may grow to
+    ``budget`` Ha (default REFINED_ERROR_BUDGET, 1e-8); a restart that would
+    exceed it redoes the FP64 Rayleigh-Ritz step below instead, and an end
+    that would exceed it leaves no state to carry (the next solve starts
+    with that step).  Near convergence the corrections are small, no FP64
+    Hamiltonian application is needed after the start, and the FP64 work of
+    a restart or of the end is one GEMM (npw x n x n).
 
-    Start: ``initial_state = (lam, R)`` (an FP64 tensor of n values and a
-    complex64 (npw, n) residual) gives H X = X lam + R for ``initial_vectors``
-    X; the SCF carries it from the previous iteration's end, adding
-    (V_new - V_old) X for the change of the local potential.  Without it
-    the start is an FP64 Rayleigh-Ritz step: one FP64 H application of the
-    block, X^H H X and X^H X in FP64, the FP64 reduced eigensolve and the
-    rotation.  ``state_out`` (a dict) receives the final ``lam`` and ``R``
-    under those keys."""
+    Start: ``initial_state = (lam, R, error)`` (an FP64 tensor of n
+    values, a complex64 (npw, n) residual and the rounding accumulated in
+    it so far, Ha) gives H X = X lam + R for ``initial_vectors`` X; the SCF
+    carries it from the previous iteration's end, adding (V_new - V_old) X
+    for the change of the local potential.  Without it the start is an
+    FP64 Rayleigh-Ritz step: one FP64 H application of the block, X^H H X
+    and X^H X in FP64, the FP64 reduced eigensolve and the rotation.
+    ``state_out`` (a dict) receives the final ``lam``, ``residual`` (None
+    when the budget is spent) and ``error``."""
     device = require_cuda()
+    if budget is None:
+        budget = REFINED_ERROR_BUDGET
     diag = to_device_f(diagonal, torch.float64, device).reshape(-1)
     npw = diag.numel()
     n = int(number_of_roots)
@@ -1185,22 +1203,29 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
                 out += K.gemm(K.OP_N, basis32[:, n:active], low).to(torch.complex128)
         return out
 
-    def correction_size(coefficients, active) -> float:
-        """Largest norm over the roots of their correction coefficients."""
+    hd_norms = torch.zeros(maximum_subspace, dtype=torch.float64, device=device)
+
+    def rounding(coefficients, active) -> float:
+        """Estimate of the FP32 rounding of the H D c_D terms of the roots'
+        residuals: 2.4e-7 max_i (sum_j |c_ji|^2 |H D_j|^2)^(1/2), the
+        rounding errors of the terms adding up as independent ones."""
         if active <= n:
             return 0.0
-        return float(torch.linalg.vector_norm(coefficients[n:active], dim=0).max())
+        weights = coefficients[n:active].abs() * hd_norms[n:active, None]
+        return _FP32_ROUNDING * float(torch.linalg.vector_norm(weights, dim=0).max())
 
     def reduced_solve(active):
         with _timer(timers, "cdiaghg"):
             return lowest_generalized_eigh(projected[:active, :active],
                                            overlap[:active, :active], n)
 
+    error = 0.0  # rounding accumulated in the carried residual (Ha)
     if initial_state is None:
         x, lam_dev, r = yield from ritz_block(x)
     else:
         lam_dev = torch.as_tensor(initial_state[0], dtype=torch.float64, device=device)
         r = initial_state[1]
+        error = float(initial_state[2]) if len(initial_state) > 2 else 0.0
         if tuple(r.shape) != (npw, n) or lam_dev.numel() != n:
             raise ValueError("initial_state does not match the initial block")
     start_block(lam_dev, r)
@@ -1230,11 +1255,14 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
             # in FP64 for the X part, R the FP32 residual of every root, or
             # a fresh FP64 Rayleigh-Ritz step while corrections are large
             x_new = vectors_of(coefficients, active)
-            if correction_size(coefficients, active) > refresh_above:
+            step = rounding(coefficients, active)
+            if error + step > budget:
                 x, lam_dev, r = yield from ritz_block(x_new)
+                error = 0.0
             else:
                 r = composite_residuals(coefficients, values_dev, lam_dev, active)
                 x, lam_dev = x_new, values_dev
+                error += step
             start_block(lam_dev, r)
             del r, x_new
             active = n
@@ -1246,6 +1274,7 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
         del corrections, block
         yield basis32[:, old:active], applied32[:, old:active]
         counts["applications"] += keep.size
+        hd_norms[old:active] = torch.sqrt(K.column_squared_norms(applied32[:, old:active]))
         update_projected(old, active, lam_dev)
         values_dev, coefficients = reduced_solve(active)
         values = values_dev.cpu().numpy()
@@ -1262,9 +1291,10 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
     residual = composite_residuals(coefficients, values_dev, lam_dev, active)
     norms = np.sqrt(np.maximum(K.column_squared_norms(residual).cpu().numpy(), 0.0))
     if state_out is not None:
-        carry = correction_size(coefficients, active) <= refresh_above
+        error += rounding(coefficients, active)
         state_out["lam"] = values_dev
-        state_out["residual"] = residual if carry else None
+        state_out["residual"] = residual if error <= budget else None
+        state_out["error"] = error
     count = int(np.count_nonzero(unconverged))
     return DavidsonResult(values, vectors, norms, completed, count == 0, count,
                           counts["applications"])

@@ -287,7 +287,7 @@ def cgemm_tf32x3(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | 
         splits = 0  # the library's choice: two whole waves, or a split tail wave
     if splits is None:
         default = int(lib.qeb_cgemm_tf32x3_default_splits(op_a, m, n, k))
-        kblocks = (2 * k + 15) // 16  # the library's K stages of 8 complex values
+        kblocks = (2 * k + 31) // 32
         tiles = ((m + 127) // 128) * ((n + 127) // 128)
         if default == 1 and not 148 < tiles < 296:
             # enough output tiles for full waves: the K split stays off

@@ -532,7 +532,7 @@ def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, to
                 occupied_roots=occ_roots, timers=timers, initial_state=carried,
                 state_out=carried_out)
             carried = (None if carried_out["residual"] is None
-                       else (carried_out["lam"], carried_out["residual"]))
+                       else (carried_out["lam"], carried_out["residual"], carried_out["error"]))
         else:
             sol = yield from davidson_steps(
                 ham.diagonal, nroots or system.nbnd, initial_vectors=vectors, tolerance=tol,
@@ -755,10 +755,10 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
                     # H X = X lam + R for the previous potential; the new one
                     # adds (V_new - V_old) X, an FP32 local apply of the
                     # (small) potential change
-                    lam_prev, r_prev, v_prev = state.refined
+                    lam_prev, r_prev, v_prev, error_prev = state.refined
                     x32 = to_device_f(state.vectors, torch.complex64, device)
                     dvx = hams32[k].local_workspace.apply(v_dev - v_prev, x32)
-                    carried = (lam_prev, r_prev + dvx)
+                    carried = (lam_prev, r_prev + dvx, error_prev)
                     del x32, dvx
             initial_applied = None
             initial_eigs = None
@@ -800,7 +800,8 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             state = states[k]
             its.append(total_its)
             state.vectors = sol.eigenvectors.to(torch.complex128).T.contiguous().T
-            state.refined = ((carried_out["lam"], carried_out["residual"], v_dev)
+            state.refined = ((carried_out["lam"], carried_out["residual"], v_dev,
+                              carried_out["error"])
                              if refined and carried_out.get("residual") is not None else None)
             state.eigenvalues = np.asarray(sol.eigenvalues)[:system.nbnd]
             local_eigenvalues[k] = state.eigenvalues
@@ -860,9 +861,14 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         fp64_done = sum(1 for p in precision_log if p == "f64")
         if current_precision == "refined":
             # measured criterion: the eigenvalues of this FP64-accurate
-            # iteration moved less than eigenvalue_change_ry from the last
-            change = max(float(np.max(np.abs(a - b))) for a, b in
-                         zip(eigenvalues, previous_eigenvalues)) if previous_eigenvalues else np.inf
+            # iteration moved less than eigenvalue_change_ry from those of
+            # the previous one, itself refined (the FP32 iterations'
+            # eigenvalues carry their 5e-7 Ha floor)
+            change = np.inf
+            if previous_eigenvalues is not None and len(precision_log) > 1 and \
+                    precision_log[-2] == "refined":
+                change = max(float(np.max(np.abs(a - b)))
+                             for a, b in zip(eigenvalues, previous_eigenvalues))
             converged = 2.0 * accuracy < system.conv_thr and 2.0 * change < eigenvalue_change_ry
         else:
             converged = 2.0 * accuracy < system.conv_thr and current_precision == "f64" and \

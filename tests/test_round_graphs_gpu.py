@@ -7,7 +7,7 @@ Checks: the replay equals the eager round on the same padded blocks bit for
 bit; the rounds' outputs for the requested columns equal the eager rounds
 on the unpadded blocks to FP32 round-off (a 5-column block is padded to 16,
 wider ones to multiples of 32); after a new potential is set the replay
-follows it.
+follows it; a round of a single k point replays the same batched launches.
 """
 
 from __future__ import annotations
@@ -70,3 +70,14 @@ def test_round_graphs_match_eager_rounds(cuda_device):
     for g, e in zip(got, eager):
         assert float((g - e).abs().max()) <= 2e-6 * float(e.abs().max())
     assert graphs.replays == 3
+
+    # a round in which one k point alone is still solving: the same batched
+    # launches, captured with their own key, twice (capture, then replay)
+    for _ in range(2):
+        vector = block(2, 20)
+        got = torch.empty_like(vector.T).T
+        graphs([(2, vector, got)])
+        eager = torch.empty_like(vector.T).T
+        apply_hamiltonians(hams, [(2, vector, eager)], potential=new_v, always_batched=True)
+        assert float((got - eager).abs().max()) <= 2e-6 * float(eager.abs().max())
+    assert graphs.captures == 2 and graphs.replays == 4
