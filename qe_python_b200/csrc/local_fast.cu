@@ -194,6 +194,27 @@ __device__ __forceinline__ void pass_c_body(
   }
 }
 
+// Spacing, in lines, between the rows (or columns) that the line groups of
+// one warp transform at the same time in pass B.  Consecutive rows of the
+// plane start 2 (FP32) or 4 (FP64) banks apart (row stride nx_pad odd).
+// Shared memory serves 8-byte accesses half a warp at a time (16-byte ones
+// a quarter), so for 64-point FP32 lines the two line groups of one half
+// warp, reading rows r and r + 1, hit the same banks: every row read, row
+// write and column read took twice the minimum of wavefronts.  With the
+// groups of a warp 8 rows apart (16 banks) they hit disjoint banks.  s comes
+// from a count of the wavefronts of those accesses for every four-step
+// length, per half (quarter) warp; s divides the 8 warps of a block.
+template <typename T, class F>
+constexpr int plane_spread() {
+  constexpr int n = F::n;
+  if (sizeof(T) == 4)
+    return (n == 32 || n == 48 || n == 64 || n == 96) ? 8
+           : (n == 16 || n == 24 || n == 90)            ? 4
+           : (n == 108 || n == 135)                     ? 2
+                                                        : 1;
+  return (n == 16 || n == 24 || n == 96 || n == 108 || n == 144) ? 4 : 1;
+}
+
 // MODE 0: local potential; MODE 1: density accumulation.
 template <typename T, class F, int MODE>
 __device__ __forceinline__ void pass_b_body(
@@ -220,9 +241,16 @@ __device__ __forceinline__ void pass_b_body(
   C2<T>* x = xbuf + g.gid * F::scratch;
   qeb::LaneTwiddles<T, F> lw;
   lw.load(g.lig, tw);
+  // the first row / column of this group: a permutation of the group ids
+  // that puts the groups of one warp plane_spread lines apart
+  constexpr int spread = plane_spread<T, F>();
+  static_assert(kWarps % spread == 0, "the spread must divide the warps of a block");
+  const int warp = threadIdx.x / 32;
+  const int first = (warp / spread) * (spread * F::per_warp) +
+                    (g.gid - warp * F::per_warp) * spread + warp % spread;
   // inverse transforms along x of the active rows (D1 in, D2 out, in place)
   if (g.valid) {
-    for (int r = g.gid; r < nay; r += g.ngroups) {
+    for (int r = first; r < nay; r += g.ngroups) {
       C2<T>* row = plane + r * nx_pad;
       C2<T> v[F::R];
       if (g.lig < F::N2) {
@@ -242,7 +270,7 @@ __device__ __forceinline__ void pass_b_body(
   double w = 0.0;
   if (MODE == 1) w = weights[band];
   if (g.valid) {
-    for (int col = g.gid; col < n; col += g.ngroups) {
+    for (int col = first; col < n; col += g.ngroups) {
       C2<T> v[F::R];
       if (g.lig < F::N2) {
 #pragma unroll
@@ -283,7 +311,7 @@ __device__ __forceinline__ void pass_b_body(
   __syncthreads();
   // forward transforms along x of the active rows (D2 in, D1 out, in place)
   if (g.valid) {
-    for (int r = g.gid; r < nay; r += g.ngroups) {
+    for (int r = first; r < nay; r += g.ngroups) {
       C2<T>* row = plane + r * nx_pad;
       C2<T> v[F::R];
       if (g.lig < F::N1) {

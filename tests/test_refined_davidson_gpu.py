@@ -2,13 +2,15 @@
 
 * Small cell: ``refined_davidson_steps`` driven with the FP64 and the
   chosen-form (FP32 FFT passes, split-TF32 / FP32 GEMMs) Hamiltonians gives
-  the eigenvalues of dense diagonalisation of the FP64 operator to 1e-9 Ha,
+  the eigenvalues of dense diagonalisation of the FP64 operator within its
+  rounding budget (1e-8 Ha by default; 1e-10 Ha with a 1e-12 budget),
   through restarts (subspace of twice the roots), and FP64 residuals of
   its eigenvectors at the Davidson threshold's level.
 * Benchmark cells (64 atoms, 4 k; 216 atoms, Gamma): the mixed SCF's final
   eigenvalues against a tight plain-FP64 Davidson on the same fixed
   potential (the mixed SCF's last V_eff) from the mixed eigenvectors:
-  every one of the nbnd eigenvalues within 1e-6 Ry.  This is the arithmetic
+  every one of the nbnd eigenvalues within 1e-7 Ry, the plain form's bar
+  (measured 4e-11 Ry; the chosen form's bar is 1e-6 Ry).  This is the arithmetic
   error of the chosen form alone; differences between two separately
   converged SCFs also carry the difference of their mixing paths.
 """
@@ -67,13 +69,17 @@ def test_refined_davidson_matches_dense(cuda_device):
     rng = np.random.default_rng(5)
     start = rng.standard_normal((npw, roots)) + 1j * rng.standard_normal((npw, roots))
     start = np.linalg.qr(start)[0]
-    steps = refined_davidson_steps(ham64.diagonal, roots,
-                                   initial_vectors=to_device_f(start, torch.complex128, cuda_device),
-                                   tolerance=1.0e-11, max_iterations=80, subspace_multiplier=2)
-    result = _drive(steps, ham64, ham32)
-    assert result.converged
-    assert result.eigenvectors.dtype == torch.complex128
-    assert np.max(np.abs(result.eigenvalues - exact[:roots])) < 1.0e-9
+    # the default rounding budget (1e-8 Ha), then a tight one: the FP64
+    # Rayleigh-Ritz step is redone whenever the carried residual's FP32
+    # rounding would pass the budget, which bounds the eigenvalue error
+    for budget, bound in ((None, 1.0e-8), (1.0e-12, 1.0e-10)):
+        steps = refined_davidson_steps(
+            ham64.diagonal, roots, initial_vectors=to_device_f(start, torch.complex128, cuda_device),
+            tolerance=1.0e-11, max_iterations=80, subspace_multiplier=2, budget=budget)
+        result = _drive(steps, ham64, ham32)
+        assert result.converged
+        assert result.eigenvectors.dtype == torch.complex128
+        assert np.max(np.abs(result.eigenvalues - exact[:roots])) < bound, budget
     hx = ham64.apply(result.eigenvectors).cpu().numpy()
     x = result.eigenvectors.cpu().numpy()
     residual = hx - x * result.eigenvalues[None, :]
@@ -110,4 +116,4 @@ def test_mixed_scf_eigenvalues_at_fixed_potential(cuda_device, name):
         diff = 2.0 * np.max(np.abs(np.asarray(check.eigenvalues)[:system.nbnd]
                                    - np.asarray(mixed.eigenvalues_ha[k])[:system.nbnd]))
         worst = max(worst, diff)
-    assert worst <= 1.0e-6, f"{name}: mixed vs FP64 at the same potential {worst:.3e} Ry"
+    assert worst <= 1.0e-7, f"{name}: mixed vs FP64 at the same potential {worst:.3e} Ry"
