@@ -74,8 +74,8 @@ def parse_args():
 
 # DRAM bytes (read + write) of one pass-B launch of the 256-band microbenchmark,
 # from one ncu capture (--set full) of `bench.py --apply-only f32`: 78.8 MB
-# read + 21.8 MB written.
-PASS_B_NCU_TRAFFIC = {("pass_b", 256): 100.64e6}
+# read + 22.7 MB written.
+PASS_B_NCU_TRAFFIC = {("pass_b", 256): 101.51e6}
 
 
 # How the SCF benchmark cells differ from the configurations they stand for:
@@ -686,8 +686,8 @@ def run_b200(args) -> None:
                     "traffic": PASS_B_NCU_TRAFFIC.get((dominant, nb)),
                     "algorithmic_bytes": amount,
                     "peak_source": peaks["source"],
-                    "note": "pass B is bound by the shared-memory data path (ncu: L1/shared "
-                            "pipe 93 % busy), not by HBM"}
+                    "note": "pass B is bound by the shared-memory data path and instruction "
+                            "issue (ncu: L1/TEX 85 %, issue 77 % active), not by HBM"}
         if dominant == "pass_b":
             roofline["fp32_fft_rate"] = plane_fft_rate(work.shape, nb, seconds)
     elif dominant in ("calbec_gemm", "add_gemm") and forms["mixed"][1].tensor_gemm:
