@@ -51,6 +51,13 @@ int64_t qeb_launch_count(void);
 int qeb_qe_random_pairs(int64_t plane_waves, int64_t bands, int64_t* table, int64_t* current,
                         int64_t* seed, double* first, double* second);
 
+/* The same stream as its integer values (each draw times 714025), for a
+ * division on the device (qeb_random_trials); host code, same arguments
+ * and state update as qeb_qe_random_pairs.  Replaces the draw of
+ * qepy_pw/pw/scf.py:855-860 (_QERandom.pairs_by_band, :493-510). */
+int qeb_qe_random_draws(int64_t plane_waves, int64_t bands, int64_t* table, int64_t* current,
+                        int64_t* seed, int32_t* first, int32_t* second);
+
 /* ------------------------------------------------------------------------
  * Local potential operator on the FFT grid (sticks / planes).
  * ---------------------------------------------------------------------- */
@@ -180,6 +187,16 @@ int qeb_projector_basis(int64_t npw, const void* kg, const void* table, int64_t 
 int qeb_symmetrize_density(int nx, int ny, int nz, int nops, const int* offsets,
                            const int* coefficients, const void* density_in, void* density_out,
                            void* stream);
+
+/* Random starting wavefunctions: out[g + b ldo] = amp e^(2 pi i phase) /
+ * (1 + 2 kinetic[g]) with amp = first[g + b npw] / 714025 and phase =
+ * second[g + b npw] / 714025 (IEEE double), stored as complex128, or
+ * complex64 when out_complex64 != 0.  Device arrays: first/second int32
+ * (npw x bands, column-major), kinetic float64 (npw).  Replaces
+ * qepy_pw/pw/scf.py:861-869. */
+int qeb_random_trials(int64_t npw, int64_t bands, const void* first, const void* second,
+                      const void* kinetic, void* out, int64_t ldo, int out_complex64,
+                      void* stream);
 
 /* out = D becp for a block-diagonal D (P x P): block k covers rows/columns
  * [start[k], start[k] + size[k]) with its size x size entries row-major at

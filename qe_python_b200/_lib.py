@@ -34,6 +34,7 @@ SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_version", _I, []),
     ("qeb_launch_count", _L, []),
     ("qeb_qe_random_pairs", _I, [_L, _L, _P, _P, _P, _P, _P]),
+    ("qeb_qe_random_draws", _I, [_L, _L, _P, _P, _P, _P, _P]),
     ("qeb_local_plan_create", _I, [ctypes.POINTER(_P), _I, _I, _I, _L, _P, _I]),
     ("qeb_local_plan_destroy", _I, [_P]),
     ("qeb_local_plan_info", _I, [_P, _P, _I]),
@@ -48,6 +49,7 @@ SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_cgemm", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
     ("qeb_projector_basis", _I, [_L, _P, _P, _L, _I, _D, _I, _P, _P, _P, _P, _L, _P]),
     ("qeb_symmetrize_density", _I, [_I, _I, _I, _I, _P, _P, _P, _P, _P]),
+    ("qeb_random_trials", _I, [_L, _L, _P, _P, _P, _P, _L, _I, _P]),
     ("qeb_zgemm_static_scratch_capacity", _L, []),
     ("qeb_zgemm_static_scratch", _I, [_I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P]),
     ("qeb_block_coupling", _I, [_I, _I, _I, _I, _P, _P, _P, _P, _P, _P, _L, _P, _L, _P]),

@@ -88,3 +88,49 @@ extern "C" int qeb_qe_random_pairs(int64_t plane_waves, int64_t bands, int64_t* 
   *seed = s;
   return QEB_OK;
 }
+
+// The same stream as integers: first/second receive the raw table values
+// (the draws times 714025), so the division happens where the draws are
+// used (on the device, in qeb_random_trials).  Every quantity fits 32 bits
+// (97 x 714024 and 1366 x 714024 + 150889 are below 2^32), so the two
+// dependency chains (the shuffle index and the LCG) run on 32-bit integer
+// arithmetic, and the output is half the bytes of the double pairs.
+extern "C" int qeb_qe_random_draws(int64_t plane_waves, int64_t bands, int64_t* table,
+                                   int64_t* current, int64_t* seed, int32_t* first,
+                                   int32_t* second) {
+  if (plane_waves < 0 || bands < 0 || table == nullptr || current == nullptr ||
+      seed == nullptr || (plane_waves * bands > 0 && (first == nullptr || second == nullptr))) {
+    qeb::set_error("qe_random_draws: invalid arguments");
+    return QEB_EINVAL;
+  }
+  if (*current < 0 || *current >= 714025 || *seed < 0 || *seed >= 714025) {
+    qeb::set_error("qe_random_draws: stream state out of range");
+    return QEB_EINVAL;
+  }
+  uint32_t shuffle[97];
+  for (int i = 0; i < 97; ++i) {
+    if (table[i] < 0 || table[i] >= 714025) {
+      qeb::set_error("qe_random_draws: shuffle table out of range");
+      return QEB_EINVAL;
+    }
+    shuffle[i] = (uint32_t)table[i];
+  }
+  uint32_t cur = (uint32_t)*current, s = (uint32_t)*seed;
+  const int64_t total = plane_waves * bands;
+  for (int64_t out = 0; out < total; ++out) {
+    uint32_t i = (97u * cur) / 714025u;
+    cur = shuffle[i];
+    s = (1366u * s + 150889u) % 714025u;
+    shuffle[i] = s;
+    first[out] = (int32_t)cur;
+    i = (97u * cur) / 714025u;
+    cur = shuffle[i];
+    s = (1366u * s + 150889u) % 714025u;
+    shuffle[i] = s;
+    second[out] = (int32_t)cur;
+  }
+  for (int i = 0; i < 97; ++i) table[i] = shuffle[i];
+  *current = cur;
+  *seed = s;
+  return QEB_OK;
+}

@@ -15,7 +15,14 @@
 // integer offsets and coefficients prepared on the host (the translation
 // times n_b, and M_ab n_b / n_a).  The whole grid (nx ny nz doubles) stays
 // in L2 on the benchmark cells, so the gathers are L2 reads.
+//
+// qeb_random_trials: the random starting wavefunctions of the first SCF
+// iteration, amp e^(2 pi i phase) / (1 + 2 T(k+G)) with T the basis's
+// kinetic table (Ha) and amp, phase the QE randy stream's pairs (qepy_pw/pw/scf.py:853-870), from the stream's
+// integer values (qeb_qe_random_draws): each draw is value / 714025 in
+// IEEE double, as on the host.
 #include <cuda_runtime.h>
+#include <cuComplex.h>
 
 #include "qeb_common.cuh"
 #include "../../include/qe_b200.h"
@@ -126,6 +133,43 @@ __global__ void projector_basis_kernel(int64_t npw, const double* __restrict__ k
   }
 }
 
+template <typename Out>
+__device__ __forceinline__ void store_trial(Out* out, int64_t at, double re, double im);
+
+template <>
+__device__ __forceinline__ void store_trial<double2>(double2* out, int64_t at, double re,
+                                                     double im) {
+  out[at] = make_double2(re, im);
+}
+
+template <>
+__device__ __forceinline__ void store_trial<float2>(float2* out, int64_t at, double re,
+                                                    double im) {
+  out[at] = make_float2((float)re, (float)im);
+}
+
+// One thread per (plane wave, band) entry, plane waves fastest, so the two
+// int32 inputs and the output are read and written coalesced.
+template <typename Out>
+__global__ void random_trials_kernel(int64_t npw, int64_t bands, const int32_t* __restrict__ first,
+                                     const int32_t* __restrict__ second,
+                                     const double* __restrict__ kinetic, Out* __restrict__ out,
+                                     int64_t ldo) {
+  const double two_pi = 6.283185307179586;
+  const int64_t total = npw * bands;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t b = e / npw;
+    const int64_t g = e - b * npw;
+    const double amp = (double)first[e] / 714025.0;
+    const double phase = (double)second[e] / 714025.0;
+    double s, c;
+    sincos(two_pi * phase, &s, &c);
+    const double den = 1.0 + 2.0 * kinetic[g];
+    store_trial(out, g + b * ldo, (amp * c) / den, (amp * s) / den);
+  }
+}
+
 // Grid-stride launches: at most 8 blocks per SM of a 148-SM B200.
 int grid_blocks(int64_t total, int threads) {
   const int64_t want = (total + threads - 1) / threads;
@@ -196,4 +240,28 @@ extern "C" int qeb_projector_basis(int64_t npw, const void* kg, const void* tabl
       1.0 / dq, ch, static_cast<double2*>(beta), ldb);
   qeb::count_launches(1);
   return qeb::cuda_status(cudaGetLastError(), "projector_basis launch");
+}
+
+extern "C" int qeb_random_trials(int64_t npw, int64_t bands, const void* first,
+                                 const void* second, const void* kinetic, void* out, int64_t ldo,
+                                 int out_complex64, void* stream) {
+  if (npw < 0 || bands < 0 || ldo < npw ||
+      (npw * bands > 0 && (first == nullptr || second == nullptr || kinetic == nullptr ||
+                           out == nullptr))) {
+    qeb::set_error("random_trials: invalid arguments");
+    return QEB_EINVAL;
+  }
+  if (npw == 0 || bands == 0) return QEB_OK;
+  const int blocks = grid_blocks(npw * bands, 256);
+  const cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (out_complex64)
+    random_trials_kernel<float2><<<blocks, 256, 0, s>>>(
+        npw, bands, static_cast<const int32_t*>(first), static_cast<const int32_t*>(second),
+        static_cast<const double*>(kinetic), static_cast<float2*>(out), ldo);
+  else
+    random_trials_kernel<double2><<<blocks, 256, 0, s>>>(
+        npw, bands, static_cast<const int32_t*>(first), static_cast<const int32_t*>(second),
+        static_cast<const double*>(kinetic), static_cast<double2*>(out), ldo);
+  qeb::count_launches(1);
+  return qeb::cuda_status(cudaGetLastError(), "random_trials launch");
 }

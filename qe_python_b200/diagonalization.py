@@ -1063,13 +1063,16 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
     eigenvectors.
 
     How FP64 accuracy comes out of FP32 work.  The block X (complex128,
-    orthonormal) comes with values lam and R = H X - X lam, so that
+    near orthonormal) comes with values lam and R = H X - X lam, so that
     H X = X lam + R exactly.  R is small once X is near the eigenvectors
     and is kept in FP32.  The subspace is [X, D_1, D_2, ...] with FP32
     correction blocks D_j and their chosen-form products H D_j; the reduced
     matrices take
-      * the X-X block as diag(lam) + X^H R (the second term, small, from an
-        FP32 product) and the overlap as 1;
+      * the X-X block as S lam + X^H R (the second term, small, from an
+        FP32 product) and the overlap as S = X^H X (1 after an FP64
+        Rayleigh-Ritz step, else an FP64 product: a block formed from the
+        reduced solution is orthonormal only to the FP32 accuracy of the
+        reduced overlap, and that drift would build up over restarts);
       * the D-X blocks as S_DX = D^H X32 and H_DX = S_DX lam + D^H R, both
         from the same FP32-accurate S_DX: an error in S_DX is an exact
         Rayleigh-Ritz step on [X, D + X dS^H], which spans the same space,
@@ -1079,7 +1082,8 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
     Residuals of the roots, X (lam - e) c_X + R c_X + (H D_j - e D_j) c_j,
     are formed in FP32 from terms that shrink as the roots converge; at a
     restart and at the end the vectors X c_X + D c_D are formed with the X
-    part in FP64 and R of the new block is that residual.  That R carries
+    part in FP64 and R of the new block is that residual (with lam = e,
+    H X = X lam + R holds for any X, orthonormal or not).  That R carries
     the FP32 rounding of the H D_j c_j terms, which enters the next X-X
     block x^H R at first order: about 2.4e-7 (sum_j |c_ji|^2 |H D_j|^2)^(1/2)
     / sqrt(npw) for root i, the rounding being independent of the unit
@@ -1092,7 +1096,7 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
     that would exceed it leaves no state to carry (the next solve starts
     with that step).  Near convergence the corrections are small, no FP64
     Hamiltonian application is needed after the start, and the FP64 work of
-    a restart or of the end is one GEMM (npw x n x n).
+    a restart is two GEMMs (npw x n x n: X c_X and X^H X), of the end one.
 
     Start: ``initial_state = (lam, R, error)`` (an FP64 tensor of n
     values, a complex64 (npw, n) residual and the rounding accumulated in
@@ -1159,15 +1163,21 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
             K.subtract_band_energies(residual, ritz, lam)
         return ritz, lam, residual
 
-    def start_block(lam, residual) -> None:
+    def start_block(lam, residual, exact: bool = False) -> None:
         """X block of the basis: X32, R, and the X-X blocks of the reduced
-        matrices, diag(lam) + X^H R and 1."""
+        matrices, S lam + X^H R and S = X^H X.  S is the identity after an
+        FP64 Rayleigh-Ritz step (``exact``); a block formed as X c_X + D c_D
+        is orthonormal only to the FP32 accuracy of the reduced overlap, a
+        drift that would build up over restarts, so S is then an FP64
+        product."""
         basis32[:, :n].copy_(x)
         applied32[:, :n].copy_(residual)
+        lam_c = lam.to(torch.complex128)
         with _timer(timers, "cegterg:over"):
             xr = K.gemm(K.OP_C, basis32[:, :n], applied32[:, :n]).to(torch.complex128)
-        projected[:n, :n] = _hermitize(xr) + torch.diag(lam.to(torch.complex128))
-        overlap[:n, :n] = eye
+            gram = eye if exact else _hermitize(K.gemm(K.OP_C, x, x))
+        projected[:n, :n] = _hermitize(xr + gram * lam_c[None, :])
+        overlap[:n, :n] = gram
 
     def update_projected(first_new: int, active: int, lam_dev) -> None:
         with _timer(timers, "cegterg:over"):
@@ -1227,6 +1237,7 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
                                            overlap[:active, :active], n)
 
     error = 0.0  # rounding accumulated in the carried residual (Ha)
+    exact = initial_state is None
     if initial_state is None:
         x, lam_dev, r = yield from ritz_block(x)
     else:
@@ -1235,7 +1246,7 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
         error = float(initial_state[2]) if len(initial_state) > 2 else 0.0
         if tuple(r.shape) != (npw, n) or lam_dev.numel() != n:
             raise ValueError("initial_state does not match the initial block")
-    start_block(lam_dev, r)
+    start_block(lam_dev, r, exact)
     del r
     active = n
     # Ritz values and residuals of the starting block (the reference's first
@@ -1263,14 +1274,15 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
             # a fresh FP64 Rayleigh-Ritz step while corrections are large
             x_new = vectors_of(coefficients, active)
             step = rounding(coefficients, active)
-            if error + step > budget:
+            exact = error + step > budget
+            if exact:
                 x, lam_dev, r = yield from ritz_block(x_new)
                 error = 0.0
             else:
                 r = composite_residuals(coefficients, values_dev, lam_dev, active)
                 x, lam_dev = x_new, values_dev
                 error += step
-            start_block(lam_dev, r)
+            start_block(lam_dev, r, exact)
             del r, x_new
             active = n
             coefficients = torch.eye(n, dtype=torch.complex128, device=device)

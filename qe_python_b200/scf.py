@@ -22,6 +22,7 @@ Energies are Hartree internally; SCFResult reports both units.
 from __future__ import annotations
 
 import ctypes
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -33,7 +34,7 @@ from . import _lib
 from . import kernels as K
 from .basis import LocalPotentialWorkspace, fft_shape, make_bases
 from .configs import DIAMOND_CUBIC, displacements, supercell
-from .device import empty_f, require_cuda, to_device_f
+from .device import empty_f, leading_dimension, require_cuda, stream_handle, to_device_f
 from .diagonalization import (
     PlaneWaveHamiltonian,
     apply_hamiltonians,
@@ -182,6 +183,61 @@ class QERandom:
             first.ctypes.data, second.ctypes.data))
         self.current, self.seed = int(cur.value), int(seed.value)
         return first, second
+
+    def draws(self, plane_waves: int, bands: int) -> tuple[np.ndarray, np.ndarray]:
+        """The next pairs as the stream's integer values (each draw times
+        714025; int32, column-major): ``pairs`` divided on the device."""
+        first = np.empty((plane_waves, bands), dtype=np.int32, order="F")
+        second = np.empty((plane_waves, bands), dtype=np.int32, order="F")
+        cur = ctypes.c_int64(self.current)
+        seed = ctypes.c_int64(self.seed)
+        _lib.check("qeb_qe_random_draws", _lib.load().qeb_qe_random_draws(
+            plane_waves, bands, self.table.ctypes.data, ctypes.byref(cur), ctypes.byref(seed),
+            first.ctypes.data, second.ctypes.data))
+        self.current, self.seed = int(cur.value), int(seed.value)
+        return first, second
+
+
+class StartingDraws:
+    """The random pairs of every k point's starting wavefunctions, drawn in
+    k-point order from one QE stream on a host thread while the SCF set-up
+    runs.  The stream is sequential (each draw picks the shuffle-table
+    entry of the previous one): the 2 x 504 x 80 725 draws of the 216-atom
+    cell take 0.5-0.7 s of one core, which the thread hides behind the
+    set-up; the ctypes call releases the GIL.  ``take(k)`` waits for k's
+    draws; those of k points outside ``keep`` (another pool's) only advance
+    the stream."""
+
+    def __init__(self, rng: QERandom, sizes, bands: int, keep=None) -> None:
+        sizes = [int(v) for v in sizes]
+        keep = set(range(len(sizes))) if keep is None else set(keep)
+        self._ready = [threading.Event() for _ in sizes]
+        self._draws: list = [None] * len(sizes)
+        self._error: BaseException | None = None
+        _lib.load()
+
+        def run() -> None:
+            try:
+                for k, npw in enumerate(sizes):
+                    pair = rng.draws(npw, bands)
+                    self._draws[k] = pair if k in keep else None
+                    self._ready[k].set()
+            except BaseException as exc:  # re-raised by take()
+                self._error = exc
+                for event in self._ready:
+                    event.set()
+
+        self._thread = threading.Thread(target=run, name="qe-random-draws", daemon=True)
+        self._thread.start()
+
+    def take(self, k: int) -> tuple[np.ndarray, np.ndarray]:
+        self._ready[k].wait()
+        if self._error is not None:
+            raise RuntimeError("random starting draws failed") from self._error
+        pair, self._draws[k] = self._draws[k], None
+        if pair is None:
+            raise RuntimeError(f"the draws of k point {k} were not kept or were already taken")
+        return pair
 
 
 class ChargeGrid:
@@ -384,21 +440,30 @@ def _as128(t: torch.Tensor) -> torch.Tensor:
     return t if t.dtype == torch.complex128 else t.to(torch.complex128).T.contiguous().T
 
 
-def random_starting_subspace(ham: PlaneWaveHamiltonian, basis, rng: QERandom, nbnd: int):
+def random_starting_subspace(ham: PlaneWaveHamiltonian, basis, source, nbnd: int):
     """Random trial vectors amp e^(2 pi i phase) / (1 + |k+G|^2) rotated by a
     Rayleigh-Ritz step in their span (qepy_pw/pw/scf.py:853-870, 923-953).
-    Returns (vectors, eigenvalues, H vectors) in the Hamiltonian's dtype."""
-    amp, phase = rng.pairs(len(basis), nbnd)
-    # the trial vectors are formed on the device (480 bands x 80 725 plane
-    # waves took a second as host complex exponentials)
+    ``source`` is a QERandom (drawn now) or the (first, second) integer
+    draws of this k point (QERandom.draws, StartingDraws.take).  Returns
+    (vectors, eigenvalues, H vectors) in the Hamiltonian's dtype."""
+    if isinstance(source, QERandom):
+        source = source.draws(len(basis), nbnd)
+    first, second = source
+    npw = len(basis)
+    if first.shape != (npw, nbnd) or second.shape != (npw, nbnd):
+        raise ValueError("the random draws do not match the basis and the band count")
+    # the trial vectors are formed on the device (qeb_random_trials): the
+    # host sends the 32-bit draws, a quarter of the complex128 trial bytes
     device = ham.device
-    amp_d = torch.from_numpy(amp).to(device)
-    phase_d = torch.from_numpy(phase).to(device)
-    denominator = 1.0 + 2.0 * torch.from_numpy(np.asarray(basis.kinetic, dtype=float)).to(device)
-    trials = torch.polar(amp_d, (2.0 * np.pi) * phase_d) / denominator[:, None]
-    del amp_d, phase_d
-    trials_dev = to_device_f(trials, ham.dtype, device)
-    del trials
+    first_d = torch.from_numpy(first.ravel(order="F")).to(device)
+    second_d = torch.from_numpy(second.ravel(order="F")).to(device)
+    kinetic = torch.from_numpy(np.ascontiguousarray(basis.kinetic, dtype=np.float64)).to(device)
+    trials_dev = empty_f(npw, nbnd, ham.dtype, device)
+    _lib.check("qeb_random_trials", _lib.load().qeb_random_trials(
+        npw, nbnd, first_d.data_ptr(), second_d.data_ptr(), kinetic.data_ptr(),
+        trials_dev.data_ptr(), leading_dimension(trials_dev),
+        1 if ham.dtype == torch.complex64 else 0, stream_handle()))
+    del first_d, second_d, kinetic
     applied = ham.apply(trials_dev)
     t128, a128 = _as128(trials_dev), _as128(applied)
     proj = K.gemm(K.OP_C, t128, a128)
@@ -451,11 +516,15 @@ class SCFSetup:
     v_ion_average: float         # its G = 0 component (QE v_of_0)
 
 
-def scf_setup(system: System, device) -> SCFSetup:
+def scf_setup(system: System, device, on_bases=None) -> SCFSetup:
     """Bases of every k point, the FFT grid by the reference's rule, the
-    charge sphere and V_ion(r) = sum_species V_loc(|G|) S(G)."""
+    charge sphere and V_ion(r) = sum_species V_loc(|G|) S(G).
+    ``on_bases(bases)``, when given, runs as soon as the bases exist (the
+    SCF starts its random draws there)."""
     reciprocal = system.reciprocal
     bases = make_bases(reciprocal, system.kpoints, system.ecutwfc)
+    if on_bases is not None:
+        on_bases(bases)
     shape = fft_shape(bases, reciprocal, system.ecutrho, fft_factors(system.operations))
     grid = ChargeGrid(shape, reciprocal, system.ecutrho)
     tables = {label: SpeciesTables(p, system.volume) for label, p in system.pseudos.items()}
@@ -663,7 +732,17 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     elif system.nbnd < occupied:
         raise ValueError("nbnd is smaller than the number of occupied states")
     fermi = None
-    setup = scf_setup(system, device)
+    draws = {}
+
+    def start_draws(bases) -> None:
+        # the first iteration's random pairs of every k point, drawn on a
+        # host thread during the rest of the set-up
+        nk_all = len(bases)
+        keep = list(pools.local_kpoints(nk_all)) if pools is not None else None
+        bands = min(system.nbnd + guard_bands, min(len(b) for b in bases))
+        draws["all"] = StartingDraws(QERandom(), [len(b) for b in bases], bands, keep)
+
+    setup = scf_setup(system, device, on_bases=start_draws)
     bases, shape, grid, cgrid = setup.bases, setup.shape, setup.grid, setup.cgrid
     tables, v_ion, v_ion_average = setup.tables, setup.v_ion, setup.v_ion_average
     if min(len(b) for b in bases) < system.nbnd:
@@ -680,8 +759,6 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
     states = [KPointState(b, shape, device) for b in bases]
     nk = len(states)
     local_k = list(pools.local_kpoints(nk)) if pools is not None else list(range(nk))
-    random_drawn = [False] * nk
-    rng = QERandom()
     davidson_tolerance = 0.5 * 1.0e-2  # diago_thr_init 1e-2 Ry -> Ha
     previous_accuracy = np.inf
     first_diagonalization = True
@@ -729,10 +806,8 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         hams, hams32, solves = {}, {}, {}
         for k, state in enumerate(states):
             if k not in local_k:
-                if state.vectors is None and iteration == 1 and not random_drawn[k]:
-                    # keep the shared random stream in step with one rank
-                    rng.pairs(len(state.basis), nsolve)
-                    random_drawn[k] = True
+                # (the shared random stream stays in step with one rank:
+                # StartingDraws draws every k point's pairs in order)
                 continue
             if state.terms is None:
                 state.terms = projector_terms(system, tables, state.basis)
@@ -764,8 +839,7 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             initial_eigs = None
             if state.vectors is None:
                 start_vectors, initial_eigs, initial_applied = random_starting_subspace(
-                    ham, state.basis, rng, nsolve)
-                random_drawn[k] = True
+                    ham, state.basis, draws["all"].take(k), nsolve)
             else:
                 start_vectors = state.vectors.to(ham.dtype).T.contiguous().T
             # first SCF iteration: rotate_wfc Ritz vectors (or the first

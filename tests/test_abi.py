@@ -58,3 +58,25 @@ def test_version_and_error_calls_need_no_gpu(library):
     status = handle.qeb_local_plan_create(ctypes.byref(plan), 0, 4, 4, 1, None, 0)
     assert status == -1
     assert "invalid grid" in _lib.last_error()
+
+
+def test_setup_entry_points_validate_before_any_launch(library):
+    """The projector-basis and symmetrisation entry points refuse bad
+    arguments with a status and a message, without touching a GPU."""
+    from qe_python_b200 import _lib
+
+    handle = _lib.load()
+    ints = (ctypes.c_int * 3)(0, 0, 0)
+    # a radial table of fewer than four rows cannot be interpolated
+    status = handle.qeb_projector_basis(10, 1, 1, 3, 1, 0.01, 1, ints, ints, ints, 1, 10, None)
+    assert status == -1 and "invalid arguments" in _lib.last_error()
+    # l = 3 channels are outside the harmonics this library tabulates
+    bad_l = (ctypes.c_int * 1)(3)
+    status = handle.qeb_projector_basis(10, 1, 1, 8, 1, 0.01, 1, ints, bad_l, ints, 1, 10, None)
+    assert status == -1 and "channel 0" in _lib.last_error()
+    offsets = (ctypes.c_int * (3 * 97))()
+    coefficients = (ctypes.c_int * (9 * 97))()
+    status = handle.qeb_symmetrize_density(4, 4, 4, 97, offsets, coefficients, 1, 2, None)
+    assert status == -2 and "operations exceed" in _lib.last_error()
+    status = handle.qeb_symmetrize_density(4, 4, 4, 2, offsets, coefficients, 1, 1, None)
+    assert status == -1 and "must differ" in _lib.last_error()

@@ -96,6 +96,52 @@ def test_qe_random_stream_matches_oracle():
     assert (a.current, a.seed) == (c2, sd2)
 
 
+def test_qe_random_integer_draws_match_pairs():
+    """The int32 stream values divided by 714025 are the double pairs, and
+    the stream state advances the same way, across several calls and a
+    draw longer than the 97-entry table."""
+    a, b = QERandom(), QERandom()
+    for npw, bands in ((7, 3), (1, 1), (0, 4), (300, 5)):
+        f1, s1 = a.pairs(npw, bands)
+        f2, s2 = b.draws(npw, bands)
+        assert f2.dtype == np.int32 and f2.flags.f_contiguous and f2.shape == (npw, bands)
+        np.testing.assert_array_equal(f1, f2 / 714025.0)
+        np.testing.assert_array_equal(s1, s2 / 714025.0)
+        assert (a.current, a.seed) == (b.current, b.seed)
+        np.testing.assert_array_equal(a.table, b.table)
+
+
+def test_starting_draws_follow_one_stream_in_kpoint_order():
+    """StartingDraws draws every k point in order on its thread; a pool
+    keeps only its own k points, and the values equal a sequential draw."""
+    from qe_python_b200.scf import StartingDraws
+
+    sizes, bands = [50, 37, 64], 4
+    serial = QERandom()
+    expected = [serial.draws(n, bands) for n in sizes]
+    everything = StartingDraws(QERandom(), sizes, bands)
+    for k in range(3):
+        got = everything.take(k)
+        np.testing.assert_array_equal(got[0], expected[k][0])
+        np.testing.assert_array_equal(got[1], expected[k][1])
+    with pytest.raises(RuntimeError, match="already taken"):
+        everything.take(0)
+    pool = StartingDraws(QERandom(), sizes, bands, keep=[1])
+    np.testing.assert_array_equal(pool.take(1)[1], expected[1][1])
+    with pytest.raises(RuntimeError, match="not kept"):
+        pool.take(2)
+
+
+def test_starting_draws_report_a_failed_draw():
+    from qe_python_b200.scf import StartingDraws
+
+    broken = QERandom()
+    broken.current = 714025  # outside the stream's range: the host routine refuses it
+    draws = StartingDraws(broken, [10, 10], 2)
+    with pytest.raises(RuntimeError, match="random starting draws failed"):
+        draws.take(1)
+
+
 def test_mixers_reduce_to_linear_on_first_step():
     s = benchmark_system("scf-fcc2")
     grid = ChargeGrid((24, 24, 24), s.reciprocal, s.ecutrho)

@@ -7,6 +7,11 @@
 * qeb_symmetrize_density against the host restatement of the reference's
   real-space symmetrizer (qepy_pw/symmetry.py:178-238), bit for bit, on the
   grids and space groups of the 2-atom fcc and 64-atom cells.
+* qeb_random_trials (the first iteration's random wavefunctions from the
+  stream's integer draws) against the reference's host formula
+  amp e^(2 pi i phase) / (1 + 2 T) (qepy_pw/pw/scf.py:855-869) on the
+  oracle's double pairs: the draws bit for bit, the complex exponential to
+  a few ulps (CUDA's sincos against NumPy's exp).
 """
 
 from __future__ import annotations
@@ -95,3 +100,45 @@ def test_symmetrize_density_matches_host(cuda_device, name):
     host = sym.apply(rho)
     got = sym.apply_device(torch.from_numpy(rho).to(cuda_device)).cpu().numpy()
     assert np.array_equal(got, host)
+
+
+@pytest.mark.parametrize("dtype_name", ["complex128", "complex64"])
+def test_random_trials_match_reference_formula(cuda_device, dtype_name):
+    import torch
+
+    from oracle import native_fft as oracle
+    from qe_python_b200.diagonalization import PlaneWaveHamiltonian
+    from qe_python_b200.scf import QERandom, benchmark_system, random_starting_subspace, scf_setup
+
+    system = benchmark_system("scf-fcc2")
+    setup = scf_setup(system, cuda_device)
+    basis = setup.bases[0]
+    npw, bands = len(basis), 8
+    rng = QERandom()
+    table, cur, seed = rng.table.copy(), rng.current, rng.seed
+    amp, phase, _, _ = oracle.qe_random_pairs(npw, bands, table, cur, seed)
+    want = amp * np.exp(2j * np.pi * phase) / (1.0 + 2.0 * basis.kinetic[:, None])
+    first, second = rng.draws(npw, bands)
+    np.testing.assert_array_equal(first / 714025.0, amp)
+    np.testing.assert_array_equal(second / 714025.0, phase)
+
+    captured = {}
+
+    class Recording(PlaneWaveHamiltonian):
+        def apply(self, x):
+            captured["trials"] = x.clone()
+            return super().apply(x)
+
+    from qe_python_b200.basis import LocalPotentialWorkspace
+    from qe_python_b200.scf import projector_terms
+
+    precision = "f64" if dtype_name == "complex128" else "f32"
+    ws = LocalPotentialWorkspace(basis, setup.shape, precision=precision, device=cuda_device)
+    ham = Recording(basis, None, projector_terms(system, setup.tables, basis), local_workspace=ws,
+                    real_potential=setup.v_ion, potential_average=setup.v_ion_average)
+    random_starting_subspace(ham, basis, (first, second), bands)
+    got = captured["trials"]
+    assert got.dtype == getattr(torch, dtype_name)
+    got = got.to(torch.complex128).cpu().numpy()
+    bound = 1.0e-15 if dtype_name == "complex128" else 1.2e-7
+    assert np.max(np.abs(got - want)) <= bound * np.max(np.abs(want))
