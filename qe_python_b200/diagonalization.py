@@ -31,6 +31,7 @@ from .device import (
     to_device_f,
     zeros_f,
 )
+from .eigensolver import ReducedSolve
 
 
 @dataclass(frozen=True)
@@ -475,21 +476,29 @@ def lowest_generalized_eigh(h: torch.Tensor, s: torch.Tensor, roots: int):
 
     Cholesky S = L L^H, reduced L^-1 H L^-H, Hermitian eigensolve, back
     transform (the transformation of LAPACK zhegv; reference fallback
-    qepy_pw/diagonalization.py:83-110).
+    qepy_pw/diagonalization.py:83-110), on the current stream
+    (eigensolver.ReducedSolve).  A subspace built from FP32 vectors can make
+    S numerically indefinite; the solve then falls back to the
+    well-conditioned part of its range (canonical orthogonalisation).
     """
-    h = h.to(torch.complex128)
-    s = s.to(torch.complex128)
-    lower, info = torch.linalg.cholesky_ex(s)
-    if int(info) != 0:
-        # A subspace built from FP32 vectors can make S numerically
-        # indefinite; solve in the well-conditioned part of its range
-        # (canonical orthogonalisation) instead of failing.
-        return _canonical_generalized_eigh(h, s, roots)
-    left = torch.linalg.solve_triangular(lower, h, upper=False)
-    reduced = torch.linalg.solve_triangular(lower, left.conj().T, upper=False).conj().T
-    values, vectors = torch.linalg.eigh(_hermitize(reduced))
-    vectors = torch.linalg.solve_triangular(lower.conj().T, vectors, upper=True)
-    return values[:roots], vectors[:, :roots]
+    solve = ReducedSolve(torch.cuda.current_stream(h.device))
+    solve.launch(h, s, roots)
+    return solve.result()
+
+
+class _Overlap:
+    """What a Davidson generator with ``overlap_solves`` yields after it has
+    enqueued its reduced eigensolve on its own stream: the driver may resume
+    the other problems (which then enqueue theirs) before this one, whose
+    next step reads the eigenvalues back to the host."""
+
+    __slots__ = ()
+
+    def __repr__(self) -> str:
+        return "OVERLAP"
+
+
+OVERLAP = _Overlap()
 
 
 def _canonical_generalized_eigh(h: torch.Tensor, s: torch.Tensor, roots: int,
@@ -563,7 +572,8 @@ def davidson(operator, diagonal, number_of_roots: int, *, initial_vectors=None,
     try:
         request = next(steps)
         while True:
-            apply_into(*request)
+            if request is not OVERLAP:
+                apply_into(*request)
             request = steps.send(None)
     except StopIteration as done:
         return done.value
@@ -727,25 +737,37 @@ def run_lockstep(problems, apply_batch) -> list:
     collects each unfinished problem's pending H application and hands them
     to ``apply_batch([(index, vectors, destination), ...])`` at once (the
     chosen form's batching of all k points into one launch per FFT pass).
+    A problem that yields OVERLAP (its reduced eigensolve enqueued on its own
+    stream) is resumed after the others have advanced to their next request
+    or OVERLAP, so the k points' eigensolves run side by side on the GPU.
     Each problem runs the same operations as alone; returns the results in
     order."""
     results = [None] * len(problems)
-    pending = {}
-    for index, steps in enumerate(problems):
-        try:
-            pending[index] = next(steps)
-        except StopIteration as done:
-            results[index] = done.value
+
+    def advance(indices, first: bool) -> dict:
+        """Resume ``indices`` until each has an H request or has finished."""
+        requests = {}
+        waiting = list(indices)
+        while waiting:
+            again = []
+            for index in waiting:
+                try:
+                    request = next(problems[index]) if first else problems[index].send(None)
+                except StopIteration as done:
+                    results[index] = done.value
+                    continue
+                if request is OVERLAP:
+                    again.append(index)
+                else:
+                    requests[index] = request
+            waiting, first = again, False
+        return requests
+
+    pending = advance(range(len(problems)), True)
     while pending:
         apply_batch([(index, vectors, destination)
                      for index, (vectors, destination) in pending.items()])
-        following = {}
-        for index in pending:
-            try:
-                following[index] = problems[index].send(None)
-            except StopIteration as done:
-                results[index] = done.value
-        pending = following
+        pending = advance(list(pending), False)
     return results
 
 
@@ -756,10 +778,14 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
                    initial_is_ritz: bool = False, initial_is_orthonormal: bool = False,
                    initial_eigenvalues=None, initial_applied=None,
                    global_dimension: int | None = None, global_row_indices=None, timers=None,
-                   dtype: torch.dtype | None = None, lock_converged: bool = False):
+                   dtype: torch.dtype | None = None, lock_converged: bool = False,
+                   overlap_solves: bool = False):
     """The Davidson algorithm of ``davidson`` as a generator: it yields
     ``(vectors, destination)`` whenever it needs destination = H vectors and
-    returns the DavidsonResult (StopIteration.value).
+    returns the DavidsonResult (StopIteration.value).  With
+    ``overlap_solves`` it runs its reduced eigensolves on a stream of its own
+    and yields OVERLAP between enqueuing one and reading its eigenvalues
+    (``run_lockstep`` overlaps the k points' solves).
 
     ``lock_converged`` (chosen form; the reference never locks): at each
     restart the roots already converged leave the reduced problem.  Their
@@ -854,11 +880,17 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
     root_ids = np.arange(number_of_roots)  # their indices among all roots
     locked = {"vectors": None, "count": 0, "values": [], "ids": [], "norms": []}
 
+    solver = ReducedSolve(torch.cuda.Stream(device) if overlap_solves
+                          else torch.cuda.current_stream(device))
+
     def ritz_values():
         """Lowest roots and coefficients of the reduced problem (:699-708)."""
         with _timer(timers, "cdiaghg"):
-            roots, coefficients = lowest_generalized_eigh(
-                projected[:active, :active], overlap[:active, :active], nroot)
+            solver.launch(projected[:active, :active], overlap[:active, :active], nroot)
+        if overlap_solves:
+            yield OVERLAP
+        with _timer(timers, "cdiaghg"):
+            roots, coefficients = solver.result()
         return roots.cpu().numpy(), roots, coefficients
 
     def ritz_columns(coefficients, roots, columns=None):
@@ -894,7 +926,7 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
         residuals = applied_storage[:, :number_of_roots].clone()
         K.subtract_band_energies(residuals, ritz_vectors, values_dev)
     else:
-        values, values_dev, coefficients = ritz_values()
+        values, values_dev, coefficients = yield from ritz_values()
         ritz_vectors, residuals = ritz_columns(coefficients, values_dev)
     track = residual_factor is not None or residual_energy_scale is not None
 
@@ -941,7 +973,7 @@ def davidson_steps(diagonal, number_of_roots: int, *, initial_vectors=None,
         yield basis_storage[:, old:active], applied_storage[:, old:active]
         applications += keep.size
         update_projected(old)
-        values, values_dev, coefficients = ritz_values()
+        values, values_dev, coefficients = yield from ritz_values()
         ritz_vectors = residuals = None
         if track:
             ritz_vectors, residuals = full_ritz()
@@ -1048,7 +1080,7 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
                            tolerance: float = 1.0e-8, max_iterations: int = 20,
                            subspace_multiplier: int = 2, occupied_roots: int | None = None,
                            timers=None, initial_state=None, state_out: dict | None = None,
-                           budget: float | None = None):
+                           budget: float | None = None, overlap_solves: bool = False):
     """Chosen-form Davidson: an FP64 block of vectors with FP32 corrections.
 
     A generator like ``davidson_steps``; it yields ``(vectors, destination)``
@@ -1106,7 +1138,8 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
     FP64 Rayleigh-Ritz step: one FP64 H application of the block, X^H H X
     and X^H X in FP64, the FP64 reduced eigensolve and the rotation.
     ``state_out`` (a dict) receives the final ``lam``, ``residual`` (None
-    when the budget is spent) and ``error``."""
+    when the budget is spent) and ``error``.  ``overlap_solves``: as in
+    ``davidson_steps`` (OVERLAP yielded around the reduced eigensolves)."""
     device = require_cuda()
     if budget is None:
         budget = REFINED_ERROR_BUDGET
@@ -1145,6 +1178,19 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
     del trial
     counts = {"applications": 0}
 
+    solver = ReducedSolve(torch.cuda.Stream(device) if overlap_solves
+                          else torch.cuda.current_stream(device))
+
+    def solve(h, s):
+        """Lowest n pairs of the pencil (h, s); OVERLAP between enqueuing
+        the solve and reading it when ``overlap_solves``."""
+        with _timer(timers, "cdiaghg"):
+            solver.launch(h, s, n)
+        if overlap_solves:
+            yield OVERLAP
+        with _timer(timers, "cdiaghg"):
+            return solver.result()
+
     def ritz_block(vectors):
         """FP64 Rayleigh-Ritz of ``vectors``: returns (X, lam, R) with X the
         Ritz vectors, lam their values and R = H X - X lam."""
@@ -1154,8 +1200,7 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
         with _timer(timers, "cegterg:over"):
             a = _hermitize(K.gemm(K.OP_C, vectors, hx))
             s = _hermitize(K.gemm(K.OP_C, vectors, vectors))
-        with _timer(timers, "cdiaghg"):
-            lam, rot = lowest_generalized_eigh(a, s, n)
+        lam, rot = yield from solve(a, s)
         with _timer(timers, "cegterg:upda"):
             rot = rot.T.contiguous().T
             ritz = K.gemm(K.OP_N, vectors, rot)
@@ -1232,9 +1277,7 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
             float(np.sqrt(npw))
 
     def reduced_solve(active):
-        with _timer(timers, "cdiaghg"):
-            return lowest_generalized_eigh(projected[:active, :active],
-                                           overlap[:active, :active], n)
+        return (yield from solve(projected[:active, :active], overlap[:active, :active]))
 
     error = 0.0  # rounding accumulated in the carried residual (Ha)
     exact = initial_state is None
@@ -1251,7 +1294,7 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
     active = n
     # Ritz values and residuals of the starting block (the reference's first
     # reduced solve, :699-724)
-    values_dev, coefficients = reduced_solve(active)
+    values_dev, coefficients = yield from reduced_solve(active)
     values = values_dev.cpu().numpy()
     block = composite_residuals(coefficients, values_dev, lam_dev, active)
     energies = values_dev
@@ -1295,7 +1338,7 @@ def refined_davidson_steps(diagonal, number_of_roots: int, *, initial_vectors,
         counts["applications"] += keep.size
         hd_norms[old:active] = torch.sqrt(K.column_squared_norms(applied32[:, old:active]))
         update_projected(old, active, lam_dev)
-        values_dev, coefficients = reduced_solve(active)
+        values_dev, coefficients = yield from reduced_solve(active)
         values = values_dev.cpu().numpy()
         converged = np.abs(values - previous) < root_tolerances
         unconverged = ~converged

@@ -36,6 +36,7 @@ from .basis import LocalPotentialWorkspace, fft_shape, make_bases
 from .configs import DIAMOND_CUBIC, displacements, supercell
 from .device import empty_f, leading_dimension, require_cuda, stream_handle, to_device_f
 from .diagonalization import (
+    OVERLAP,
     PlaneWaveHamiltonian,
     apply_hamiltonians,
     davidson,
@@ -581,15 +582,17 @@ MIXED_GUARD_BANDS = 24  # mixed form: extra Davidson roots beyond nbnd (run_scf 
 
 
 def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, tol, occ_roots,
-                   is_ritz, timers, lock=False, nroots=None, refined=False, carried=None):
+                   is_ritz, timers, lock=False, nroots=None, refined=False, carried=None,
+                   overlap=False):
     """One k point's diagonalisation as a generator of H applications: the
     Davidson of qepy_pw/pw/scf.py:3496-3556 (20 iterations), repeated up to
     five more times from its last vectors while more than five roots remain
     unconverged.  ``refined``: the chosen form's FP64-accurate Davidson
     (``refined_davidson_steps``: FP64 block, FP32 corrections), started
     from ``carried`` = (lam, R) when given; the final (lam, R) are left in
-    ``carried_out``.  Returns (DavidsonResult, Davidson iterations,
-    carried_out)."""
+    ``carried_out``.  ``overlap``: the solves yield OVERLAP around their
+    reduced eigensolves (lockstep k points).  Returns (DavidsonResult,
+    Davidson iterations, carried_out)."""
     attempt, total_its = 0, 0.0
     vectors, eigs, applied = start_vectors, initial_eigs, initial_applied
     carried_out: dict = {}
@@ -599,7 +602,7 @@ def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, to
                 ham.diagonal, nroots or system.nbnd, initial_vectors=vectors, tolerance=tol,
                 max_iterations=20, subspace_multiplier=system.diago_david_ndim,
                 occupied_roots=occ_roots, timers=timers, initial_state=carried,
-                state_out=carried_out)
+                state_out=carried_out, overlap_solves=overlap)
             carried = (None if carried_out["residual"] is None
                        else (carried_out["lam"], carried_out["residual"], carried_out["error"]))
         else:
@@ -609,7 +612,7 @@ def _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied, to
                 subspace_multiplier=system.diago_david_ndim, residual_factor=None,
                 residual_energy_scale=None, occupied_roots=occ_roots, initial_is_ritz=is_ritz,
                 initial_is_orthonormal=True, initial_eigenvalues=eigs, initial_applied=applied,
-                timers=timers, dtype=ham.dtype, lock_converged=lock)
+                timers=timers, dtype=ham.dtype, lock_converged=lock, overlap_solves=overlap)
         attempt += 1
         total_its += sol.iterations
         if sol.converged or sol.number_unconverged <= 5 or attempt >= 6:
@@ -624,8 +627,9 @@ def _drive(steps, ham, ham32=None):
     try:
         request = next(steps)
         while True:
-            target = ham32 if ham32 is not None and request[0].dtype == torch.complex64 else ham
-            target.apply_into(*request)
+            if request is not OVERLAP:
+                target = ham32 if ham32 is not None and request[0].dtype == torch.complex64 else ham
+                target.apply_into(*request)
             request = steps.send(None)
     except StopIteration as done:
         return done.value
@@ -804,6 +808,8 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         local_eigenvalues = {}
         its = []
         hams, hams32, solves = {}, {}, {}
+        # lockstep k points: their reduced eigensolves run side by side
+        lockstep = bool(batch_kpoints) and len(local_k) > 1
         for k, state in enumerate(states):
             if k not in local_k:
                 # (the shared random stream stays in step with one rank:
@@ -851,9 +857,9 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
             solves[k] = _k_point_solve(ham, system, start_vectors, initial_eigs, initial_applied,
                                        tol, occ_roots, iteration == 1, timers,
                                        lock=lock_converged, nroots=nsolve, refined=refined,
-                                       carried=carried)
+                                       carried=carried, overlap=lockstep)
         k_order = sorted(solves)
-        if batch_kpoints and len(k_order) > 1:
+        if lockstep:
             # chosen form: the k points' Davidson solves advance together and
             # each round's H applications share one launch per FFT pass
             table = [hams[k] for k in k_order]
