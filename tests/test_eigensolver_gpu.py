@@ -117,10 +117,10 @@ def test_solves_on_four_streams_equal_sequential_solves(cuda_device):
     solves = [ReducedSolve(torch.cuda.Stream(cuda_device)) for _ in pencils]
     for solve, (h, s) in zip(solves, pencils):
         solve.launch(h, s, 100)
-    for solve, (want_values, want_vectors) in zip(solves, sequential):
+    for solve, (h, s), (want_values, want_vectors) in zip(solves, pencils, sequential):
         values, vectors = solve.result()
         np.testing.assert_allclose(values.cpu().numpy(), want_values, rtol=0, atol=1e-13)
-        # eigenvectors up to a phase per column
+        # S-orthonormal eigenvectors, equal up to a phase per column
         got = vectors.cpu().numpy()
-        phase = np.sum(want_vectors.conj() * got, axis=0)
+        phase = np.sum(want_vectors.conj() * (s.cpu().numpy() @ got), axis=0)
         assert np.allclose(np.abs(phase), 1.0, atol=1e-10)
