@@ -229,12 +229,37 @@ def _charge_extent(reciprocal: np.ndarray, ecut_ry: float) -> np.ndarray:
     ecut_ha = 0.5 * float(ecut_ry)
     sigma_min = float(np.linalg.svd(reciprocal, compute_uv=False)[-1])
     bound = int(_search_bound(reciprocal, np.zeros(3), ecut_ha, sigma_min))
-    cube = _miller_cube(bound)
-    g = cube @ reciprocal
-    inside = 0.5 * np.einsum("ij,ij->i", g, g) <= ecut_ha + _CUTOFF_SLACK
-    if not inside.any():
-        raise ValueError("ecutrho produces an empty charge sphere")
-    return np.max(np.abs(cube[inside]), axis=0)
+    # Along axis a the sphere reaches |m_a| <= sqrt(2 ecut) |column a of
+    # reciprocal^-1|; the planes m_a = +-m are checked from that bound down
+    # with the same row test as the whole Miller cube (2-D slices of it
+    # instead of the cube itself: the 216-atom cell's charge sphere spans a
+    # 137^3 cube).
+    inverse_norms = np.linalg.norm(np.linalg.inv(reciprocal), axis=0)
+    axis = np.arange(-bound, bound + 1, dtype=np.int32)
+    u, v = np.meshgrid(axis, axis, indexing="ij")
+    u, v = u.ravel(), v.ravel()
+    extent = np.zeros(3, dtype=np.int64)
+    for a in range(3):
+        top = min(bound, int(np.floor(np.sqrt(2.0 * (ecut_ha + _CUTOFF_SLACK))
+                                      * inverse_norms[a])) + 1)
+        others = [b for b in range(3) if b != a]
+        found = -1
+        for m in range(top, -1, -1):
+            for sign in ((1, -1) if m else (1,)):
+                rows = np.empty((u.size, 3), dtype=np.int32)
+                rows[:, a] = sign * m
+                rows[:, others[0]] = u
+                rows[:, others[1]] = v
+                g = rows @ reciprocal
+                if np.any(0.5 * np.einsum("ij,ij->i", g, g) <= ecut_ha + _CUTOFF_SLACK):
+                    found = m
+                    break
+            if found >= 0:
+                break
+        if found < 0:
+            raise ValueError("ecutrho produces an empty charge sphere")
+        extent[a] = found
+    return extent
 
 
 def make_basis(reciprocal, k_crystal, ecut_ry: float) -> PlaneWaveBasis:

@@ -85,6 +85,24 @@ def lagrange4(table: np.ndarray, q: np.ndarray) -> np.ndarray:
             + table[lower + 3] * (f * u * v / 6.0)[:, None])
 
 
+def lagrange4_derivative(table: np.ndarray, q: np.ndarray) -> np.ndarray:
+    """d/dq of ``lagrange4``: the derivatives of the four Lagrange weights
+    in the fraction f = q/dq - floor(q/dq), divided by dq
+    (qepy_pw/upf.py:880-914)."""
+    scaled = q / DQ
+    lower = np.floor(scaled).astype(np.int64)
+    f = scaled - lower
+    u, v, w = 1.0 - f, 2.0 - f, 3.0 - f
+    weights = (-(v * w + u * w + u * v) / 6.0, (v * w - f * (v + w)) / 2.0,
+               -(u * w - f * (u + w)) / 2.0, (u * v - f * (u + v)) / 6.0)
+    out = 0.0
+    for offset, weight in enumerate(weights):
+        sample = table[lower + offset]
+        out = out + (sample * (weight / DQ) if table.ndim == 1
+                     else sample * (weight / DQ)[:, None])
+    return out
+
+
 class SpeciesTables:
     """V_loc(q) and beta_l(q) of one pseudopotential in one cell volume."""
 
@@ -143,6 +161,22 @@ class SpeciesTables:
                 * np.exp(-0.25 * qp**2) / qp**2
         return out
 
+    def vloc_with_derivative(self, q: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+        """V_loc(|G|) and dV_loc/d|G| (zero at G = 0): the table's
+        interpolation derivative plus that of the analytic -Z erf(r)/r tail
+        (qepy_pw/upf.py:224-261)."""
+        q = np.asarray(q, dtype=float)
+        values = self.vloc(q)
+        derivative = np.zeros_like(q)
+        positive = q > 1.0e-12
+        if np.any(positive):
+            qp = q[positive]
+            table = self._vloc_table(float(qp.max()))
+            tail = -(4.0 * np.pi / self.volume) * self.pseudo.z_valence \
+                * np.exp(-0.25 * qp**2) / qp**2
+            derivative[positive] = lagrange4_derivative(table, qp) + tail * (-0.5 * qp - 2.0 / qp)
+        return values, derivative
+
     # -- projectors -----------------------------------------------------------
     def _beta_table(self, qmax: float) -> np.ndarray:
         if self._beta is not None and self._beta_qmax + 1.0e-14 >= qmax:
@@ -197,6 +231,47 @@ class SpeciesTables:
                 if li == lj and mi == mj:
                     coupling[i, j] = 0.5 * p.dij_ry[ri, rj]
         return beta, coupling
+
+    def projectors_with_gradient(self, kg: np.ndarray):
+        """``projectors`` and the Cartesian gradient of every column with
+        respect to k+G, (npw, channels, 3): (-i)^l (dbeta/dq Y_lm khat +
+        beta grad Y_lm), zero at k+G = 0 (qepy_pw/upf.py:558-597).  The l = 1
+        harmonics are s1 (z, -x, -y)/q, whose gradients are
+        s1 (e_a - khat_a khat)/q."""
+        p = self.pseudo
+        beta, coupling = self.projectors(kg)
+        q = np.sqrt(kg[:, 0] ** 2 + kg[:, 1] ** 2 + kg[:, 2] ** 2)
+        table = self._beta_table(float(q.max()) if q.size else 0.0)
+        radial = lagrange4(table, q)
+        radial_d = lagrange4_derivative(table, q)
+        safe = q > 1.0e-14
+        inv = np.where(safe, 1.0 / np.where(safe, q, 1.0), 0.0)
+        khat = kg * inv[:, None]
+        s0 = 1.0 / math.sqrt(4.0 * math.pi)
+        s1 = math.sqrt(3.0 / (4.0 * math.pi))
+        gradient = np.zeros((len(q), beta.shape[1], 3), dtype=np.complex128)
+        column = 0
+        for index, l in enumerate(p.angular_momenta):
+            phase = (-1j) ** l
+            if l == 0:
+                harmonics = [(np.full_like(q, s0), np.zeros((len(q), 3)))]
+            elif l == 1:
+                harmonics = []
+                for axis, sign in ((2, 1.0), (0, -1.0), (1, -1.0)):
+                    unit = np.zeros(3)
+                    unit[axis] = 1.0
+                    value = sign * s1 * khat[:, axis]
+                    grad = sign * s1 * (unit[None, :] - khat[:, axis:axis + 1] * khat) \
+                        * inv[:, None]
+                    harmonics.append((value, grad))
+            else:
+                raise ValueError("only l <= 1 projectors are supported")
+            for value, grad in harmonics:
+                gradient[:, column, :] = phase * (radial_d[:, index, None] * khat * value[:, None]
+                                                  + radial[:, index, None] * grad)
+                column += 1
+        gradient[~safe] = 0.0
+        return beta, coupling, gradient
 
 
 def channel_list(angular_momenta) -> list[tuple[int, int, int]]:

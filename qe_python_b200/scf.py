@@ -83,6 +83,7 @@ class System:
     diago_david_ndim: int = 2
     maxiter: int = 100
     forces: bool = False
+    stress: bool = False         # analytic stress at convergence (tstress)
     name: str = ""
     occupations: str = "fixed"   # or "smearing"
     smearing: str = "gaussian"
@@ -251,11 +252,16 @@ class ChargeGrid:
         x, y, z = axes[0][:, None, None], axes[1][None, :, None], axes[2][None, None, :]
         g2 = (metric[0, 0] * x * x + metric[1, 1] * y * y + metric[2, 2] * z * z
               + 2.0 * metric[0, 1] * x * y + 2.0 * metric[0, 2] * x * z + 2.0 * metric[1, 2] * y * z)
-        self.slots = np.argwhere(g2 <= cutoff_ry + 1.0e-12).astype(np.int32)
+        # C-order grid points inside the sphere (argwhere's order), found
+        # through their flat offsets
+        flat = np.flatnonzero(g2 <= cutoff_ry + 1.0e-12)
+        i0, rest = np.divmod(flat, self.shape[1] * self.shape[2])
+        i1, i2 = np.divmod(rest, self.shape[2])
+        self.slots = np.column_stack((i0, i1, i2)).astype(np.int32)
         self.index = tuple(self.slots.T)
-        self.miller = np.column_stack([axes[a][self.slots[:, a]] for a in range(3)]).astype(np.int32)
+        self.miller = np.column_stack((axes[0][i0], axes[1][i1], axes[2][i2])).astype(np.int32)
         self.vectors = self.miller @ reciprocal
-        self.g2 = g2[self.index]
+        self.g2 = g2.reshape(-1)[flat]
         self.size = int(np.prod(self.shape))
 
     def to_g(self, grid: np.ndarray) -> np.ndarray:
@@ -394,6 +400,9 @@ class SCFResult:
     # point's eigenvectors (device, complex128, nbnd + guard columns)
     potential: "torch.Tensor | None" = None
     eigenvectors: list = field(default_factory=list)
+    # analytic stress and its symmetrised terms (Ha/bohr^3) when asked for
+    stress_ha_per_bohr3: np.ndarray | None = None
+    stress_terms: "object | None" = None
 
     @property
     def total_energy_ry(self) -> float:
@@ -981,8 +990,19 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
         if converged:
             break
         iteration += 1
+    rho_device = rho
     rho = rho.cpu().numpy()
     forces = None
+    stress = stress_terms = None
+    if system.stress and converged:
+        from .stress import scf_stress
+
+        t0 = time.perf_counter()
+        stress, stress_terms = scf_stress(system, [states[k] for k in local_k], tables, grid, cgrid,
+                                          rho_device, [band_occ[k] for k in local_k],
+                                          [system.weights[k] for k in local_k], pools=pools)
+        tick("stress", t0)
+    del rho_device
     if system.forces and converged:
         from .forces import hellmann_feynman_forces
 
@@ -996,4 +1016,4 @@ def run_scf(system: System, precision: str = "f64", switch_ry: float = 1.0e-5,
                      [s.eigenvalues for s in states], energy_terms, rho, forces,
                      time.perf_counter() - started, precision_log, david_its, timings,
                      [np.asarray(f) for f in band_occ], fermi, v_dev,
-                     [states[k].vectors for k in local_k])
+                     [states[k].vectors for k in local_k], stress, stress_terms)

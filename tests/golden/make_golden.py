@@ -449,6 +449,43 @@ def displaced_energies(workdir: Path, filename: str, coordinates, step: float) -
         (HERE / filename).write_text(json.dumps(record, indent=1))
 
 
+def stress(name: str, workdir: Path, filename: str) -> None:
+    """The reference's analytic stress (tstress) at SCF convergence and its
+    seven terms, Ha/bohr^3 (qepy_pw/pw/scf.py:1676-1931, ewald.py:261)."""
+    from qepy_pw.pw.input import read_pw_input
+    from qepy_pw.scf import run_scf
+
+    from qe_python_b200.configs import ELECTRON_OVERRIDES, config_input
+    from qe_python_b200.pseudo import write_synthetic_upf
+
+    write_synthetic_upf(workdir / "X.upf")
+    text = config_input(name, str(workdir))
+    text = text.replace("disk_io = 'none'", "disk_io = 'none',\n  tstress = .true.", 1)
+    text = text.replace("conv_thr = 1e-08", "conv_thr = 1e-10")
+    path = workdir / f"{name}-stress.in"
+    path.write_text(text)
+    pw = read_pw_input(path)
+    pw.electrons.update({k: v for k, v in ELECTRON_OVERRIDES.get(name, {}).items()
+                         if k != "conv_thr"})
+    started = time.perf_counter()
+    result = run_scf(pw)
+    elapsed = time.perf_counter() - started
+    terms = result.stress_terms
+    record = {
+        "config": name, "conv_thr_ry": 1.0e-10,
+        "total_energy_ry": 2.0 * float(result.iterations[-1].total_energy_ha),
+        "stress_ha_per_bohr3": np.asarray(result.stress_ha_per_bohr3).tolist(),
+        "terms_ha_per_bohr3": {field: np.asarray(getattr(terms, field)).tolist()
+                               for field in ("kinetic_ha_per_bohr3", "local_ha_per_bohr3",
+                                             "nonlocal_ha_per_bohr3", "hartree_ha_per_bohr3",
+                                             "xc_ha_per_bohr3", "core_correction_ha_per_bohr3",
+                                             "ewald_ha_per_bohr3")},
+        "reference_wall_seconds": elapsed,
+    }
+    (HERE / filename).write_text(json.dumps(record, indent=1))
+    print(f"{name}: stress (Ha/bohr^3) {record['stress_ha_per_bohr3']} in {elapsed:.1f} s")
+
+
 def _displace(text: str, atom: int, axis: int, delta: float) -> str:
     """Move one atom of a pw.x input's ATOMIC_POSITIONS (bohr) block."""
     lines = text.splitlines()
@@ -479,7 +516,7 @@ def main() -> None:
     parser.add_argument("--skip-scf", action="store_true")
     parser.add_argument("--only", default=None,
                         help="comma-separated subset: first-iteration-dia64, "
-                             "first-iteration-dia216, fd-forces")
+                             "first-iteration-dia216, fd-forces, stress")
     args = parser.parse_args()
     load_reference()
     if args.only:
@@ -491,6 +528,9 @@ def main() -> None:
                 elif part == "first-iteration-dia216":
                     first_iteration("scf-dia216", workdir, "first_iteration_dia216.json", 20,
                                     tolerance=1.0e-8)
+                elif part == "stress":
+                    stress("scf-fcc2", workdir, "stress_fcc2.json")
+                    stress("scf-dia8-disp", workdir, "stress_dia8.json")
                 elif part == "fd-forces":
                     displaced_energies(workdir, "fd_forces_dia8.json",
                                        [(0, 0), (3, 1), (5, 2), (6, 0)], 1.0e-3)
