@@ -74,6 +74,13 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr) {
          ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
+// The same with a 64-byte swizzle: 64-byte K-major rows (16 FP32 words),
+// 8-row groups 512 bytes apart (SBO), tile base 512-byte aligned.
+__device__ __forceinline__ uint64_t smem_desc_sw64(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(512 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+
 // Instruction descriptor: D = F32, A = B = TF32, both K-major, M x N.
 __host__ __device__ constexpr uint32_t idesc_tf32(int m, int n) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(n >> 3) << 17) |
