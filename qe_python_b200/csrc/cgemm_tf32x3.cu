@@ -4,47 +4,36 @@
 //
 // A, B and C are column-major complex64 matrices.  Unlike qeb_tf32_gemm,
 // nothing is packed beforehand: each pipeline stage TMA-loads the raw FP32
-// words of one 128-row by 8-complex slab of A and of B into shared memory,
-// and the splitter warps split every value x into hi = tf32(x) and
-// lo = tf32(x - hi) in place, in the 64-byte-swizzled K-major layout that
+// words of one 128-row by 16-complex slab of A and of B into shared memory,
+// and the worker warps split every value x into hi = tf32(x) and
+// lo = tf32(x - hi) in place, in the 128-byte-swizzled K-major layout that
 // tcgen05.mma reads.  The complex product is carried by real products over
 // (re, im) pairs interleaved along K:
 //   OP_C  Re(conj(a) b) = [a_re, a_im].[b_re, b_im]
 //         Im(conj(a) b) = [a_re, a_im].[b_im, -b_re]       (B1 = swap-negated B)
 //   OP_N  Re(a b)       = [a_re, -a_im].[b_re, b_im]      (A0, A transposed by
-//         Im(a b)       = [a_im, a_re].[b_re, b_im]        the splitters)
+//         Im(a b)       = [a_im, a_re].[b_re, b_im]        the workers)
 // and each real product is hi*hi + hi*lo + lo*hi, three tcgen05.mma.kind::tf32.
 //
 // Two-level accumulation: the tensor cores add each MMA's products into the
 // FP32 accumulator with an error that grows with the number of additions
 // (measured: 7e-6 relative after 384 MMAs into one accumulator, 2e-4 after
-// 12 000), so every pair of stages (12 MMAs per accumulator) starts a fresh
-// tensor-memory accumulator (two buffers of Re and Im, 512 columns) and the
-// drain warps add it into FP32 registers with round-to-nearest.  The result
-// is as accurate as an FP32 FMA GEMM.
+// 12 000), so each stage's 12 MMAs per accumulator start a fresh tensor-memory
+// accumulator (two buffers of Re and Im, 512 columns) and the worker warps add
+// it into FP32 registers with round-to-nearest.  The result is as accurate
+// as an FP32 FMA GEMM.
 //
-// Stages are 8 complex values deep along K (64-byte K-major rows, 64-byte
-// swizzle), so that four fit in shared memory and the producer runs up to
-// three stages ahead of the tensor cores: the TMA latency hides behind the
-// MMAs of the stages in between.  The roles are split over warps so that
-// the split of one stage, the MMAs of another and the drain of a third
-// overlap:
-//   warp 0 lane 0 : TMA producer, four stages
+// One CTA = 320 threads computes a 128 x 128 output tile over a K range:
+//   warp 0 lane 0 : TMA producer, two stages
 //   warp 1 lane 0 : MMA issuer; warp 1 owns the tensor-memory allocation
-//   warps 2-3     : splitters: hi/lo (and the OP_N transpose) of each stage
-//                   in place; they hold no accumulators, so each thread
-//                   issues all of its shared-memory loads before converting
-//   warps 4-11    : drainers: add each accumulator pair into registers,
-//                   then store C
-// (With two 16-deep stages and one group of warps that split, drained and
-// held the accumulators, the load latency of every stage was exposed and the
-// tensor pipe was busy ~40 % of the time; four 8-deep stages with the same
-// warps doubled the drains and were slower.)  Drain warp w reads
-// tensor-memory lanes 32 (w % 4) .. +31 (its rows) and columns
-// 64 ((w - 4) / 4) .. +63 of Re and of Im.  K is split across CTAs (grid.z)
-// into caller scratch when the output has few tiles; a second kernel sums the
-// slices in a fixed order.  Every wait is bounded; on timeout the CTA records
-// an error code in the device word read by qeb_tf32_gemm_error and unwinds.
+//   warps 2-9     : workers: split the next stage, drain the previous
+//                   stage's accumulator into registers, then store C
+// Worker warp w reads tensor-memory lanes 32 (w % 4) .. +31 (its rows) and
+// columns 64 ((w - 2) / 4) .. +63 of Re and of Im.  K is split across CTAs
+// (grid.z) into caller scratch when the output has few tiles; a second kernel
+// sums the slices in a fixed order.  Every wait is bounded; on timeout the
+// CTA records an error code in the device word read by qeb_tf32_gemm_error
+// and unwinds.
 //
 // Requirements (else QEB_STATUS_EUNSUPPORTED, and the caller uses the packed
 // path): A and B 16-byte aligned with even leading dimensions (TMA rows must
@@ -61,23 +50,18 @@ namespace {
 using namespace qeb::tc;
 
 constexpr int BM = 128, BN = 128;
-constexpr int BKF = 16;              // FP32 words along K per stage (8 complex values)
-constexpr int TILE = 8192;           // bytes of one 128-row x 16-word tile
-constexpr int ROW_BYTES = BKF * 4;   // one K-major tile row: 64 bytes
-constexpr int STAGES = 4;
-constexpr int KT_WORDS = 32;         // words of the host's K tiles (two stages)
-constexpr int SPLITTERS = 2;                    // warps 2 .. 3
-constexpr int SPLIT_THREADS = 32 * SPLITTERS;
-constexpr int DRAINERS = 8;                     // warps 4 .. 11
-constexpr int FIRST_DRAINER = 2 + SPLITTERS;
-constexpr int THREADS = 32 * (FIRST_DRAINER + DRAINERS);
+constexpr int BKF = 32;      // FP32 words along K per stage (16 complex values)
+constexpr int TILE = 16384;  // bytes of one 128-row x 32-word tile
+constexpr int STAGES = 2;
+constexpr int WORKERS = 8;                 // worker warps (2 .. 9)
+constexpr int WORKER_THREADS = 32 * WORKERS;
+constexpr int THREADS = 64 + WORKER_THREADS;
 constexpr int ACC_COLS = 2 * BN;           // Re and Im of one accumulator buffer
 constexpr int TMEM_COLS = 2 * ACC_COLS;    // two buffers
 constexpr uint32_t kIdesc = idesc_tf32(BM, BN);
-static_assert(DRAINERS == 8, "eight drain warps cover 4 lane windows x 2 column halves");
 
 // Tile slots of one stage.  OP_C: 0 A (raw, then hi), 1 A lo, 2 B (raw, then
-// hi), 3 B lo, 4 B1 hi, 5 B1 lo.  OP_N: 0 A raw (8 x 256 words, row-major,
+// hi), 3 B lo, 4 B1 hi, 5 B1 lo.  OP_N: 0 A raw (16 x 256 words, row-major,
 // unswizzled), 1 B (raw, then hi), 2 B lo, 3 A0 hi, 4 A0 lo, 5 A1 hi, 6 A1 lo.
 template <int OP>
 struct Slots {
@@ -109,22 +93,15 @@ __device__ __forceinline__ float4 lo4(float4 v, float4 h) {
 }
 
 // Split one K-major tile in place (hi) with its lo part into another slot.
-// The split is elementwise, so the swizzle needs no attention.  A splitter
-// thread owns kSplitPer 16-byte units and loads all of them first.
-constexpr int kSplitPer = TILE / 16 / SPLIT_THREADS;
-static_assert(kSplitPer * 16 * SPLIT_THREADS == TILE, "the splitters cover a tile exactly");
-
+// The split is elementwise, so the 128-byte swizzle needs no attention.
 __device__ __forceinline__ void split_tile(unsigned char* tile, unsigned char* lo, int ct,
                                            unsigned char* swap_hi, unsigned char* swap_lo) {
   float4* t = reinterpret_cast<float4*>(tile);
   float4* l = reinterpret_cast<float4*>(lo);
-  float4 v[kSplitPer];
-#pragma unroll
-  for (int j = 0; j < kSplitPer; ++j) v[j] = t[ct + j * SPLIT_THREADS];
-#pragma unroll
-  for (int j = 0; j < kSplitPer; ++j) {
-    const int c = ct + j * SPLIT_THREADS;
-    const float4 h = hi4(v[j]), w = lo4(v[j], h);
+#pragma unroll 2
+  for (int c = ct; c < TILE / 16; c += WORKER_THREADS) {
+    const float4 v = t[c];
+    const float4 h = hi4(v), w = lo4(v, h);
     t[c] = h;
     l[c] = w;
     if (swap_hi != nullptr) {  // (re, im) -> (im, -re)
@@ -134,33 +111,21 @@ __device__ __forceinline__ void split_tile(unsigned char* tile, unsigned char* l
   }
 }
 
-// OP_N: transpose the raw M-major slab of A (8 K rows x 128 complex) into the
-// K-major tiles A0 = [re, -im] and A1 = [im, re], hi and lo.  64-byte
-// swizzle: the 16-byte chunk c of row m sits at chunk c ^ ((m / 2) % 4).
-constexpr int kTransposePer = BM * (BKF / 4) / SPLIT_THREADS;
-static_assert(kTransposePer * SPLIT_THREADS == BM * (BKF / 4), "the splitters cover a slab");
-
+// OP_N: transpose the raw M-major slab of A (16 K rows x 128 complex) into
+// the K-major swizzled tiles A0 = [re, -im] and A1 = [im, re], hi and lo.
 __device__ __forceinline__ void transpose_a(const unsigned char* raw, unsigned char* a0h,
                                             unsigned char* a0l, unsigned char* a1h,
                                             unsigned char* a1l, int ct) {
   const float2* x = reinterpret_cast<const float2*>(raw);
-  float2 xs[kTransposePer][2];
-#pragma unroll
-  for (int j = 0; j < kTransposePer; ++j) {
-    const int it = ct + j * SPLIT_THREADS;
+#pragma unroll 2
+  for (int it = ct; it < BM * 8; it += WORKER_THREADS) {
     const int m = it & (BM - 1), kp = it >> 7;  // kp: pair of K values 2kp, 2kp+1
-    xs[j][0] = x[(2 * kp) * BM + m];
-    xs[j][1] = x[(2 * kp + 1) * BM + m];
-  }
-#pragma unroll
-  for (int j = 0; j < kTransposePer; ++j) {
-    const int it = ct + j * SPLIT_THREADS;
-    const int m = it & (BM - 1), kp = it >> 7;
-    const float2 x0 = xs[j][0], x1 = xs[j][1];
+    const float2 x0 = x[(2 * kp) * BM + m];
+    const float2 x1 = x[(2 * kp + 1) * BM + m];
     const float4 r0 = make_float4(x0.x, -x0.y, x1.x, -x1.y);
     const float4 r1 = make_float4(x0.y, x0.x, x1.y, x1.x);
     const float4 h0 = hi4(r0), h1 = hi4(r1);
-    const int off = m * ROW_BYTES + ((kp ^ ((m >> 1) & 3)) << 4);
+    const int off = m * 128 + ((kp ^ (m & 7)) << 4);
     *reinterpret_cast<float4*>(a0h + off) = h0;
     *reinterpret_cast<float4*>(a0l + off) = lo4(r0, h0);
     *reinterpret_cast<float4*>(a1h + off) = h1;
@@ -168,14 +133,14 @@ __device__ __forceinline__ void transpose_a(const unsigned char* raw, unsigned c
   }
 }
 
-// Drain side of accumulator pair p: wait until its MMAs are done, add Re
-// (columns [0, 64) of this warp's half) and Im into registers, release the
-// buffer.  False on a timed-out wait.
+// Worker side of one stage's accumulator buffer: wait until its MMAs are
+// done, add Re (columns [0, 64) of this warp's half) and Im into registers,
+// release the buffer.  False on a timed-out wait.
 __device__ __forceinline__ bool drain_accumulator(float (&acc)[BN], uint64_t* acc_full,
-                                                  uint64_t* acc_empty, int p, uint32_t lane_base,
+                                                  uint64_t* acc_empty, int i, uint32_t lane_base,
                                                   int lane) {
-  const int b = p & 1;
-  if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], (p >> 1) & 1))) return false;
+  const int b = i & 1;
+  if (!__all_sync(0xffffffffu, mbar_wait(&acc_full[b], (i >> 1) & 1))) return false;
   asm volatile("tcgen05.fence::after_thread_sync;");
   const uint32_t t = lane_base + b * ACC_COLS;
 #pragma unroll
@@ -197,21 +162,20 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
     const __grid_constant__ Maps maps, int M, int N, int kb_per_split, int kb_total, float2 alpha,
     float2 beta, float2* C, int64_t ldc, float2* split, int* error, int skip_m, int skip_n,
     int m_off, int n_off, int tail_tiles) {
-  // kb_*: K ranges in stages of BKF words.  TAIL == false: grid (M tiles,
-  // N tiles, K slices); the tiles of column skip_n from row skip_m on belong
-  // to a tail launch and return at once.  TAIL: grid (tail tiles, 1, K
-  // slices) over rows m_off + x of column n_off; the K slices go to compact
-  // BM x BN partial tiles.
+  // TAIL == false: grid (M tiles, N tiles, K slices); the tiles of column
+  // skip_n from row skip_m on belong to a tail launch and return at once.
+  // TAIL: grid (tail tiles, 1, K slices) over rows m_off + x of column
+  // n_off; the K slices go to compact BM x BN partial tiles.
   if (!TAIL && (int)blockIdx.y == skip_n && (int)blockIdx.x >= skip_m) return;
   using S = Slots<OP>;
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   unsigned char* base = reinterpret_cast<unsigned char*>(
       (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(base + STAGES * S::stage_bytes);
-  uint64_t* conv = full + STAGES;       // stage split by the splitters
+  uint64_t* conv = full + STAGES;       // stage split by the workers
   uint64_t* empty = conv + STAGES;      // stage consumed by the MMAs
   uint64_t* acc_full = empty + STAGES;  // accumulator buffer written by the MMAs
-  uint64_t* acc_empty = acc_full + 2;   // accumulator buffer drained by the drainers
+  uint64_t* acc_empty = acc_full + 2;   // accumulator buffer drained by the workers
   uint64_t* done = acc_empty + 2;       // every MMA issued has completed
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(done + 1);
   int* abort_flag = reinterpret_cast<int*>(tmem_slot + 1);
@@ -222,17 +186,16 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
   const int n0 = ((int)blockIdx.y + (TAIL ? n_off : 0)) * BN;
   const int kb0 = blockIdx.z * kb_per_split;
   const int nk = max(0, min(kb_total, kb0 + kb_per_split) - kb0);
-  const int npairs = (nk + 1) / 2;  // accumulator pairs (the last may hold one stage)
 
   if (threadIdx.x == 0) {
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(&full[s], 1);
-      mbar_init(&conv[s], SPLITTERS);  // one arrival per splitter warp
+      mbar_init(&conv[s], WORKERS);  // one arrival per worker warp
       mbar_init(&empty[s], 1);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&acc_full[b], 1);
-      mbar_init(&acc_empty[b], DRAINERS);
+      mbar_init(&acc_empty[b], WORKERS);
     }
     mbar_init(done, 1);
     *abort_flag = 0;
@@ -273,12 +236,10 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
   } else if (warp == 1) {
     if (lane == 0) {
       for (int i = 0; i < nk; ++i) {
-        const int s = i % STAGES, p = i >> 1, b = p & 1;
-        const bool first = (i & 1) == 0;  // first stage of accumulator pair p
-        // the stage is split, and (first stage of a pair) this accumulator
-        // buffer was drained (pair p - 2)
+        const int s = i % STAGES, b = i & 1;
+        // the stage is split, and this accumulator buffer was drained (i - 2)
         if (!mbar_wait(&conv[s], (i / STAGES) & 1) ||
-            (first && p >= 2 && !mbar_wait(&acc_empty[b], ((p >> 1) - 1) & 1))) {
+            (i >= 2 && !mbar_wait(&acc_empty[b], ((i >> 1) - 1) & 1))) {
           atomicExch(error, 12);
           *abort_v = 1;
           break;
@@ -289,15 +250,15 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
 #pragma unroll
         for (int kk = 0; kk < BKF / 8; ++kk) {
           const uint32_t off = kk * 32;  // 8 tf32 words along K
-          const uint32_t acc = (first && kk == 0) ? 0u : 1u;
-          const uint64_t arh = smem_desc_sw64(st + S::a_re_hi * TILE + off);
-          const uint64_t arl = smem_desc_sw64(st + S::a_re_lo * TILE + off);
-          const uint64_t aih = smem_desc_sw64(st + S::a_im_hi * TILE + off);
-          const uint64_t ail = smem_desc_sw64(st + S::a_im_lo * TILE + off);
-          const uint64_t brh = smem_desc_sw64(st + S::b_re_hi * TILE + off);
-          const uint64_t brl = smem_desc_sw64(st + S::b_re_lo * TILE + off);
-          const uint64_t bih = smem_desc_sw64(st + S::b_im_hi * TILE + off);
-          const uint64_t bil = smem_desc_sw64(st + S::b_im_lo * TILE + off);
+          const uint32_t acc = kk > 0 ? 1u : 0u;
+          const uint64_t arh = smem_desc_sw128(st + S::a_re_hi * TILE + off);
+          const uint64_t arl = smem_desc_sw128(st + S::a_re_lo * TILE + off);
+          const uint64_t aih = smem_desc_sw128(st + S::a_im_hi * TILE + off);
+          const uint64_t ail = smem_desc_sw128(st + S::a_im_lo * TILE + off);
+          const uint64_t brh = smem_desc_sw128(st + S::b_re_hi * TILE + off);
+          const uint64_t brl = smem_desc_sw128(st + S::b_re_lo * TILE + off);
+          const uint64_t bih = smem_desc_sw128(st + S::b_im_hi * TILE + off);
+          const uint64_t bil = smem_desc_sw128(st + S::b_im_lo * TILE + off);
           mma_tf32(t_re, arh, brh, kIdesc, acc);
           mma_tf32(t_re, arh, brl, kIdesc, 1u);
           mma_tf32(t_re, arl, brh, kIdesc, 1u);
@@ -305,22 +266,26 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
           mma_tf32(t_im, aih, bil, kIdesc, 1u);
           mma_tf32(t_im, ail, bih, kIdesc, 1u);
         }
-        mma_commit(&empty[s]);  // the stage may be reloaded
-        if (!first || i == nk - 1) mma_commit(&acc_full[b]);  // the pair may be drained
+        mma_commit(&empty[s]);     // the stage may be reloaded
+        mma_commit(&acc_full[b]);  // the accumulator buffer may be drained
       }
       // tensor memory is freed below only after every MMA issued completed
       mma_commit(done);
       if (!mbar_wait(done, 0)) atomicExch(error, 14);
     }
-  } else if (warp < FIRST_DRAINER) {
-    const int ct = threadIdx.x - 64;  // 0 .. SPLIT_THREADS - 1
-    for (int i = 0; i < nk; ++i) {
+  } else {
+    const int ct = threadIdx.x - 64;          // 0 .. WORKER_THREADS - 1
+    const int quarter = warp & 3;             // tensor-memory lane window
+    const int half = (warp - 2) >> 2;         // column half of Re and Im
+    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16) + half * (BN / 2);
+    float acc[BN];                            // Re [0, 64), Im [64, 128) of this row
+#pragma unroll
+    for (int j = 0; j < BN; ++j) acc[j] = 0.0f;
+    bool ok = true;
+    for (int i = 0; i < nk && ok; ++i) {
       const int s = i % STAGES;
       if (!__all_sync(0xffffffffu, mbar_wait(&full[s], (i / STAGES) & 1)) || *abort_v) {
-        if (lane == 0) {
-          atomicExch(error, 15);
-          *abort_v = 1;
-        }
+        ok = false;
         break;
       }
       unsigned char* st = base + s * S::stage_bytes;
@@ -336,18 +301,10 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
       fence_proxy_async_smem();
       __syncwarp();
       if (lane == 0) mbar_arrive(&conv[s]);
+      if (i > 0 && !drain_accumulator(acc, acc_full, acc_empty, i - 1, lane_base, lane)) ok = false;
     }
-  } else {
-    const int quarter = warp & 3;                    // tensor-memory lane window
-    const int half = (warp - FIRST_DRAINER) >> 2;    // column half of Re and Im
-    const uint32_t lane_base = tmem + ((uint32_t)(quarter * 32) << 16) + half * (BN / 2);
-    float acc[BN];                                   // Re [0, 64), Im [64, 128) of this row
-#pragma unroll
-    for (int j = 0; j < BN; ++j) acc[j] = 0.0f;
-    bool ok = true;
-    for (int p = 0; p < npairs && ok; ++p) {
-      if (*abort_v || !drain_accumulator(acc, acc_full, acc_empty, p, lane_base, lane)) ok = false;
-    }
+    if (ok && nk > 0 && !drain_accumulator(acc, acc_full, acc_empty, nk - 1, lane_base, lane))
+      ok = false;
     if (!ok && lane == 0) {
       atomicExch(error, 13);
       *abort_v = 1;
@@ -470,7 +427,7 @@ int encode_map(qeb::EncodeTiled enc, CUtensorMap* map, const void* ptr, uint64_t
   const cuuint32_t estr[2] = {1, 1};
   CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(ptr), dims, strides,
                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                   swizzle ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                   swizzle ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) {
     qeb::set_error("cgemm_tf32x3: cuTensorMapEncodeTiled failed (%d) for %llu x %llu words",
@@ -498,7 +455,7 @@ int sm_count() {
 // 25-30 % faster on the Davidson overlaps (K = 80 725).
 int choose_splits(int M, int N, int K) {
   const int tiles = ((M + BM - 1) / BM) * ((N + BN - 1) / BN);
-  const int kblocks = (2 * K + KT_WORDS - 1) / KT_WORDS;  // K tiles of two stages
+  const int kblocks = (2 * K + BKF - 1) / BKF;
   int s = (2 * sm_count()) / tiles;
   if (s > 0 && kblocks / s < 64) s = sm_count() / tiles;
   if (s > kblocks / 4) s = kblocks / 4;  // at least four stages per slice
@@ -515,7 +472,7 @@ int tail_splits(int M, int N, int K, int64_t* bytes) {
   const int mt = (M + BM - 1) / BM;
   const int tiles = mt * ((N + BN - 1) / BN);
   const int sm = sm_count();
-  const int kblocks = (2 * K + KT_WORDS - 1) / KT_WORDS;
+  const int kblocks = (2 * K + BKF - 1) / BKF;
   *bytes = 0;
   if (tiles <= sm) return 0;
   const int rem = tiles % sm;
@@ -534,10 +491,7 @@ int launch(const Maps& maps, int M, int N, int K, float2 al, float2 be, float2* 
   cudaError_t e = qeb::raise_smem_limit(cgemm_tf32x3_kernel<OP>, smem_bytes<OP>());
   if (e == cudaSuccess) e = qeb::raise_smem_limit(cgemm_tf32x3_kernel<OP, true>, smem_bytes<OP>());
   if (e != cudaSuccess) return qeb::cuda_status(e, "cgemm_tf32x3 shared-memory limit");
-  // slices are chosen in K tiles of KT_WORDS words (two stages); the
-  // kernels count stages
-  const int kblocks = (2 * K + KT_WORDS - 1) / KT_WORDS;
-  const int kstages = (2 * K + BKF - 1) / BKF;
+  const int kblocks = (2 * K + BKF - 1) / BKF;
   int splits = requested_splits > 0 ? (requested_splits < kblocks ? requested_splits : kblocks)
                                     : choose_splits(M, N, K);
   if (splits == 1) {
@@ -549,11 +503,11 @@ int launch(const Maps& maps, int M, int N, int K, float2 al, float2 be, float2* 
       float2* part = static_cast<float2*>(scratch);
       // every tile but the tail (the last rem rows of the last tile column), unsplit
       cgemm_tf32x3_kernel<OP><<<dim3(mt, nt, 1), THREADS, smem_bytes<OP>(), s>>>(
-          maps, M, N, kstages, kstages, al, be, C, ldc, nullptr, err, mt - rem, nt - 1, 0, 0, 0);
+          maps, M, N, kblocks, kblocks, al, be, C, ldc, nullptr, err, mt - rem, nt - 1, 0, 0, 0);
       const int per_t = (kblocks + ts - 1) / ts;
       ts = (kblocks + per_t - 1) / per_t;
       cgemm_tf32x3_kernel<OP, true><<<dim3(rem, 1, ts), THREADS, smem_bytes<OP>(), s>>>(
-          maps, M, N, 2 * per_t, kstages, al, be, C, ldc, part, err, 0, -1, mt - rem, nt - 1, rem);
+          maps, M, N, per_t, kblocks, al, be, C, ldc, part, err, 0, -1, mt - rem, nt - 1, rem);
       int blocks = (int)(((int64_t)rem * BM * BN + 255) / 256);
       if (blocks > 4 * sm_count()) blocks = 4 * sm_count();
       reduce_tail<<<blocks, 256, 0, s>>>(M, N, ts, mt - rem, nt - 1, rem, part, al, be, C, ldc);
@@ -570,9 +524,9 @@ int launch(const Maps& maps, int M, int N, int K, float2 al, float2 be, float2* 
   splits = (kblocks + per - 1) / per;
   float2* part = splits > 1 ? static_cast<float2*>(scratch) : nullptr;
   const dim3 grid((M + BM - 1) / BM, (N + BN - 1) / BN, splits);
-  cgemm_tf32x3_kernel<OP><<<grid, THREADS, smem_bytes<OP>(), s>>>(maps, M, N, 2 * per, kstages,
-                                                                  al, be, C, ldc, part, err, 0,
-                                                                  -1, 0, 0, 0);
+  cgemm_tf32x3_kernel<OP><<<grid, THREADS, smem_bytes<OP>(), s>>>(maps, M, N, per, kblocks, al,
+                                                                  be, C, ldc, part, err, 0, -1,
+                                                                  0, 0, 0);
   qeb::count_launches(1);
   if (splits > 1) {
     int blocks = (int)(((int64_t)M * N + 255) / 256);
