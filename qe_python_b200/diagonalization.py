@@ -402,8 +402,15 @@ class HostStreamedHpsi:
     (alternating, so chunk c's projector GEMMs can overlap chunk c+1's FFT
     passes), and its result copied out on another stream, so chunk c's
     compute overlaps chunk c+1's input and chunk c-1's output copies (H|psi>
-    is independent per band; each graph has its own scratch).  Host buffers are pinned, with the (nbands, ld) storage layout of
-    the device buffers so that each copy is one contiguous DMA.
+    is independent per band; each graph has its own scratch).  Host buffers
+    are pinned, with the (nbands, ld) storage layout of the device buffers so
+    that each copy is one contiguous DMA.
+
+    ``capture(host_in, host_out)`` records that whole pipeline for one pair
+    of host buffers — every copy, every chunk's kernels and the cross-stream
+    waits — as one CUDA graph, and ``replay()`` runs it: the host issues one
+    launch per application instead of a few dozen stream operations, which
+    otherwise left the copy engines and the SMs waiting for the host.
     """
 
     def __init__(self, ham: PlaneWaveHamiltonian, nbands: int, chunk: int = 64,
@@ -420,6 +427,7 @@ class HostStreamedHpsi:
         self.copy_out = torch.cuda.Stream(device=ham.device)
         self.computes = [torch.cuda.Stream(device=ham.device)
                          for _ in range(max(1, int(compute_streams)))]
+        self._pipeline = None
 
     def host_buffers(self) -> tuple[torch.Tensor, torch.Tensor]:
         """Pinned (nbands, ld) input and output storage; band b's plane-wave
@@ -428,16 +436,20 @@ class HostStreamedHpsi:
         make = lambda: torch.zeros((self.nbands, self.ld), dtype=dtype).pin_memory()  # noqa: E731
         return make(), make()
 
-    def __call__(self, host_in: torch.Tensor, host_out: torch.Tensor) -> None:
-        """host_out = H host_in (both from host_buffers()); returns once the
-        copies are queued; synchronise the device (or copy_out) to read."""
+    def _check(self, host_in: torch.Tensor, host_out: torch.Tensor) -> None:
         if tuple(host_in.shape) != (self.nbands, self.ld) or host_in.shape != host_out.shape:
             raise ValueError("use buffers of host_buffers()")
+
+    def _enqueue(self, host_in: torch.Tensor, host_out: torch.Tensor, captured: bool) -> None:
+        """The pipeline's stream operations on the current stream's timeline;
+        ``captured``: each chunk's H|psi> runs its kernels (with the private
+        scratch of its buffer's graph) instead of replaying that graph."""
         n = len(self.graphs)
         ready_in, done_compute, done_out = [], [], []
         current = torch.cuda.current_stream(self.ham.device)
         for stream in (self.copy_in, self.copy_out, *self.computes):
             stream.wait_stream(current)
+        workspace = self.ham.local_workspace
         for index, start in enumerate(range(0, self.nbands, self.chunk)):
             stop = min(self.nbands, start + self.chunk)
             graph = self.graphs[index % n]
@@ -452,7 +464,11 @@ class HostStreamedHpsi:
             compute = self.computes[index % len(self.computes)]
             with torch.cuda.stream(compute):
                 compute.wait_event(ready_in[-1])
-                graph.replay()
+                if captured:
+                    workspace.scratch_pool, self.ham._stream_side = graph._scratch_pool, graph._side
+                    self.ham.apply_into(graph.input, graph.output)
+                else:
+                    graph.replay()
                 done_compute.append(torch.cuda.Event())
                 done_compute[-1].record(compute)
             with torch.cuda.stream(self.copy_out):
@@ -460,7 +476,47 @@ class HostStreamedHpsi:
                 host_out[start:stop].copy_(graph.output_storage[:stop - start], non_blocking=True)
                 done_out.append(torch.cuda.Event())
                 done_out[-1].record(self.copy_out)
-        current.wait_stream(self.copy_out)
+        for stream in (self.copy_in, *self.computes, self.copy_out):
+            current.wait_stream(stream)
+
+    def __call__(self, host_in: torch.Tensor, host_out: torch.Tensor) -> None:
+        """host_out = H host_in (both from host_buffers()); returns once the
+        copies are queued; synchronise the device (or copy_out) to read."""
+        self._check(host_in, host_out)
+        self._enqueue(host_in, host_out, captured=False)
+
+    def capture(self, host_in: torch.Tensor, host_out: torch.Tensor) -> None:
+        """Record the pipeline for these two pinned buffers as one CUDA graph
+        (after one eager run that settles allocations and tuned choices)."""
+        self._check(host_in, host_out)
+        if not (host_in.is_pinned() and host_out.is_pinned()):
+            raise ValueError("captured copies need pinned host buffers")
+        self(host_in, host_out)
+        torch.cuda.synchronize()
+        ham, workspace = self.ham, self.ham.local_workspace
+        shared_pool, shared_side = workspace.scratch_pool, getattr(ham, "_stream_side", None)
+        pipeline = torch.cuda.CUDAGraph()
+        stream = torch.cuda.Stream(device=ham.device)
+        stream.wait_stream(torch.cuda.current_stream(ham.device))
+        try:
+            with torch.cuda.graph(pipeline, stream=stream):
+                self._enqueue(host_in, host_out, captured=True)
+            torch.cuda.synchronize()
+        finally:
+            workspace.scratch_pool = shared_pool
+            if shared_side is None:
+                if hasattr(ham, "_stream_side"):
+                    del ham._stream_side
+            else:
+                ham._stream_side = shared_side
+        self._pipeline = (pipeline, host_in, host_out)
+
+    def replay(self) -> None:
+        """Run the captured pipeline (``capture`` first) on the current
+        stream: host_out = H host_in for the captured buffers."""
+        if self._pipeline is None:
+            raise RuntimeError("capture() the pipeline first")
+        self._pipeline[0].replay()
 
 
 # ---------------------------------------------------------------------------

@@ -70,3 +70,13 @@ def test_host_streamed_hpsi_equals_direct_apply(cuda_device):
                 got = host_out[start:stop, :npw]
                 scale = float(expected.abs().max())
                 assert float((got - expected).abs().max()) <= 1e-5 * scale
+        # the same pipeline captured as one CUDA graph (every chunk's kernels
+        # on the compute streams) reproduces the eager pipeline's result
+        eager = host_out.clone()
+        streamed.capture(host_in, host_out)
+        scale = float(eager[:, :npw].abs().max())
+        for _ in range(2):
+            host_out.zero_()
+            streamed.replay()
+            torch.cuda.synchronize()
+            assert float((host_out[:, :npw] - eager[:, :npw]).abs().max()) <= 1e-6 * scale
