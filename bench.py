@@ -51,7 +51,7 @@ WORKLOAD = ("H|psi> microbenchmark: cubic L=15.8 bohr, ecutwfc 30 Ry, 64^3 grid,
             "11019 plane waves, 256 bands, 64 atoms x 8 projectors (P=512)")
 L2_FLUSH_BYTES = 256 << 20
 # host-streamed end-to-end leg: chunk of bands, device buffers, compute streams
-E2E_CHUNK, E2E_BUFFERS, E2E_STREAMS = 64, 4, 2
+E2E_CHUNK, E2E_BUFFERS, E2E_STREAMS = 64, 4, 1
 
 
 def parse_args():
