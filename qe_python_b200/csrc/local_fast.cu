@@ -96,7 +96,8 @@ __device__ __forceinline__ void pass_a_body(
     const C2<T>* __restrict__ psi, int64_t ld, int nst,
     const int32_t* __restrict__ entry_g, const int32_t* __restrict__ entry_z,
     const int32_t* __restrict__ entry_stick, const int32_t* __restrict__ stick_off,
-    const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks, int block_x, int64_t band) {
+    const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks, uint32_t zmask, int block_x,
+    int64_t band) {
   constexpr int nz = F::n;
   constexpr int nz_pad = line_stride<F>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -118,8 +119,10 @@ __device__ __forceinline__ void pass_a_body(
       C2<T>* line = lines + s * nz_pad;
       C2<T> v[F::R];
       if (g.lig < F::N2) {
+        // blocks of z that hold no entry are zero: no load
 #pragma unroll
-        for (int i = 0; i < F::N1; ++i) v[i] = line[g.lig + F::N2 * i];
+        for (int i = 0; i < F::N1; ++i)
+          v[i] = ((zmask >> i) & 1u) ? line[g.lig + F::N2 * i] : qeb::mk<T>(0, 0);
       }
       __syncwarp(g.mask);  // the line becomes the exchange buffer
       qeb::four_inverse<T, F>(v, g.lig, line, tw, g.mask);
@@ -144,7 +147,7 @@ __device__ __forceinline__ void pass_c_body(
     const int32_t* __restrict__ entry_z, const int32_t* __restrict__ entry_stick,
     const int32_t* __restrict__ stick_off, const C2<T>* __restrict__ tw_z,
     const C2<T>* __restrict__ psi, int64_t ld, const T* __restrict__ kinetic, T inv_n,
-    C2<T>* __restrict__ out, int64_t ldo, int block_x, int64_t band) {
+    C2<T>* __restrict__ out, int64_t ldo, uint32_t zmask, int block_x, int64_t band) {
   constexpr int nz = F::n;
   constexpr int nz_pad = line_stride<F>();
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -171,8 +174,10 @@ __device__ __forceinline__ void pass_c_body(
       __syncwarp(g.mask);  // the line becomes the exchange buffer
       qeb::four_forward<T, F>(v, g.lig, line, tw, g.mask);
       if (g.lig < F::N2) {
+        // only the z of entries are gathered below
 #pragma unroll
-        for (int i = 0; i < F::N1; ++i) line[g.lig + F::N2 * i] = v[i];
+        for (int i = 0; i < F::N1; ++i)
+          if ((zmask >> i) & 1u) line[g.lig + F::N2 * i] = v[i];
       }
       __syncwarp(g.mask);
     }
@@ -221,7 +226,8 @@ __device__ __forceinline__ void pass_b_body(
     C2<T>* __restrict__ sticks, int nst, int nz, int nay, int nx_pad,
     const int32_t* __restrict__ stick_pos, const int32_t* __restrict__ y_to_ay,
     const C2<T>* __restrict__ tw_xy, const T* __restrict__ potential,
-    const double* __restrict__ weights, double* __restrict__ density, int z, int64_t band) {
+    const double* __restrict__ weights, double* __restrict__ density, uint32_t xmask, int z,
+    int64_t band) {
   constexpr int n = F::n;  // nx == ny
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2<T>* plane = reinterpret_cast<C2<T>*>(smem_raw);  // [nay][nx_pad]
@@ -254,8 +260,10 @@ __device__ __forceinline__ void pass_b_body(
       C2<T>* row = plane + r * nx_pad;
       C2<T> v[F::R];
       if (g.lig < F::N2) {
+        // blocks of x that hold no stick are zero: no load
 #pragma unroll
-        for (int i = 0; i < F::N1; ++i) v[i] = row[g.lig + F::N2 * i];
+        for (int i = 0; i < F::N1; ++i)
+          v[i] = ((xmask >> i) & 1u) ? row[g.lig + F::N2 * i] : qeb::mk<T>(0, 0);
       }
       qeb::four_inverse<T, F>(v, g.lig, x, lw, g.mask);
       if (g.lig < F::N1) {
@@ -320,8 +328,10 @@ __device__ __forceinline__ void pass_b_body(
       }
       qeb::four_forward<T, F>(v, g.lig, x, lw, g.mask);
       if (g.lig < F::N2) {
+        // only the x of sticks are gathered below
 #pragma unroll
-        for (int i = 0; i < F::N1; ++i) row[g.lig + F::N2 * i] = v[i];
+        for (int i = 0; i < F::N1; ++i)
+          if ((xmask >> i) & 1u) row[g.lig + F::N2 * i] = v[i];
       }
       __syncwarp(g.mask);
     }
@@ -340,8 +350,8 @@ __global__ void __launch_bounds__(kThreads) four_pass_a(
     const C2<T>* __restrict__ psi, int64_t ld, int nst,
     const int32_t* __restrict__ entry_g, const int32_t* __restrict__ entry_z,
     const int32_t* __restrict__ entry_stick, const int32_t* __restrict__ stick_off,
-    const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks) {
-  pass_a_body<T, F>(psi, ld, nst, entry_g, entry_z, entry_stick, stick_off, tw_z, sticks,
+    const C2<T>* __restrict__ tw_z, C2<T>* __restrict__ sticks, uint32_t zmask) {
+  pass_a_body<T, F>(psi, ld, nst, entry_g, entry_z, entry_stick, stick_off, tw_z, sticks, zmask,
                     blockIdx.x, blockIdx.y);
 }
 
@@ -351,9 +361,9 @@ __global__ void __launch_bounds__(kThreads) four_pass_c(
     const int32_t* __restrict__ entry_z, const int32_t* __restrict__ entry_stick,
     const int32_t* __restrict__ stick_off, const C2<T>* __restrict__ tw_z,
     const C2<T>* __restrict__ psi, int64_t ld, const T* __restrict__ kinetic, T inv_n,
-    C2<T>* __restrict__ out, int64_t ldo) {
+    C2<T>* __restrict__ out, int64_t ldo, uint32_t zmask) {
   pass_c_body<T, F>(sticks, nst, entry_g, entry_z, entry_stick, stick_off, tw_z, psi, ld,
-                    kinetic, inv_n, out, ldo, blockIdx.x, blockIdx.y);
+                    kinetic, inv_n, out, ldo, zmask, blockIdx.x, blockIdx.y);
 }
 
 template <typename T, class F, int MODE>
@@ -361,9 +371,9 @@ __global__ void __launch_bounds__(kThreads) four_pass_b(
     C2<T>* __restrict__ sticks, int nst, int nz, int nay, int nx_pad,
     const int32_t* __restrict__ stick_pos, const int32_t* __restrict__ y_to_ay,
     const C2<T>* __restrict__ tw_xy, const T* __restrict__ potential,
-    const double* __restrict__ weights, double* __restrict__ density) {
+    const double* __restrict__ weights, double* __restrict__ density, uint32_t xmask) {
   pass_b_body<T, F, MODE>(sticks, nst, nz, nay, nx_pad, stick_pos, y_to_ay, tw_xy, potential,
-                          weights, density, blockIdx.x, blockIdx.y);
+                          weights, density, xmask, blockIdx.x, blockIdx.y);
 }
 
 template <typename T>
@@ -380,6 +390,7 @@ struct KDesc {
   const int32_t* y_to_ay;
   int64_t ld, ldo;
   int nst, nay, nb;
+  uint32_t xmask, zmask;
 };
 
 template <typename T>
@@ -393,7 +404,7 @@ __global__ void __launch_bounds__(kThreads) four_pass_a_multi(const __grid_const
   const KDesc<T>& d = kb.k[blockIdx.z];
   if ((int)blockIdx.x * kSticksPerBlock >= d.nst || (int)blockIdx.y >= d.nb) return;
   pass_a_body<T, F>(d.psi, d.ld, d.nst, d.entry_g, d.entry_z, d.entry_stick, d.stick_off,
-                    tw_z, d.sticks, blockIdx.x, blockIdx.y);
+                    tw_z, d.sticks, d.zmask, blockIdx.x, blockIdx.y);
 }
 
 template <typename T, class F>
@@ -404,7 +415,7 @@ __global__ void __launch_bounds__(kThreads) four_pass_b_multi(const __grid_const
   const KDesc<T>& d = kb.k[blockIdx.z];
   if ((int)blockIdx.y >= d.nb) return;
   pass_b_body<T, F, 0>(d.sticks, d.nst, nz, d.nay, nx_pad, d.stick_pos, d.y_to_ay, tw_xy,
-                       potential, nullptr, nullptr, blockIdx.x, blockIdx.y);
+                       potential, nullptr, nullptr, d.xmask, blockIdx.x, blockIdx.y);
 }
 
 template <typename T, class F>
@@ -413,7 +424,8 @@ __global__ void __launch_bounds__(kThreads) four_pass_c_multi(const __grid_const
   const KDesc<T>& d = kb.k[blockIdx.z];
   if ((int)blockIdx.x * kSticksPerBlock >= d.nst || (int)blockIdx.y >= d.nb) return;
   pass_c_body<T, F>(d.sticks, d.nst, d.entry_g, d.entry_z, d.entry_stick, d.stick_off,
-                    tw_z, d.psi, d.ld, d.kinetic, inv_n, d.out, d.ldo, blockIdx.x, blockIdx.y);
+                    tw_z, d.psi, d.ld, d.kinetic, inv_n, d.out, d.ldo, d.zmask, blockIdx.x,
+                    blockIdx.y);
 }
 
 template <typename T>
@@ -475,7 +487,7 @@ struct PassA {
     const dim3 grid((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
     four_pass_a<T, F><<<grid, kThreads, ac_smem<T, F>(), s>>>(
         psi, ld, p->nst, p->entry_g, p->entry_z, p->entry_stick, p->stick_off,
-        tw_at<T>(p, 2), sticks);
+        tw_at<T>(p, 2), sticks, p->zmask);
     return QEB_OK;
   }
 };
@@ -490,7 +502,7 @@ struct PassC {
     const T inv_n = T(1.0 / ((double)p->nx * p->ny * p->nz));
     four_pass_c<T, F><<<grid, kThreads, ac_smem<T, F>(), s>>>(
         sticks, p->nst, p->entry_g, p->entry_z, p->entry_stick, p->stick_off,
-        tw_at<T>(p, 2), psi, ld, kinetic, inv_n, out, ldo);
+        tw_at<T>(p, 2), psi, ld, kinetic, inv_n, out, ldo, p->zmask);
     return QEB_OK;
   }
 };
@@ -504,7 +516,7 @@ struct PassB {
     const dim3 grid(p->nz, (unsigned)nb);
     four_pass_b<T, F, MODE><<<grid, kThreads, b_smem<T, F>(p), s>>>(
         sticks, p->nst, p->nz, p->nay, p->nx_pad, p->stick_pos, p->y_to_ay, tw_at<T>(p, 0),
-        potential, weights, density);
+        potential, weights, density, p->xmask);
     return QEB_OK;
   }
 };
@@ -585,6 +597,8 @@ int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* stick
     d.nst = p->nst;
     d.nay = p->nay;
     d.nb = (int)nb[k];
+    d.xmask = p->xmask;
+    d.zmask = p->zmask;
     max_nb = max(max_nb, d.nb);
     max_blocks = max(max_blocks, (p->nst + kSticksPerBlock - 1) / kSticksPerBlock);
     size_t sb = 0;
@@ -630,6 +644,20 @@ int four_variant(int n) {
   for (int i = 0; i < kFourCount; ++i)
     if (kFourLengths[i] == n) return i;
   return -1;
+}
+
+bool four_split(int variant, int* n1, int* n2) {
+  int index = 0;
+#define QEB_SPLIT(n, a, b) \
+  if (variant == index) {  \
+    *n1 = a;               \
+    *n2 = b;               \
+    return true;           \
+  }                        \
+  ++index;
+  QEB_FOUR_SIZES(QEB_SPLIT)
+#undef QEB_SPLIT
+  return false;
 }
 
 int init_small_dft_twiddles() {

@@ -23,6 +23,13 @@ struct qeb_local_plan {
   qeb::FftDesc fx, fy, fz;
   int fast_xy;   // four-step variant of nx (== ny), or -1: generic pass B
   int fast_z;    // four-step variant of nz, or -1: generic passes A and C
+  // Four-step kernels: bit i set when the block of N2 consecutive points
+  // [N2 i, N2 i + N2) of the line (the values one lane holds in the D1
+  // distribution, x = j + N2 i) contains a stick's x (xmask, plane rows) or
+  // an entry's z (zmask, stick lines).  The other blocks are zero on input
+  // and unread on output: the passes skip their shared-memory loads and
+  // stores.
+  uint32_t xmask, zmask;
   // device arrays (plan-owned)
   int32_t* entry_g;      // npw: plane-wave row, CSR-ordered by (stick, z)
   int32_t* entry_z;      // npw: z slot
@@ -39,6 +46,8 @@ namespace qeb {
 // Four-step variant index of a line length (-1 when only the generic
 // Stockham engine handles it).
 int four_variant(int n);
+// N1 and N2 of a four-step variant (false when it does not exist).
+bool four_split(int variant, int* n1, int* n2);
 
 // Launchers of the four-step kernels (local_fast.cu).  Each returns QEB_OK
 // or an error status; events may be null.
