@@ -226,8 +226,7 @@ __device__ __forceinline__ void pass_b_body(
     C2<T>* __restrict__ sticks, int nst, int nz, int nay, int nx_pad,
     const int32_t* __restrict__ stick_pos, const int32_t* __restrict__ y_to_ay,
     const C2<T>* __restrict__ tw_xy, const T* __restrict__ potential,
-    const double* __restrict__ weights, double* __restrict__ density, uint32_t xmask, int z,
-    int64_t band) {
+    const double* __restrict__ weights, double* __restrict__ density, int z, int64_t band) {
   constexpr int n = F::n;  // nx == ny
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C2<T>* plane = reinterpret_cast<C2<T>*>(smem_raw);  // [nay][nx_pad]
@@ -260,10 +259,8 @@ __device__ __forceinline__ void pass_b_body(
       C2<T>* row = plane + r * nx_pad;
       C2<T> v[F::R];
       if (g.lig < F::N2) {
-        // blocks of x that hold no stick are zero: no load
 #pragma unroll
-        for (int i = 0; i < F::N1; ++i)
-          v[i] = ((xmask >> i) & 1u) ? row[g.lig + F::N2 * i] : qeb::mk<T>(0, 0);
+        for (int i = 0; i < F::N1; ++i) v[i] = row[g.lig + F::N2 * i];
       }
       qeb::four_inverse<T, F>(v, g.lig, x, lw, g.mask);
       if (g.lig < F::N1) {
@@ -328,10 +325,8 @@ __device__ __forceinline__ void pass_b_body(
       }
       qeb::four_forward<T, F>(v, g.lig, x, lw, g.mask);
       if (g.lig < F::N2) {
-        // only the x of sticks are gathered below
 #pragma unroll
-        for (int i = 0; i < F::N1; ++i)
-          if ((xmask >> i) & 1u) row[g.lig + F::N2 * i] = v[i];
+        for (int i = 0; i < F::N1; ++i) row[g.lig + F::N2 * i] = v[i];
       }
       __syncwarp(g.mask);
     }
@@ -371,9 +366,9 @@ __global__ void __launch_bounds__(kThreads) four_pass_b(
     C2<T>* __restrict__ sticks, int nst, int nz, int nay, int nx_pad,
     const int32_t* __restrict__ stick_pos, const int32_t* __restrict__ y_to_ay,
     const C2<T>* __restrict__ tw_xy, const T* __restrict__ potential,
-    const double* __restrict__ weights, double* __restrict__ density, uint32_t xmask) {
+    const double* __restrict__ weights, double* __restrict__ density) {
   pass_b_body<T, F, MODE>(sticks, nst, nz, nay, nx_pad, stick_pos, y_to_ay, tw_xy, potential,
-                          weights, density, xmask, blockIdx.x, blockIdx.y);
+                          weights, density, blockIdx.x, blockIdx.y);
 }
 
 template <typename T>
@@ -390,7 +385,7 @@ struct KDesc {
   const int32_t* y_to_ay;
   int64_t ld, ldo;
   int nst, nay, nb;
-  uint32_t xmask, zmask;
+  uint32_t zmask;
 };
 
 template <typename T>
@@ -415,7 +410,7 @@ __global__ void __launch_bounds__(kThreads) four_pass_b_multi(const __grid_const
   const KDesc<T>& d = kb.k[blockIdx.z];
   if ((int)blockIdx.y >= d.nb) return;
   pass_b_body<T, F, 0>(d.sticks, d.nst, nz, d.nay, nx_pad, d.stick_pos, d.y_to_ay, tw_xy,
-                       potential, nullptr, nullptr, d.xmask, blockIdx.x, blockIdx.y);
+                       potential, nullptr, nullptr, blockIdx.x, blockIdx.y);
 }
 
 template <typename T, class F>
@@ -516,7 +511,7 @@ struct PassB {
     const dim3 grid(p->nz, (unsigned)nb);
     four_pass_b<T, F, MODE><<<grid, kThreads, b_smem<T, F>(p), s>>>(
         sticks, p->nst, p->nz, p->nay, p->nx_pad, p->stick_pos, p->y_to_ay, tw_at<T>(p, 0),
-        potential, weights, density, p->xmask);
+        potential, weights, density);
     return QEB_OK;
   }
 };
@@ -597,7 +592,6 @@ int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* stick
     d.nst = p->nst;
     d.nay = p->nay;
     d.nb = (int)nb[k];
-    d.xmask = p->xmask;
     d.zmask = p->zmask;
     max_nb = max(max_nb, d.nb);
     max_blocks = max(max_blocks, (p->nst + kSticksPerBlock - 1) / kSticksPerBlock);

@@ -420,13 +420,8 @@ extern "C" int qeb_local_plan_create(qeb_local_plan** out, int nx, int ny, int n
     const int x = (int)(sticks[s] / ny), y = (int)(sticks[s] % ny);
     stick_pos[s] = y_to_ay[y] * p->nx_pad + x;
   }
-  p->xmask = p->zmask = 0xffffffffu;
+  p->zmask = 0xffffffffu;
   int n1 = 0, n2 = 0;
-  if (p->fast_xy >= 0 && qeb::four_split(p->fast_xy, &n1, &n2)) {
-    uint32_t m = 0;
-    for (int s = 0; s < nst; ++s) m |= 1u << ((int)(sticks[s] / ny) / n2);
-    p->xmask = m;
-  }
   if (p->fast_z >= 0 && qeb::four_split(p->fast_z, &n1, &n2)) {
     uint32_t m = 0;
     for (int64_t e = 0; e < npw; ++e) m |= 1u << (entry_z[e] / n2);
