@@ -5,7 +5,8 @@ points, five per rank) on the GPU; the partial densities are summed and the
 eigenvalues gathered through the process group, as the k-point pools of
 qepy_pw (QE's -npool) combine them.  Both ranks must reproduce the
 single-rank SCF: total energy within 1e-10 Ry, eigenvalues within 1e-9 Ry,
-the same iteration count.  The collectives are gloo's (host memory), so the
+the same iteration count, and the analytic stress (its kinetic and nonlocal
+k sums combined over the pools) within 1e-12 Ha/bohr^3.  The collectives are gloo's (host memory), so the
 two processes' kernels never wait on one another.
 """
 
@@ -37,11 +38,14 @@ os.environ["MASTER_PORT"] = port
 dist.init_process_group("gloo", rank=rank, world_size=size, timeout=timedelta(seconds=120))
 try:
     torch.cuda.set_device(0)
-    result = run_scf(benchmark_system("scf-fcc2"), precision="f64", pools=KPointPools())
+    system = benchmark_system("scf-fcc2")
+    system.stress = True
+    result = run_scf(system, precision="f64", pools=KPointPools())
     Path = __import__("pathlib").Path
     Path(path).write_text(json.dumps({
         "energy_ry": result.total_energy_ry, "iterations": result.iterations,
         "converged": bool(result.converged),
+        "stress": np.asarray(result.stress_ha_per_bohr3).tolist(),
         "eigenvalues_ry": [(2.0 * np.asarray(e)).tolist() for e in result.eigenvalues_ha]}))
 finally:
     dist.destroy_process_group()
@@ -51,7 +55,9 @@ finally:
 def test_two_pools_on_one_gpu_reproduce_single_rank_scf(cuda_device, tmp_path):
     from qe_python_b200.scf import benchmark_system, run_scf
 
-    single = run_scf(benchmark_system("scf-fcc2"), precision="f64")
+    system = benchmark_system("scf-fcc2")
+    system.stress = True
+    single = run_scf(system, precision="f64")
     assert single.converged
     repo = Path(__file__).resolve().parents[1]
     with socket.socket() as sock:  # a free local port for the rendezvous
@@ -75,3 +81,4 @@ def test_two_pools_on_one_gpu_reproduce_single_rank_scf(cuda_device, tmp_path):
         assert abs(got["energy_ry"] - single.total_energy_ry) <= 1e-10
         for mine, ref in zip(got["eigenvalues_ry"], single.eigenvalues_ha):
             assert np.max(np.abs(np.asarray(mine) - 2.0 * np.asarray(ref))) <= 1e-9
+        assert np.max(np.abs(np.asarray(got["stress"]) - single.stress_ha_per_bohr3)) <= 1e-12
