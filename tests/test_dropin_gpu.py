@@ -83,3 +83,35 @@ def test_reference_run_scf_with_b200_hot_path(cuda_device, tmp_path):
     assert len(result.iterations) == golden["iterations"]
     for got, want in zip(result.eigenvalues_ha, golden["eigenvalues_ry"]):
         assert np.max(np.abs(2.0 * np.asarray(got) - np.asarray(want))) <= 1.0e-7
+
+
+@pytest.mark.skipif(not reference_env.reference_available(),
+                    reason="the reference package is not staged (baseline/stage_reference.py)")
+def test_reference_stress_with_b200_hot_path(cuda_device, tmp_path):
+    """The reference's tstress run (its own stress code, qepy_pw/pw/scf.py:
+    1676-1931, on the converged eigenvectors and density) with the B200
+    classes bound in reproduces the reference's recorded stress of the same
+    input (tests/golden/stress_fcc2.json, conv_thr 1e-10 Ry) to 1e-8
+    Ha/bohr^3, and this package's own GPU stress of that SCF agrees."""
+    from qe_python_b200 import dropin
+    from qe_python_b200.configs import ELECTRON_OVERRIDES, config_input
+    from qe_python_b200.pseudo import write_synthetic_upf
+
+    reference_env.load_reference()
+    import qepy_pw.pw.scf as reference_scf
+    from qepy_pw.input import read_pw_input
+
+    want = json.loads((GOLDEN / "stress_fcc2.json").read_text())
+    write_synthetic_upf(tmp_path / "X.upf")
+    text = config_input("scf-fcc2", str(tmp_path))
+    text = text.replace("disk_io = 'none'", "disk_io = 'none',\n  tstress = .true.", 1)
+    text = text.replace("conv_thr = 1e-08", "conv_thr = 1e-10")
+    path = tmp_path / "scf-fcc2-stress.in"
+    path.write_text(text)
+    pw = read_pw_input(path)
+    pw.electrons.update(ELECTRON_OVERRIDES["scf-fcc2"])
+    with dropin.bound(reference_scf):
+        result = reference_scf.run_scf(pw)
+    stress = np.asarray(result.stress_ha_per_bohr3)
+    assert np.max(np.abs(stress - np.asarray(want["stress_ha_per_bohr3"]))) <= 1.0e-8
+    assert abs(2.0 * float(result.iterations[-1].total_energy_ha) - want["total_energy_ry"]) <= 1e-8
