@@ -92,7 +92,7 @@ def test_reference_stress_with_b200_hot_path(cuda_device, tmp_path):
     1676-1931, on the converged eigenvectors and density) with the B200
     classes bound in reproduces the reference's recorded stress of the same
     input (tests/golden/stress_fcc2.json, conv_thr 1e-10 Ry) to 1e-8
-    Ha/bohr^3, and this package's own GPU stress of that SCF agrees."""
+    Ha/bohr^3."""
     from qe_python_b200 import dropin
     from qe_python_b200.configs import ELECTRON_OVERRIDES, config_input
     from qe_python_b200.pseudo import write_synthetic_upf
