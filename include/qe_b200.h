@@ -110,6 +110,16 @@ int qeb_apply_local_multi(int nk, const qeb_local_plan* const* plans, void* scra
                           const void* const* kinetic, void* const* out, const int64_t* ld_out,
                           void* stream);
 
+/* Process-wide choice of how the four-step passes run (qeb_apply_local and
+ * qeb_apply_local_multi on cubic grids): 0 (default) three launches, one
+ * per pass; 1 one persistent cooperative launch that runs the three passes
+ * of every k point with a grid barrier between them (the barrier's words
+ * are the last 256 bytes of the caller's scratch; a barrier that gives up
+ * after about a second records code 21 in qeb_tf32_gemm_error).  The same
+ * arithmetic either way.  qeb_persistent_passes() returns the choice. */
+int qeb_set_persistent_passes(int enabled);
+int qeb_persistent_passes(void);
+
 /* density[(x*ny + y)*nz + z] += sum_b weights[b] |FFT^+(psi[:, b])(x,y,z)|^2
  * (float64 accumulation; weights is a device float64 array of nbands).
  * Replaces accumulate_density_serial(_spatial)

@@ -44,6 +44,8 @@ SIGNATURES: list[tuple[str, object, list]] = [
     ("qeb_accumulate_density", _I, [_P, _P, _L, _P, _L, _L, _P, _P, _P]),
     ("qeb_local_multi_scratch_bytes", _L, [_I, _P, _P]),
     ("qeb_apply_local_multi", _I, [_I, _P, _P, _L, _P, _P, _P, _P, _P, _P, _P, _P]),
+    ("qeb_set_persistent_passes", _I, [_I]),
+    ("qeb_persistent_passes", _I, []),
     ("qeb_zgemm_scratch_bytes", _L, [_I, _I, _I, _I, _I]),
     ("qeb_zgemm", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),
     ("qeb_cgemm", _I, [_I, _I, _I, _I, _P, _P, _L, _P, _L, _P, _P, _L, _P, _L, _P]),

@@ -586,6 +586,19 @@ def apply_local_potential(vg: np.ndarray, indices: np.ndarray, coefficients: np.
 _MULTI_SCRATCH = FFTScratchPool()
 
 
+def set_persistent_passes(enabled: bool) -> None:
+    """Run the three four-step passes of a local apply (one k point or a
+    batch) as one persistent cooperative launch with grid barriers between
+    them (True), or as three launches (False, the default).  Process-wide;
+    the arithmetic is the same either way (qeb_set_persistent_passes)."""
+    _lib.check("qeb_set_persistent_passes",
+               _lib.load().qeb_set_persistent_passes(1 if enabled else 0))
+
+
+def persistent_passes() -> bool:
+    return bool(_lib.load().qeb_persistent_passes())
+
+
 def apply_local_multi(workspaces, potential: torch.Tensor, vectors, kinetics, targets,
                       scratch_pool: FFTScratchPool | None = None) -> None:
     """targets[k] = (T_k + V) vectors[k] for several k points on one grid, one

@@ -13,6 +13,7 @@
 //   pass C : forward z transforms, gather, 1/N and the kinetic term
 // Used when the line length has a listed factorisation n = N1 * N2 (pass B:
 // nx == ny); other grids take the generic Stockham kernels.
+#include <atomic>
 #include <mutex>
 
 #include "fft4.cuh"
@@ -20,6 +21,11 @@
 #include "../../include/qe_b200.h"
 
 using qeb::C2;
+
+namespace qeb {
+// The device word of bounded waits that gave up (tf32_gemm.cu).
+int tensor_error_word(int** out);
+}  // namespace qeb
 
 namespace {
 
@@ -423,6 +429,92 @@ __global__ void __launch_bounds__(kThreads) four_pass_c_multi(const __grid_const
                     blockIdx.y);
 }
 
+// ---------------------------------------------------------------------------
+// Persistent form: the three passes of every k point in one cooperative
+// launch of as many blocks as fit on the GPU at once; each block takes work
+// items (a stick block or a z plane of one band of one k point) in turn, and
+// a grid barrier separates the passes.  Same bodies, same arithmetic as the
+// three launches.
+
+constexpr long long kBarrierLimit = 1ll << 24;  // polls before a barrier gives up
+
+// Grid barrier over `nblocks` co-resident blocks on two words of global
+// memory (arrival count, generation), bounded: false when the wait gave up,
+// which the caller records.  The last block to arrive resets the count and
+// advances the generation; the others wait for the generation to change.
+__device__ __forceinline__ bool grid_barrier(unsigned int* words, unsigned int nblocks) {
+  __shared__ int ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    ok = 1;
+    volatile unsigned int* generation = words + 1;
+    const unsigned int g = *generation;
+    __threadfence();  // this block's writes before its arrival
+    if (atomicAdd(words, 1u) == nblocks - 1) {
+      words[0] = 0u;
+      __threadfence();
+      atomicAdd(words + 1, 1u);
+    } else {
+      long long polls = 0;
+      while (*generation == g) {
+        if (++polls > kBarrierLimit) {
+          ok = 0;
+          break;
+        }
+      }
+    }
+    __threadfence();  // the other blocks' writes before this block reads
+  }
+  __syncthreads();
+  return ok != 0;
+}
+
+template <typename T, class F>
+__global__ void __launch_bounds__(kThreads) four_passes_persistent(
+    const __grid_constant__ KBatch<T> kb, int nk, int sblocks, int max_nb, int nx_pad,
+    const C2<T>* tw_z, const C2<T>* tw_xy, const T* potential, T inv_n, unsigned int* barrier,
+    int* error) {
+  constexpr int nz = F::n;  // cubic grids only: one four-step type for z and the planes
+  const int64_t per_k_ac = (int64_t)max_nb * sblocks;
+  const int64_t items_ac = (int64_t)nk * per_k_ac;
+  for (int64_t it = blockIdx.x; it < items_ac; it += gridDim.x) {
+    const int k = (int)(it / per_k_ac);
+    const int64_t r = it - k * per_k_ac;
+    const int band = (int)(r / sblocks), bx = (int)(r - (int64_t)band * sblocks);
+    const KDesc<T>& d = kb.k[k];
+    if (bx * kSticksPerBlock >= d.nst || band >= d.nb) continue;
+    __syncthreads();  // shared memory of the previous item
+    pass_a_body<T, F>(d.psi, d.ld, d.nst, d.entry_g, d.entry_z, d.entry_stick, d.stick_off,
+                      tw_z, d.sticks, d.zmask, bx, band);
+  }
+  if (!grid_barrier(barrier, gridDim.x) && threadIdx.x == 0) atomicExch(error, 21);
+  const int64_t per_k_b = (int64_t)max_nb * nz;
+  const int64_t items_b = (int64_t)nk * per_k_b;
+  for (int64_t it = blockIdx.x; it < items_b; it += gridDim.x) {
+    const int k = (int)(it / per_k_b);
+    const int64_t r = it - k * per_k_b;
+    const int band = (int)(r / nz), z = (int)(r - (int64_t)band * nz);
+    const KDesc<T>& d = kb.k[k];
+    if (band >= d.nb) continue;
+    __syncthreads();
+    pass_b_body<T, F, 0>(d.sticks, d.nst, nz, d.nay, nx_pad, d.stick_pos, d.y_to_ay, tw_xy,
+                         potential, nullptr, nullptr, z, band);
+  }
+  if (!grid_barrier(barrier, gridDim.x) && threadIdx.x == 0) atomicExch(error, 21);
+  for (int64_t it = blockIdx.x; it < items_ac; it += gridDim.x) {
+    const int k = (int)(it / per_k_ac);
+    const int64_t r = it - k * per_k_ac;
+    const int band = (int)(r / sblocks), bx = (int)(r - (int64_t)band * sblocks);
+    const KDesc<T>& d = kb.k[k];
+    if (bx * kSticksPerBlock >= d.nst || band >= d.nb) continue;
+    __syncthreads();
+    pass_c_body<T, F>(d.sticks, d.nst, d.entry_g, d.entry_z, d.entry_stick, d.stick_off, tw_z,
+                      d.psi, d.ld, d.kinetic, inv_n, d.out, d.ldo, d.zmask, bx, band);
+  }
+}
+
+std::atomic<int> g_persistent{0};
+
 template <typename T>
 const C2<T>* tw_at(const qeb_local_plan* p, int which) {
   const C2<T>* base = static_cast<const C2<T>*>(p->tw);
@@ -469,6 +561,10 @@ struct SetLimits {
         err = qeb::raise_smem_limit(four_pass_b<T, F, 1>, s);
       if (err == cudaSuccess)
         err = qeb::raise_smem_limit(four_pass_b_multi<T, F>, s);
+      // the persistent launch takes the larger of the two footprints of
+      // whichever plans share it: allow all of a block's shared memory
+      if (err == cudaSuccess && p->fast_z == p->fast_xy)
+        err = qeb::raise_smem_limit(four_passes_persistent<T, F>, 227 * 1024);
     }
     return qeb::cuda_status(err, "four-step shared memory attribute");
   }
@@ -554,6 +650,48 @@ struct PassCMulti {
   }
 };
 
+template <typename T>
+struct PersistentLaunch {
+  const KBatch<T>* kb; int nk; int sblocks; int nb; int nx_pad; const C2<T>* tw_z;
+  const C2<T>* tw_xy; const T* potential; T inv_n; size_t smem_b; unsigned int* barrier;
+  cudaStream_t s;
+  template <class F>
+  int operator()() const {
+    const size_t ac = ac_smem<T, F>();
+    const size_t smem = ac > smem_b ? ac : smem_b;
+    int per_sm = 0, device = 0, sms = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, four_passes_persistent<T, F>, kThreads, smem);
+    if (e == cudaSuccess) e = cudaGetDevice(&device);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) return qeb::cuda_status(e, "persistent passes: occupancy");
+    if (per_sm < 1) {
+      qeb::set_error("persistent passes: a block of %zu bytes of shared memory does not fit", smem);
+      return QEB_EUNSUPPORTED;
+    }
+    int* error = nullptr;
+    int rc = qeb::tensor_error_word(&error);
+    if (rc) return rc;
+    e = cudaMemsetAsync(barrier, 0, 2 * sizeof(unsigned int), s);
+    if (e != cudaSuccess) return qeb::cuda_status(e, "persistent passes: barrier reset");
+    KBatch<T> batch = *kb;
+    int nk_ = nk, sblocks_ = sblocks, nb_ = nb, nx_pad_ = nx_pad;
+    const C2<T>* tw_z_ = tw_z;
+    const C2<T>* tw_xy_ = tw_xy;
+    const T* potential_ = potential;
+    T inv_n_ = inv_n;
+    unsigned int* barrier_ = barrier;
+    void* args[] = {&batch, &nk_, &sblocks_, &nb_, &nx_pad_, &tw_z_, &tw_xy_, &potential_,
+                    &inv_n_, &barrier_, &error};
+    // cooperative: every block of the grid is resident at once, which the
+    // grid barrier needs
+    e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(four_passes_persistent<T, F>),
+                                    dim3(per_sm * sms), dim3(kThreads), args, smem, s);
+    qeb::count_launches(1);
+    return qeb::cuda_status(e, "persistent passes launch");
+  }
+};
+
 // Largest pass-B shared memory over the batch (the plane holds nay rows).
 template <typename T>
 struct BSmem {
@@ -570,7 +708,7 @@ template <typename T>
 int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* sticks,
                   const void* const* psi, const int64_t* ld, const int64_t* nb,
                   const void* potential, const void* const* kinetic, void* const* out,
-                  const int64_t* ldo, cudaStream_t s, cudaEvent_t* ev = nullptr) {
+                  const int64_t* ldo, cudaStream_t s, cudaEvent_t* ev, unsigned int* barrier) {
   KBatch<T> kb;
   int max_nb = 0, max_blocks = 0;
   size_t smem_b = 0;
@@ -603,6 +741,14 @@ int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* stick
   if (max_nb == 0) return QEB_OK;
   const qeb_local_plan* p0 = plans[0];
   int rc;
+  if (g_persistent.load() && ev == nullptr && barrier != nullptr && p0->fast_z == p0->fast_xy) {
+    const T inv_n = T(1.0 / ((double)p0->nx * p0->ny * p0->nz));
+    return with_variant(p0->fast_z,
+                        PersistentLaunch<T>{&kb, nk, max_blocks, max_nb, p0->nx_pad,
+                                            tw_at<T>(p0, 2), tw_at<T>(p0, 0),
+                                            static_cast<const T*>(potential), inv_n, smem_b,
+                                            barrier, s});
+  }
   if (ev) cudaEventRecord(ev[0], s);
   if ((rc = with_variant(p0->fast_z, PassAMulti<T>{&kb, p0, nk, max_blocks, max_nb, s}))) return rc;
   if (ev) cudaEventRecord(ev[1], s);
@@ -695,19 +841,19 @@ int fast_smem_limits(const qeb_local_plan* p) {
 int fast_apply_multi(int nk, const qeb_local_plan* const* plans, void* const* sticks,
                      const void* const* psi, const int64_t* ld, const int64_t* nb,
                      const void* potential, const void* const* kinetic, void* const* out,
-                     const int64_t* ldo, cudaStream_t stream) {
+                     const int64_t* ldo, cudaStream_t stream, unsigned int* barrier) {
   if (plans[0]->precision == QEB_F64)
     return apply_multi_t<double>(nk, plans, sticks, psi, ld, nb, potential, kinetic, out, ldo,
-                                 stream);
+                                 stream, nullptr, barrier);
   return apply_multi_t<float>(nk, plans, sticks, psi, ld, nb, potential, kinetic, out, ldo,
-                              stream);
+                              stream, nullptr, barrier);
 }
 
 // One plan runs through the batched kernels with a batch of one, so a k point
 // gives the same bits alone and inside a batch.
 int fast_apply(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
                const void* potential, const void* kinetic, void* out, int64_t ldo,
-               cudaStream_t stream, cudaEvent_t* events) {
+               cudaStream_t stream, cudaEvent_t* events, unsigned int* barrier) {
   const qeb_local_plan* plans[1] = {p};
   void* st[1] = {sticks};
   const void* ps[1] = {psi};
@@ -716,8 +862,9 @@ int fast_apply(const qeb_local_plan* p, void* sticks, const void* psi, int64_t l
   const int64_t lds[1] = {ld}, nbs[1] = {nb}, ldos[1] = {ldo};
   if (p->precision == QEB_F64)
     return apply_multi_t<double>(1, plans, st, ps, lds, nbs, potential, kin, o, ldos, stream,
-                                 events);
-  return apply_multi_t<float>(1, plans, st, ps, lds, nbs, potential, kin, o, ldos, stream, events);
+                                 events, barrier);
+  return apply_multi_t<float>(1, plans, st, ps, lds, nbs, potential, kin, o, ldos, stream, events,
+                              barrier);
 }
 
 int fast_density(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
@@ -730,3 +877,10 @@ int fast_density(const qeb_local_plan* p, void* sticks, const void* psi, int64_t
 }
 
 }  // namespace qeb
+
+extern "C" int qeb_set_persistent_passes(int enabled) {
+  g_persistent.store(enabled ? 1 : 0);
+  return QEB_OK;
+}
+
+extern "C" int qeb_persistent_passes(void) { return g_persistent.load(); }

@@ -212,6 +212,14 @@ const C2<T>* tw_ptr(const qeb_local_plan* p, int which) {
   return base + p->nx + p->ny;
 }
 
+// Scratch of one apply: the stick buffer (nbands x nz x nst values), rounded
+// up to 256 bytes, then the 256-byte word block of the persistent launch's
+// grid barrier (local_fast.cu).
+static int64_t stick_region_bytes(const qeb_local_plan* p, int64_t nbands) {
+  const int64_t elem = (p->precision == QEB_F64) ? 16 : 8;
+  return (nbands * (int64_t)p->nz * p->nst * elem + 255) / 256 * 256;
+}
+
 template <typename T>
 int launch_apply(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64_t ld,
                  int64_t nb, const T* potential, const T* kinetic, C2<T>* out, int64_t ldo,
@@ -222,7 +230,9 @@ int launch_apply(const qeb_local_plan* p, C2<T>* sticks, const C2<T>* psi, int64
     return QEB_EINVAL;
   }
   if (p->fast_xy >= 0 && p->fast_z >= 0)
-    return qeb::fast_apply(p, sticks, psi, ld, nb, potential, kinetic, out, ldo, stream, events);
+    return qeb::fast_apply(p, sticks, psi, ld, nb, potential, kinetic, out, ldo, stream, events,
+                           reinterpret_cast<unsigned int*>(reinterpret_cast<unsigned char*>(sticks) +
+                                                           stick_region_bytes(p, nb)));
   const dim3 grid_ac((p->nst + kSticksPerBlock - 1) / kSticksPerBlock, (unsigned)nb);
   const dim3 grid_b(p->nz, (unsigned)nb);
   if (events) cudaEventRecord(events[0], stream);
@@ -487,8 +497,7 @@ extern "C" int qeb_local_plan_info(const qeb_local_plan* p, int64_t* info, int n
 
 extern "C" int64_t qeb_local_scratch_bytes(const qeb_local_plan* p, int64_t nbands) {
   if (p == nullptr || nbands < 0) return -1;
-  const int64_t elem = (p->precision == QEB_F64) ? 16 : 8;
-  return nbands * (int64_t)p->nz * p->nst * elem;
+  return stick_region_bytes(p, nbands) + 256;
 }
 
 static int check_call(const qeb_local_plan* p, const void* scratch, int64_t scratch_bytes,
@@ -607,7 +616,10 @@ extern "C" int qeb_apply_local_multi(int nk, const qeb_local_plan* const* plans,
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   if (fused)
     return qeb::fast_apply_multi(nk, plans, sticks, psi, ld_psi, nbands, potential_native, kinetic,
-                                 out, ld_out, s);
+                                 out, ld_out, s,
+                                 reinterpret_cast<unsigned int*>(
+                                     static_cast<unsigned char*>(sticks[0]) +
+                                     stick_region_bytes(plans[0], nbands[0])));
   // grids without a four-step variant: one launch sequence per k point
   for (int k = 0; k < nk; ++k) {
     const int rc = qeb_apply_local(plans[k], sticks[k],

@@ -52,9 +52,11 @@ bool four_split(int variant, int* n1, int* n2);
 // Launchers of the four-step kernels (local_fast.cu).  Each returns QEB_OK
 // or an error status; events may be null.
 int fast_smem_limits(const qeb_local_plan* p);
+// ``barrier``: two words of the caller's scratch for the grid barrier of the
+// persistent launch (qeb_set_persistent_passes); unused otherwise.
 int fast_apply(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
                const void* potential, const void* kinetic, void* out, int64_t ldo,
-               cudaStream_t stream, cudaEvent_t* events);
+               cudaStream_t stream, cudaEvent_t* events, unsigned int* barrier);
 int fast_density(const qeb_local_plan* p, void* sticks, const void* psi, int64_t ld, int64_t nb,
                  const double* weights, double* density, cudaStream_t stream);
 // The three passes once for nk <= QEB_MAX_KBATCH plans on one grid (same
@@ -62,6 +64,6 @@ int fast_density(const qeb_local_plan* p, void* sticks, const void* psi, int64_t
 int fast_apply_multi(int nk, const qeb_local_plan* const* plans, void* const* sticks,
                      const void* const* psi, const int64_t* ld, const int64_t* nb,
                      const void* potential, const void* const* kinetic, void* const* out,
-                     const int64_t* ldo, cudaStream_t stream);
+                     const int64_t* ldo, cudaStream_t stream, unsigned int* barrier);
 
 }  // namespace qeb
