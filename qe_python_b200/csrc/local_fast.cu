@@ -562,9 +562,10 @@ struct SetLimits {
       if (err == cudaSuccess)
         err = qeb::raise_smem_limit(four_pass_b_multi<T, F>, s);
       // the persistent launch takes the larger of the two footprints of
-      // whichever plans share it: allow all of a block's shared memory
+      // whichever plans share it: allow a block's shared memory less 1 KB
+      // for the barrier's static word (dynamic + static may not pass 227 KB)
       if (err == cudaSuccess && p->fast_z == p->fast_xy)
-        err = qeb::raise_smem_limit(four_passes_persistent<T, F>, 227 * 1024);
+        err = qeb::raise_smem_limit(four_passes_persistent<T, F>, 226 * 1024);
     }
     return qeb::cuda_status(err, "four-step shared memory attribute");
   }
