@@ -13,9 +13,12 @@
 //   forward: the mirror image (DFT_N2 first, twiddle w^(k q2), DFT_N1).
 // with w = exp(s 2 pi i / n) read from the per-line table tw[m] (forward
 // sign; conjugated for the inverse).  Small DFTs of length 2..16 run fully
-// unrolled in registers; composite lengths use the same Cooley-Tukey split
-// with their twiddles from __constant__ tables (filled on the host from
-// long-double evaluations, see init_small_dft_twiddles).
+// unrolled in registers: coprime composite lengths by the prime-factor
+// mapping, the others (8, 9, 16) by the Cooley-Tukey split with their
+// twiddles from __constant__ tables (filled on the host from long-double
+// evaluations, see init_small_dft_twiddles).  A lane's index within its
+// group is below G, so the role tests of the group whose size is G itself
+// are resolved at compile time.
 #pragma once
 
 #include "qeb_common.cuh"
@@ -72,7 +75,21 @@ __device__ __forceinline__ C2<T> mul_w8(C2<T> u, int m) {
              : mk<T>(r * (u.im - u.re), -r * (u.re + u.im));
 }
 
+constexpr int gcd_c(int a, int b) { return b == 0 ? a : gcd_c(b, a % b); }
+
+// The inverse of a modulo m (a and m coprime, both small).
+constexpr int inverse_mod_c(int a, int m) {
+  for (int x = 1; x < m; ++x)
+    if ((a * x) % m == 1) return x;
+  return m == 1 ? 0 : -1;
+}
+
 // In-register DFT of compile-time length N (sign +1 if BWD else -1).
+// Coprime splits N = A B (6, 10, 12, 15) use the prime-factor (Good-Thomas)
+// mapping: input n = (B n1 + A n2) mod N, output k with k = k1 (mod A) and
+// k = k2 (mod B), so w_N^(n k) = w_A^(n1 k1) w_B^(n2 k2) and no twiddle
+// multiplications sit between the two stages.  Other composite lengths use
+// the Cooley-Tukey split with twiddles.
 template <typename T, int N, bool BWD>
 __device__ __forceinline__ void dft(C2<T>* v) {
   constexpr T sgn = BWD ? T(1) : T(-1);
@@ -80,6 +97,27 @@ __device__ __forceinline__ void dft(C2<T>* v) {
     return;
   } else if constexpr (N == 2 || N == 3 || N == 4 || N == 5) {
     dft_small(v, N, sgn);
+  } else if constexpr (gcd_c(Split<N>::A, Split<N>::B) == 1) {
+    constexpr int A = Split<N>::A, B = Split<N>::B;
+    constexpr int eA = B * inverse_mod_c(B % A, A), eB = A * inverse_mod_c(A % B, B);
+    static_assert(eA % A == 1 && eA % B == 0 && eB % B == 1 && eB % A == 0,
+                  "CRT idempotents of the prime-factor split");
+    C2<T> y[A][B];
+#pragma unroll
+    for (int n2 = 0; n2 < B; ++n2) {
+      C2<T> u[A];
+#pragma unroll
+      for (int n1 = 0; n1 < A; ++n1) u[n1] = v[(B * n1 + A * n2) % N];
+      dft<T, A, BWD>(u);
+#pragma unroll
+      for (int k1 = 0; k1 < A; ++k1) y[k1][n2] = u[k1];
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+      dft<T, B, BWD>(y[k1]);
+#pragma unroll
+      for (int k2 = 0; k2 < B; ++k2) v[(k1 * eA + k2 * eB) % N] = y[k1][k2];
+    }
   } else {
     constexpr int A = Split<N>::A, B = Split<N>::B;
     C2<T> y[B][A];
@@ -132,7 +170,7 @@ struct Four {
 template <typename T, class F>
 __device__ __forceinline__ void four_inverse(C2<T>* v, int lane, C2<T>* x, const C2<T>* tw,
                                              unsigned mask) {
-  if (lane < F::N2) {
+  if (F::N2 == F::G || lane < F::N2) {
     dft<T, F::N1, true>(v);
 #pragma unroll
     for (int k = 1; k < F::N1; ++k) {
@@ -144,7 +182,7 @@ __device__ __forceinline__ void four_inverse(C2<T>* v, int lane, C2<T>* x, const
     for (int k = 0; k < F::N1; ++k) x[k * F::xstride + lane] = v[k];
   }
   __syncwarp(mask);
-  if (lane < F::N1) {
+  if (F::N1 == F::G || lane < F::N1) {
 #pragma unroll
     for (int i = 0; i < F::N2; ++i) v[i] = x[lane * F::xstride + i];
     dft<T, F::N2, true>(v);
@@ -157,7 +195,7 @@ __device__ __forceinline__ void four_inverse(C2<T>* v, int lane, C2<T>* x, const
 template <typename T, class F>
 __device__ __forceinline__ void four_forward(C2<T>* v, int lane, C2<T>* x, const C2<T>* tw,
                                              unsigned mask) {
-  if (lane < F::N1) {
+  if (F::N1 == F::G || lane < F::N1) {
     dft<T, F::N2, false>(v);
 #pragma unroll
     for (int q = 1; q < F::N2; ++q) v[q] = cmul(v[q], tw[(lane * q) % F::n]);
@@ -165,7 +203,7 @@ __device__ __forceinline__ void four_forward(C2<T>* v, int lane, C2<T>* x, const
     for (int q = 0; q < F::N2; ++q) x[lane * F::xstride + q] = v[q];
   }
   __syncwarp(mask);
-  if (lane < F::N2) {
+  if (F::N2 == F::G || lane < F::N2) {
 #pragma unroll
     for (int k = 0; k < F::N1; ++k) v[k] = x[k * F::xstride + lane];
     dft<T, F::N1, false>(v);
@@ -196,7 +234,7 @@ struct LaneTwiddles {
 template <typename T, class F>
 __device__ __forceinline__ void four_inverse(C2<T>* v, int lane, C2<T>* x,
                                              const LaneTwiddles<T, F>& w, unsigned mask) {
-  if (lane < F::N2) {
+  if (F::N2 == F::G || lane < F::N2) {
     dft<T, F::N1, true>(v);
 #pragma unroll
     for (int k = 1; k < F::N1; ++k) v[k] = cmul(v[k], w.inv[k]);
@@ -204,7 +242,7 @@ __device__ __forceinline__ void four_inverse(C2<T>* v, int lane, C2<T>* x,
     for (int k = 0; k < F::N1; ++k) x[k * F::xstride + lane] = v[k];
   }
   __syncwarp(mask);
-  if (lane < F::N1) {
+  if (F::N1 == F::G || lane < F::N1) {
 #pragma unroll
     for (int i = 0; i < F::N2; ++i) v[i] = x[lane * F::xstride + i];
     dft<T, F::N2, true>(v);
@@ -215,7 +253,7 @@ __device__ __forceinline__ void four_inverse(C2<T>* v, int lane, C2<T>* x,
 template <typename T, class F>
 __device__ __forceinline__ void four_forward(C2<T>* v, int lane, C2<T>* x,
                                              const LaneTwiddles<T, F>& w, unsigned mask) {
-  if (lane < F::N1) {
+  if (F::N1 == F::G || lane < F::N1) {
     dft<T, F::N2, false>(v);
 #pragma unroll
     for (int q = 1; q < F::N2; ++q) v[q] = cmul(v[q], w.fwd[q]);
@@ -223,7 +261,7 @@ __device__ __forceinline__ void four_forward(C2<T>* v, int lane, C2<T>* x,
     for (int q = 0; q < F::N2; ++q) x[lane * F::xstride + q] = v[q];
   }
   __syncwarp(mask);
-  if (lane < F::N2) {
+  if (F::N2 == F::G || lane < F::N2) {
 #pragma unroll
     for (int k = 0; k < F::N1; ++k) v[k] = x[k * F::xstride + lane];
     dft<T, F::N1, false>(v);

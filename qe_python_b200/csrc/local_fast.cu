@@ -84,6 +84,32 @@ constexpr int line_stride() {
   return (F::scratch > F::n ? F::scratch : F::n) | 1;
 }
 
+// Line rounds of the z passes.  When the line groups fill the warp, the
+// groups of a warp take lines lead + gw (lead = the warp's first group id)
+// in rounds that every lane runs, and synchronise with the full mask (no
+// run-time membership check).  A round's line then stays below
+// kSticksPerBlock: the round starts at a multiple of per_warp below nsl <=
+// kSticksPerBlock, and per_warp divides 32.  Otherwise each group runs its
+// own rounds over lines gid, gid + ngroups, ...
+template <class F>
+struct ZRounds {
+  static constexpr bool kFull = F::G * F::per_warp == 32;
+  static_assert(!kFull || kSticksPerBlock % F::per_warp == 0, "rounds stay inside the block");
+  // every lane of a group holds a value of the N1 (N2) role; resolved at
+  // compile time only with full-warp rounds (with partial warps, ptxas 12.9
+  // failed register allocation on the compile-time form)
+  static constexpr bool kWhole1 = kFull && F::N1 == F::G;
+  static constexpr bool kWhole2 = kFull && F::N2 == F::G;
+  int start, offset;
+  unsigned mask;
+  __device__ explicit ZRounds(const GroupIds<F>& g) {
+    const int gw = g.gid % F::per_warp;
+    start = kFull ? g.gid - gw : g.gid;
+    offset = kFull ? gw : 0;
+    mask = kFull ? 0xffffffffu : g.mask;
+  }
+};
+
 template <typename T, class F>
 constexpr size_t ac_smem() {
   return sizeof(C2<T>) * ((size_t)kSticksPerBlock * line_stride<F>() + F::n);
@@ -120,23 +146,25 @@ __device__ __forceinline__ void pass_a_body(
     lines[(entry_stick[e] - s0) * nz_pad + entry_z[e]] = col[entry_g[e]];
   __syncthreads();
   const GroupIds<F> g;
+  const ZRounds<F> zr(g);
   if (g.valid) {
-    for (int s = g.gid; s < nsl; s += g.ngroups) {
-      C2<T>* line = lines + s * nz_pad;
+    for (int base = zr.start; base < nsl; base += g.ngroups) {
+      // a line past nsl (full-warp rounds only) is a zeroed line of the block
+      C2<T>* line = lines + (base + zr.offset) * nz_pad;
       C2<T> v[F::R];
-      if (g.lig < F::N2) {
+      if (ZRounds<F>::kWhole2 || g.lig < F::N2) {
         // blocks of z that hold no entry are zero: no load
 #pragma unroll
         for (int i = 0; i < F::N1; ++i)
           v[i] = ((zmask >> i) & 1u) ? line[g.lig + F::N2 * i] : qeb::mk<T>(0, 0);
       }
-      __syncwarp(g.mask);  // the line becomes the exchange buffer
-      qeb::four_inverse<T, F>(v, g.lig, line, tw, g.mask);
-      if (g.lig < F::N1) {
+      __syncwarp(zr.mask);  // the line becomes the exchange buffer
+      qeb::four_inverse<T, F>(v, g.lig, line, tw, zr.mask);
+      if (ZRounds<F>::kWhole1 || g.lig < F::N1) {
 #pragma unroll
         for (int p = 0; p < F::N2; ++p) line[g.lig + F::N1 * p] = v[p];
       }
-      __syncwarp(g.mask);
+      __syncwarp(zr.mask);
     }
   }
   __syncthreads();
@@ -169,23 +197,26 @@ __device__ __forceinline__ void pass_c_body(
   }
   __syncthreads();
   const GroupIds<F> g;
+  const ZRounds<F> zr(g);
   if (g.valid) {
-    for (int s = g.gid; s < nsl; s += g.ngroups) {
-      C2<T>* line = lines + s * nz_pad;
+    for (int base = zr.start; base < nsl; base += g.ngroups) {
+      // a line past nsl (full-warp rounds only) is a line of the block that
+      // nothing gathers from
+      C2<T>* line = lines + (base + zr.offset) * nz_pad;
       C2<T> v[F::R];
-      if (g.lig < F::N1) {
+      if (ZRounds<F>::kWhole1 || g.lig < F::N1) {
 #pragma unroll
         for (int p = 0; p < F::N2; ++p) v[p] = line[g.lig + F::N1 * p];
       }
-      __syncwarp(g.mask);  // the line becomes the exchange buffer
-      qeb::four_forward<T, F>(v, g.lig, line, tw, g.mask);
-      if (g.lig < F::N2) {
+      __syncwarp(zr.mask);  // the line becomes the exchange buffer
+      qeb::four_forward<T, F>(v, g.lig, line, tw, zr.mask);
+      if (ZRounds<F>::kWhole2 || g.lig < F::N2) {
         // only the z of entries are gathered below
 #pragma unroll
         for (int i = 0; i < F::N1; ++i)
           if ((zmask >> i) & 1u) line[g.lig + F::N2 * i] = v[i];
       }
-      __syncwarp(g.mask);
+      __syncwarp(zr.mask);
     }
   }
   __syncthreads();
@@ -226,6 +257,20 @@ constexpr int plane_spread() {
   return (n == 16 || n == 24 || n == 96 || n == 108 || n == 144) ? 4 : 1;
 }
 
+// Blocks per SM that the plane pass keeps resident (its launch bound): the
+// register-limited count of the unconstrained build of each variant, so the
+// bound caps registers at the same occupancy, raised where a tighter cap
+// measured faster on B200 (FP32 135-point lines: 3 blocks instead of 2,
+// 3.79 -> 3.46 ms for 256 bands; FP64 64-point lines: 3 instead of 2).  A
+// bound below the natural count spilled (FP32 64-point lines at 5 blocks).
+template <typename T, class F>
+constexpr int b_min_blocks() {
+  constexpr int n = F::n;
+  if (sizeof(T) == 4)
+    return n <= 16 ? 8 : (n == 24 || n == 36) ? 6 : n <= 90 ? 4 : n == 128 ? 2 : 3;
+  return n <= 16 ? 4 : n == 24 ? 3 : n == 36 ? 4 : n == 64 ? 3 : n <= 96 ? 2 : 1;
+}
+
 // MODE 0: local potential; MODE 1: density accumulation.
 template <typename T, class F, int MODE>
 __device__ __forceinline__ void pass_b_body(
@@ -257,48 +302,60 @@ __device__ __forceinline__ void pass_b_body(
   constexpr int spread = plane_spread<T, F>();
   static_assert(kWarps % spread == 0, "the spread must divide the warps of a block");
   const int warp = threadIdx.x / 32;
-  const int first = (warp / spread) * (spread * F::per_warp) +
-                    (g.gid - warp * F::per_warp) * spread + warp % spread;
+  const int gw = g.gid - warp * F::per_warp;  // the group's index within its warp
+  const int lead = (warp / spread) * (spread * F::per_warp) + warp % spread;
+  const int first = lead + gw * spread;
+  // When the line groups fill the warp, every lane runs the same number of
+  // line rounds (a group past the end transforms but loads and stores
+  // nothing) and the warp synchronises with the full mask, which needs no
+  // run-time membership check; otherwise each group runs its own rounds.
+  constexpr bool kFull = F::G * F::per_warp == 32;
+  const unsigned mask = kFull ? 0xffffffffu : g.mask;
+  const int start = kFull ? lead : first;
   // inverse transforms along x of the active rows (D1 in, D2 out, in place)
-  if (g.valid) {
-    for (int r = first; r < nay; r += g.ngroups) {
+  if (kFull || g.valid) {
+    for (int base = start; base < nay; base += g.ngroups) {
+      const int r = kFull ? base + gw * spread : base;
+      const bool on = !kFull || r < nay;  // per-group rounds stop at nay
       C2<T>* row = plane + r * nx_pad;
       C2<T> v[F::R];
-      if (g.lig < F::N2) {
+      if (F::N2 == F::G || g.lig < F::N2) {
 #pragma unroll
-        for (int i = 0; i < F::N1; ++i) v[i] = row[g.lig + F::N2 * i];
+        for (int i = 0; i < F::N1; ++i) v[i] = on ? row[g.lig + F::N2 * i] : qeb::mk<T>(0, 0);
       }
-      qeb::four_inverse<T, F>(v, g.lig, x, lw, g.mask);
-      if (g.lig < F::N1) {
+      qeb::four_inverse<T, F>(v, g.lig, x, lw, mask);
+      if (on && (F::N1 == F::G || g.lig < F::N1)) {
 #pragma unroll
         for (int p = 0; p < F::N2; ++p) row[g.lig + F::N1 * p] = v[p];
       }
-      __syncwarp(g.mask);
+      __syncwarp(mask);
     }
   }
   __syncthreads();
   // columns: inverse y transform, V (or |psi|^2), forward y transform
   double w = 0.0;
   if (MODE == 1) w = weights[band];
-  if (g.valid) {
-    for (int col = first; col < n; col += g.ngroups) {
+  if (kFull || g.valid) {
+    for (int base = start; base < n; base += g.ngroups) {
+      const int col = kFull ? base + gw * spread : base;
+      const bool on = !kFull || col < n;
       C2<T> v[F::R];
-      if (g.lig < F::N2) {
+      if (F::N2 == F::G || g.lig < F::N2) {
 #pragma unroll
         for (int i = 0; i < F::N1; ++i) {
           const int ay = yay[g.lig + F::N2 * i];
-          v[i] = (ay >= 0) ? plane[ay * nx_pad + col] : qeb::mk<T>(0, 0);
+          v[i] = (on && ay >= 0) ? plane[ay * nx_pad + col] : qeb::mk<T>(0, 0);
         }
       }
-      qeb::four_inverse<T, F>(v, g.lig, x, lw, g.mask);
+      qeb::four_inverse<T, F>(v, g.lig, x, lw, mask);
       if (MODE == 0) {
-        if (g.lig < F::N1) {
+        if (on && (F::N1 == F::G || g.lig < F::N1)) {
           const T* vcol = potential + ((int64_t)z * n + col) * n;
 #pragma unroll
           for (int p = 0; p < F::N2; ++p) v[p] = qeb::scale(v[p], __ldg(vcol + g.lig + F::N1 * p));
         }
-        qeb::four_forward<T, F>(v, g.lig, x, lw, g.mask);
-        if (g.lig < F::N2) {
+        qeb::four_forward<T, F>(v, g.lig, x, lw, mask);
+        if (on && (F::N2 == F::G || g.lig < F::N2)) {
 #pragma unroll
           for (int i = 0; i < F::N1; ++i) {
             const int ay = yay[g.lig + F::N2 * i];
@@ -306,7 +363,7 @@ __device__ __forceinline__ void pass_b_body(
           }
         }
       } else {
-        if (g.lig < F::N1) {
+        if (on && (F::N1 == F::G || g.lig < F::N1)) {
 #pragma unroll
           for (int p = 0; p < F::N2; ++p) {
             const int y = g.lig + F::N1 * p;
@@ -315,26 +372,28 @@ __device__ __forceinline__ void pass_b_body(
           }
         }
       }
-      __syncwarp(g.mask);
+      __syncwarp(mask);
     }
   }
   if (MODE == 1) return;
   __syncthreads();
   // forward transforms along x of the active rows (D2 in, D1 out, in place)
-  if (g.valid) {
-    for (int r = first; r < nay; r += g.ngroups) {
+  if (kFull || g.valid) {
+    for (int base = start; base < nay; base += g.ngroups) {
+      const int r = kFull ? base + gw * spread : base;
+      const bool on = !kFull || r < nay;  // per-group rounds stop at nay
       C2<T>* row = plane + r * nx_pad;
       C2<T> v[F::R];
-      if (g.lig < F::N1) {
+      if (F::N1 == F::G || g.lig < F::N1) {
 #pragma unroll
-        for (int p = 0; p < F::N2; ++p) v[p] = row[g.lig + F::N1 * p];
+        for (int p = 0; p < F::N2; ++p) v[p] = on ? row[g.lig + F::N1 * p] : qeb::mk<T>(0, 0);
       }
-      qeb::four_forward<T, F>(v, g.lig, x, lw, g.mask);
-      if (g.lig < F::N2) {
+      qeb::four_forward<T, F>(v, g.lig, x, lw, mask);
+      if (on && (F::N2 == F::G || g.lig < F::N2)) {
 #pragma unroll
         for (int i = 0; i < F::N1; ++i) row[g.lig + F::N2 * i] = v[i];
       }
-      __syncwarp(g.mask);
+      __syncwarp(mask);
     }
   }
   __syncthreads();
@@ -368,7 +427,7 @@ __global__ void __launch_bounds__(kThreads) four_pass_c(
 }
 
 template <typename T, class F, int MODE>
-__global__ void __launch_bounds__(kThreads) four_pass_b(
+__global__ void __launch_bounds__(kThreads, (b_min_blocks<T, F>())) four_pass_b(
     C2<T>* __restrict__ sticks, int nst, int nz, int nay, int nx_pad,
     const int32_t* __restrict__ stick_pos, const int32_t* __restrict__ y_to_ay,
     const C2<T>* __restrict__ tw_xy, const T* __restrict__ potential,
@@ -409,7 +468,7 @@ __global__ void __launch_bounds__(kThreads) four_pass_a_multi(const __grid_const
 }
 
 template <typename T, class F>
-__global__ void __launch_bounds__(kThreads) four_pass_b_multi(const __grid_constant__ KBatch<T> kb,
+__global__ void __launch_bounds__(kThreads, (b_min_blocks<T, F>())) four_pass_b_multi(const __grid_constant__ KBatch<T> kb,
                                                               int nz, int nx_pad,
                                                               const C2<T>* tw_xy,
                                                               const T* potential) {
