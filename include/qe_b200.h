@@ -72,7 +72,8 @@ typedef struct qeb_local_plan qeb_local_plan;
 int qeb_local_plan_create(qeb_local_plan** plan, int nx, int ny, int nz, int64_t npw,
                           const int64_t* z_major_slots, int precision);
 int qeb_local_plan_destroy(qeb_local_plan* plan);
-/* info[0..7] = nx, ny, nz, npw, sticks, active y rows, precision, device. */
+/* info[0..7] = nx, ny, nz, npw, sticks, active y rows, precision, device;
+ * with n >= 9, info[8] = K of the pruned plane pass (0: active-row plane). */
 int qeb_local_plan_info(const qeb_local_plan* plan, int64_t* info, int n);
 /* Bytes of caller scratch needed for nbands (the stick buffer
  * nbands*nz*sticks complex values); the role of the grid scratch argument

@@ -392,11 +392,14 @@ class LocalPotentialWorkspace:
                 self.plane_waves, slots64.ctypes.data, self._code,
             )
         _lib.check("qeb_local_plan_create", status)
-        info = np.zeros(8, dtype=np.int64)
+        info = np.zeros(9, dtype=np.int64)
         _lib.check("qeb_local_plan_info",
-                   lib.qeb_local_plan_info(self._plan, info.ctypes.data, 8))
+                   lib.qeb_local_plan_info(self._plan, info.ctypes.data, 9))
         self.stick_count = int(info[4])
         self.active_rows = int(info[5])
+        # K of the pruned plane pass (every stick within the 2 K N2 kept rows
+        # and columns of a 64-point plane), 0 for the active-row plane
+        self.pruned_plane = int(info[8])
         self._potential_cache: tuple | None = None
         self._kinetic_cache: tuple | None = None
         # When a list, each apply batch appends its (A, B, C) pass times in ms.

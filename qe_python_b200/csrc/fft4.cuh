@@ -21,6 +21,8 @@
 // are resolved at compile time.
 #pragma once
 
+#include <type_traits>
+
 #include "qeb_common.cuh"
 
 namespace qeb {
@@ -84,18 +86,58 @@ constexpr int inverse_mod_c(int a, int m) {
   return m == 1 ? 0 : -1;
 }
 
+// Calls fn(std::integral_constant<int, I>{}) for I = BEGIN .. END - 1: a loop
+// whose index is a constant expression (a template argument inside fn).
+template <int BEGIN, int END, class Fn>
+__device__ __forceinline__ void static_for(Fn&& fn) {
+  if constexpr (BEGIN < END) {
+    fn(std::integral_constant<int, BEGIN>{});
+    static_for<BEGIN + 1, END>(fn);
+  }
+}
+
+// Known-zero mask of the inputs of the first-stage DFT u[n1] = v[m(n1)],
+// n1 < A, from the mask Z of v: bit n1 of the result is bit m(n1) of Z.
+template <int A, int N, unsigned Z, int STRIDE, int OFFSET>
+constexpr unsigned sub_zero_mask() {
+  unsigned m = 0;
+  for (int n1 = 0; n1 < A; ++n1)
+    if ((Z >> ((STRIDE * n1 + OFFSET) % N)) & 1u) m |= 1u << n1;
+  return m;
+}
+
 // In-register DFT of compile-time length N (sign +1 if BWD else -1).
+// Bit i of Z marks input i as zero: it is neither read nor added (the
+// result is the same as the DFT of an input whose entry i is zero; an entry
+// of v marked in Z need not be initialised).  Length 2 skips the addition
+// of a zero; the first stage of a split passes the marks on; other lengths
+// fill the marked entries with zeros.
 // Coprime splits N = A B (6, 10, 12, 15) use the prime-factor (Good-Thomas)
 // mapping: input n = (B n1 + A n2) mod N, output k with k = k1 (mod A) and
 // k = k2 (mod B), so w_N^(n k) = w_A^(n1 k1) w_B^(n2 k2) and no twiddle
 // multiplications sit between the two stages.  Other composite lengths use
 // the Cooley-Tukey split with twiddles.
-template <typename T, int N, bool BWD>
+template <typename T, int N, bool BWD, unsigned Z = 0u>
 __device__ __forceinline__ void dft(C2<T>* v) {
   constexpr T sgn = BWD ? T(1) : T(-1);
+  constexpr unsigned kAll = (N >= 32) ? 0xffffffffu : ((1u << N) - 1u);
   if constexpr (N == 1) {
+    if constexpr (Z & 1u) v[0] = mk<T>(0, 0);
     return;
+  } else if constexpr ((Z & kAll) == kAll) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = mk<T>(0, 0);
+  } else if constexpr (N == 2 && Z != 0u) {
+    if constexpr (Z & 1u) {  // (0, b) -> (b, -b)
+      v[0] = v[1];
+      v[1] = mk<T>(-v[1].re, -v[1].im);
+    } else {  // (a, 0) -> (a, a)
+      v[1] = v[0];
+    }
   } else if constexpr (N == 2 || N == 3 || N == 4 || N == 5) {
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+      if ((Z >> i) & 1u) v[i] = mk<T>(0, 0);
     dft_small(v, N, sgn);
   } else if constexpr (gcd_c(Split<N>::A, Split<N>::B) == 1) {
     constexpr int A = Split<N>::A, B = Split<N>::B;
@@ -103,15 +145,16 @@ __device__ __forceinline__ void dft(C2<T>* v) {
     static_assert(eA % A == 1 && eA % B == 0 && eB % B == 1 && eB % A == 0,
                   "CRT idempotents of the prime-factor split");
     C2<T> y[A][B];
-#pragma unroll
-    for (int n2 = 0; n2 < B; ++n2) {
+    static_for<0, B>([&](auto c) {
+      constexpr int n2 = decltype(c)::value;
       C2<T> u[A];
 #pragma unroll
-      for (int n1 = 0; n1 < A; ++n1) u[n1] = v[(B * n1 + A * n2) % N];
-      dft<T, A, BWD>(u);
+      for (int n1 = 0; n1 < A; ++n1)
+        if (!((Z >> ((B * n1 + A * n2) % N)) & 1u)) u[n1] = v[(B * n1 + A * n2) % N];
+      dft<T, A, BWD, sub_zero_mask<A, N, Z, B, A * n2>()>(u);
 #pragma unroll
       for (int k1 = 0; k1 < A; ++k1) y[k1][n2] = u[k1];
-    }
+    });
 #pragma unroll
     for (int k1 = 0; k1 < A; ++k1) {
       dft<T, B, BWD>(y[k1]);
@@ -121,12 +164,13 @@ __device__ __forceinline__ void dft(C2<T>* v) {
   } else {
     constexpr int A = Split<N>::A, B = Split<N>::B;
     C2<T> y[B][A];
-#pragma unroll
-    for (int n2 = 0; n2 < B; ++n2) {
+    static_for<0, B>([&](auto c) {
+      constexpr int n2 = decltype(c)::value;
       C2<T> u[A];
 #pragma unroll
-      for (int n1 = 0; n1 < A; ++n1) u[n1] = v[B * n1 + n2];
-      dft<T, A, BWD>(u);
+      for (int n1 = 0; n1 < A; ++n1)
+        if (!((Z >> (B * n1 + n2)) & 1u)) u[n1] = v[B * n1 + n2];
+      dft<T, A, BWD, sub_zero_mask<A, N, Z, B, n2>()>(u);
 #pragma unroll
       for (int k1 = 0; k1 < A; ++k1) {
         if (n2 * k1 == 0)
@@ -136,7 +180,7 @@ __device__ __forceinline__ void dft(C2<T>* v) {
         else
           y[n2][k1] = cmul(u[k1], small_tw<T, N, BWD>(n2 * k1));
       }
-    }
+    });
 #pragma unroll
     for (int k1 = 0; k1 < A; ++k1) {
       C2<T> w[B];
@@ -231,11 +275,13 @@ struct LaneTwiddles {
   }
 };
 
-template <typename T, class F>
+// Z: known-zero mask of the D1 inputs (bit i: x[j + N2 i] is zero on every
+// lane j), passed to the first DFT, which then neither reads nor adds them.
+template <typename T, class F, unsigned Z = 0u>
 __device__ __forceinline__ void four_inverse(C2<T>* v, int lane, C2<T>* x,
                                              const LaneTwiddles<T, F>& w, unsigned mask) {
   if (F::N2 == F::G || lane < F::N2) {
-    dft<T, F::N1, true>(v);
+    dft<T, F::N1, true, Z>(v);
 #pragma unroll
     for (int k = 1; k < F::N1; ++k) v[k] = cmul(v[k], w.inv[k]);
 #pragma unroll

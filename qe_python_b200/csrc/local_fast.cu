@@ -400,6 +400,119 @@ __device__ __forceinline__ void pass_b_body(
   for (int s = threadIdx.x; s < nst; s += kThreads) srow[s] = plane[stick_pos[s]];
 }
 
+// The pruned plane pass (MODE 0 only): the plane holds the 2 K N2 slots of
+// the rows y in [0, K N2) and [n - K N2, n), and with every stick inside
+// them, the D1 blocks K <= i < N1 - K of a line (x or y = j + N2 i) are zero
+// on input to the inverse transforms and unread after the forward ones.  So
+// the first DFT of an inverse transform neither loads nor adds them, the
+// last DFT of a forward transform does not store them, and a column's
+// values sit at compile-time offsets from its lane's first slot (no row
+// table).  Each step adds or multiplies the same values as pass_b_body, so
+// the output is the same bit for bit.
+template <class F>
+constexpr bool prunable() {
+  return F::N1 == 8 && F::N2 == 8;
+}
+constexpr int kPruneK = 2;
+
+template <typename T, class F, int K>
+size_t b_pruned_smem(const qeb_local_plan* p) {
+  return sizeof(C2<T>) *
+         ((size_t)2 * K * F::N2 * p->nx_pad + F::n + (size_t)kWarps * F::per_warp * F::scratch);
+}
+
+template <typename T, class F, int K>
+__device__ __forceinline__ void pass_b_pruned_body(
+    C2<T>* __restrict__ sticks, int nst, int nz, int nay, int nx_pad,
+    const int32_t* __restrict__ slot_pos, const int32_t* __restrict__ ay_to_slot,
+    const C2<T>* __restrict__ tw_xy, const T* __restrict__ potential, int z, int64_t band) {
+  constexpr int n = F::n, N1 = F::N1, N2 = F::N2;
+  constexpr int half = K * N2, slots = 2 * half, gap = n - slots;
+  static_assert(F::G * F::per_warp == 32 && 2 * K < N1, "pruned plane: full-warp groups");
+  // D1 blocks that are zero on input and unread on output
+  constexpr unsigned kZero = ((1u << (N1 - K)) - 1u) & ~((1u << K) - 1u);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C2<T>* plane = reinterpret_cast<C2<T>*>(smem_raw);  // [slots][nx_pad]
+  C2<T>* tw = plane + slots * nx_pad;
+  C2<T>* xbuf = tw + n;
+  for (int i = threadIdx.x; i < n; i += kThreads) tw[i] = tw_xy[i];
+  for (int i = threadIdx.x; i < slots * nx_pad; i += kThreads) plane[i] = qeb::mk<T>(0, 0);
+  __syncthreads();
+  C2<T>* srow = sticks + (band * nz + z) * (int64_t)nst;
+  for (int s = threadIdx.x; s < nst; s += kThreads) plane[slot_pos[s]] = srow[s];
+  __syncthreads();
+  const GroupIds<F> g;
+  C2<T>* x = xbuf + g.gid * F::scratch;
+  qeb::LaneTwiddles<T, F> lw;
+  lw.load(g.lig, tw);
+  constexpr int spread = plane_spread<T, F>();
+  const int warp = threadIdx.x / 32;
+  const int gw = g.gid - warp * F::per_warp;
+  const int lead = (warp / spread) * (spread * F::per_warp) + warp % spread;
+  constexpr unsigned mask = 0xffffffffu;
+  // slot offset of D1 block i (y = j + N2 i) from the lane's slot j
+  auto slot_off = [](int i) { return N2 * i - (i < K ? 0 : gap); };
+  // inverse transforms along x of the active rows
+  for (int base = lead; base < nay; base += g.ngroups) {
+    const int r = base + gw * spread;
+    const bool on = r < nay;
+    C2<T>* row = plane + (on ? __ldg(ay_to_slot + r) : 0) * nx_pad;
+    C2<T> v[F::R];
+#pragma unroll
+    for (int i = 0; i < N1; ++i)
+      if (!((kZero >> i) & 1u)) v[i] = on ? row[g.lig + N2 * i] : qeb::mk<T>(0, 0);
+    qeb::four_inverse<T, F, kZero>(v, g.lig, x, lw, mask);
+    if (on) {
+#pragma unroll
+      for (int p = 0; p < N2; ++p) row[g.lig + N1 * p] = v[p];
+    }
+    __syncwarp(mask);
+  }
+  __syncthreads();
+  // columns: inverse y transform, V, forward y transform
+  for (int base = lead; base < n; base += g.ngroups) {
+    const int col = base + gw * spread;
+    const bool on = col < n;
+    C2<T>* c0 = plane + g.lig * nx_pad + (on ? col : 0);
+    C2<T> v[F::R];
+#pragma unroll
+    for (int i = 0; i < N1; ++i)
+      if (!((kZero >> i) & 1u)) v[i] = on ? c0[slot_off(i) * nx_pad] : qeb::mk<T>(0, 0);
+    qeb::four_inverse<T, F, kZero>(v, g.lig, x, lw, mask);
+    if (on) {
+      const T* vcol = potential + ((int64_t)z * n + col) * n;
+#pragma unroll
+      for (int p = 0; p < N2; ++p) v[p] = qeb::scale(v[p], __ldg(vcol + g.lig + N1 * p));
+    }
+    qeb::four_forward<T, F>(v, g.lig, x, lw, mask);
+    if (on) {
+#pragma unroll
+      for (int i = 0; i < N1; ++i)
+        if (!((kZero >> i) & 1u)) c0[slot_off(i) * nx_pad] = v[i];
+    }
+    __syncwarp(mask);
+  }
+  __syncthreads();
+  // forward transforms along x of the active rows
+  for (int base = lead; base < nay; base += g.ngroups) {
+    const int r = base + gw * spread;
+    const bool on = r < nay;
+    C2<T>* row = plane + (on ? __ldg(ay_to_slot + r) : 0) * nx_pad;
+    C2<T> v[F::R];
+#pragma unroll
+    for (int p = 0; p < N2; ++p) v[p] = on ? row[g.lig + N1 * p] : qeb::mk<T>(0, 0);
+    qeb::four_forward<T, F>(v, g.lig, x, lw, mask);
+    if (on) {
+#pragma unroll
+      for (int i = 0; i < N1; ++i)
+        if (!((kZero >> i) & 1u)) row[g.lig + N2 * i] = v[i];
+    }
+    __syncwarp(mask);
+  }
+  __syncthreads();
+  for (int s = threadIdx.x; s < nst; s += kThreads) srow[s] = plane[slot_pos[s]];
+}
+
 // ---------------------------------------------------------------------------
 // Launch wrappers: one plan (grid.x, grid.y = blocks, bands) or a batch of
 // k points on the same grid (grid.z = k; blocks past a k point's sticks or
@@ -448,6 +561,8 @@ struct KDesc {
   const int32_t* stick_off;
   const int32_t* stick_pos;
   const int32_t* y_to_ay;
+  const int32_t* slot_pos;
+  const int32_t* ay_to_slot;
   int64_t ld, ldo;
   int nst, nay, nb;
   uint32_t zmask;
@@ -476,6 +591,16 @@ __global__ void __launch_bounds__(kThreads, (b_min_blocks<T, F>())) four_pass_b_
   if ((int)blockIdx.y >= d.nb) return;
   pass_b_body<T, F, 0>(d.sticks, d.nst, nz, d.nay, nx_pad, d.stick_pos, d.y_to_ay, tw_xy,
                        potential, nullptr, nullptr, blockIdx.x, blockIdx.y);
+}
+
+template <typename T, class F, int K>
+__global__ void __launch_bounds__(kThreads, (b_min_blocks<T, F>())) four_pass_b_pruned_multi(
+    const __grid_constant__ KBatch<T> kb, int nz, int nx_pad, const C2<T>* tw_xy,
+    const T* potential) {
+  const KDesc<T>& d = kb.k[blockIdx.z];
+  if ((int)blockIdx.y >= d.nb) return;
+  pass_b_pruned_body<T, F, K>(d.sticks, d.nst, nz, d.nay, nx_pad, d.slot_pos, d.ay_to_slot,
+                              tw_xy, potential, blockIdx.x, blockIdx.y);
 }
 
 template <typename T, class F>
@@ -620,6 +745,11 @@ struct SetLimits {
         err = qeb::raise_smem_limit(four_pass_b<T, F, 1>, s);
       if (err == cudaSuccess)
         err = qeb::raise_smem_limit(four_pass_b_multi<T, F>, s);
+      if constexpr (prunable<F>()) {
+        if (err == cudaSuccess && p->prune_k == kPruneK)
+          err = qeb::raise_smem_limit(four_pass_b_pruned_multi<T, F, kPruneK>,
+                                      b_pruned_smem<T, F, kPruneK>(p));
+      }
       // the persistent launch takes the larger of the two footprints of
       // whichever plans share it: allow a block's shared memory less 1 KB
       // for the barrier's static word (dynamic + static may not pass 227 KB)
@@ -698,6 +828,25 @@ struct PassBMulti {
 };
 
 template <typename T>
+struct PassBPrunedMulti {
+  const KBatch<T>* kb; const qeb_local_plan* p0; int nk; int nb; const T* potential;
+  cudaStream_t s;
+  template <class F>
+  int operator()() const {
+    if constexpr (prunable<F>()) {
+      const dim3 grid(p0->nz, (unsigned)nb, (unsigned)nk);
+      four_pass_b_pruned_multi<T, F, kPruneK><<<grid, kThreads,
+                                                b_pruned_smem<T, F, kPruneK>(p0), s>>>(
+          *kb, p0->nz, p0->nx_pad, tw_at<T>(p0, 0), potential);
+      return QEB_OK;
+    } else {
+      qeb::set_error("four-step variant of length %d has no pruned plane pass", F::n);
+      return QEB_EUNSUPPORTED;
+    }
+  }
+};
+
+template <typename T>
 struct PassCMulti {
   const KBatch<T>* kb; const qeb_local_plan* p0; int nk; int sblocks; int nb; cudaStream_t s;
   template <class F>
@@ -770,6 +919,7 @@ int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* stick
                   const void* potential, const void* const* kinetic, void* const* out,
                   const int64_t* ldo, cudaStream_t s, cudaEvent_t* ev, unsigned int* barrier) {
   KBatch<T> kb;
+  bool pruned = true;  // every plan on the pruned plane
   int max_nb = 0, max_blocks = 0;
   size_t smem_b = 0;
   for (int k = 0; k < nk; ++k) {
@@ -785,6 +935,9 @@ int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* stick
     d.stick_off = p->stick_off;
     d.stick_pos = p->stick_pos;
     d.y_to_ay = p->y_to_ay;
+    d.slot_pos = p->slot_pos;
+    d.ay_to_slot = p->ay_to_slot;
+    pruned = pruned && p->prune_k == kPruneK;
     d.ld = ld[k];
     d.ldo = ldo[k];
     d.nst = p->nst;
@@ -812,9 +965,14 @@ int apply_multi_t(int nk, const qeb_local_plan* const* plans, void* const* stick
   if (ev) cudaEventRecord(ev[0], s);
   if ((rc = with_variant(p0->fast_z, PassAMulti<T>{&kb, p0, nk, max_blocks, max_nb, s}))) return rc;
   if (ev) cudaEventRecord(ev[1], s);
-  if ((rc = with_variant(p0->fast_xy,
-                         PassBMulti<T>{&kb, p0, nk, max_nb, smem_b, static_cast<const T*>(potential), s})))
+  if (pruned) {
+    if ((rc = with_variant(p0->fast_xy, PassBPrunedMulti<T>{&kb, p0, nk, max_nb,
+                                                            static_cast<const T*>(potential), s})))
+      return rc;
+  } else if ((rc = with_variant(p0->fast_xy, PassBMulti<T>{&kb, p0, nk, max_nb, smem_b,
+                                                           static_cast<const T*>(potential), s}))) {
     return rc;
+  }
   if (ev) cudaEventRecord(ev[2], s);
   if ((rc = with_variant(p0->fast_z, PassCMulti<T>{&kb, p0, nk, max_blocks, max_nb, s}))) return rc;
   if (ev) cudaEventRecord(ev[3], s);
@@ -858,6 +1016,16 @@ bool four_split(int variant, int* n1, int* n2) {
   QEB_FOUR_SIZES(QEB_SPLIT)
 #undef QEB_SPLIT
   return false;
+}
+
+int prune_k_of(int variant) {
+  int index = 0, k = 0;
+#define QEB_PRUNE(n, a, b)                                             \
+  if (variant == index) k = prunable<qeb::Four<a, b>>() ? kPruneK : 0; \
+  ++index;
+  QEB_FOUR_SIZES(QEB_PRUNE)
+#undef QEB_PRUNE
+  return k;
 }
 
 int init_small_dft_twiddles() {

@@ -296,6 +296,8 @@ void free_plan(qeb_local_plan* p) {
   cudaFree(p->stick_pos);
   cudaFree(p->ay_to_y);
   cudaFree(p->y_to_ay);
+  cudaFree(p->slot_pos);
+  cudaFree(p->ay_to_slot);
   cudaFree(p->tw);
   delete p;
 }
@@ -437,7 +439,35 @@ extern "C" int qeb_local_plan_create(qeb_local_plan** out, int nx, int ny, int n
     for (int64_t e = 0; e < npw; ++e) m |= 1u << (entry_z[e] / n2);
     p->zmask = m;
   }
+  // Pruned plane: every stick's x and y within the 2 K N2 kept rows.
+  p->prune_k = 0;
+  std::vector<int32_t> slot_pos, ay_to_slot;
+  const char* prune_env = std::getenv("QEB_PRUNE_PLANE");
+  const int prune_k = p->fast_xy >= 0 ? qeb::prune_k_of(p->fast_xy) : 0;
+  if (prune_k > 0 && !(prune_env && prune_env[0] == '0') &&
+      qeb::four_split(p->fast_xy, &n1, &n2)) {
+    const int half = prune_k * n2, gap = nx - 2 * half;
+    auto kept = [&](int c) { return c < half || c >= nx - half; };
+    bool fits = 2 * prune_k < n1;
+    for (int s = 0; s < nst && fits; ++s)
+      fits = kept((int)(sticks[s] / ny)) && kept((int)(sticks[s] % ny));
+    if (fits) {
+      auto slot = [&](int y) { return y < half ? y : y - gap; };
+      slot_pos.resize(nst);
+      for (int s = 0; s < nst; ++s) {
+        const int x = (int)(sticks[s] / ny), y = (int)(sticks[s] % ny);
+        slot_pos[s] = slot(y) * p->nx_pad + x;
+      }
+      for (int y : ay_to_y) ay_to_slot.push_back(slot(y));
+      p->prune_k = prune_k;
+    }
+  }
   int rc = QEB_OK;
+  if (p->prune_k > 0 &&
+      ((rc = upload(&p->slot_pos, slot_pos)) || (rc = upload(&p->ay_to_slot, ay_to_slot)))) {
+    free_plan(p);
+    return rc;
+  }
   if ((rc = upload(&p->entry_g, entry_g)) || (rc = upload(&p->entry_z, entry_z)) ||
       (rc = upload(&p->entry_stick, entry_stick)) || (rc = upload(&p->stick_off, stick_off)) ||
       (rc = upload(&p->stick_pos, stick_pos)) || (rc = upload(&p->ay_to_y, ay_to_y)) ||
@@ -492,6 +522,7 @@ extern "C" int qeb_local_plan_info(const qeb_local_plan* p, int64_t* info, int n
   info[5] = p->nay;
   info[6] = p->precision;
   info[7] = p->device;
+  if (n >= 9) info[8] = p->prune_k;
   return QEB_OK;
 }
 

@@ -30,6 +30,14 @@ struct qeb_local_plan {
   // shared-memory loads and stores.  (The same skip for the plane rows of
   // pass B measured 7 % slower on the 64^3 grid: 0.271 -> 0.292 ms.)
   uint32_t zmask;
+  // Pruned plane of pass B (the potential apply; 64-point four-step planes,
+  // n = N1 N2 with N1 = N2 = 8): when every stick's x and y lie in
+  // [0, K N2) or [n - K N2, n) (K = prune_k, 2K < N1), the plane keeps only
+  // the 2 K N2 rows ("slots") of those y, and the inverse line transforms
+  // skip the blocks [N2 i, N2 i + N2), K <= i < N1 - K, that are zero on
+  // input (the forward ones do not store them).  0: the plane of the nay
+  // active rows.  QEB_PRUNE_PLANE=0 keeps every plan on the active-row plane.
+  int prune_k;
   // device arrays (plan-owned)
   int32_t* entry_g;      // npw: plane-wave row, CSR-ordered by (stick, z)
   int32_t* entry_z;      // npw: z slot
@@ -38,6 +46,8 @@ struct qeb_local_plan {
   int32_t* stick_pos;    // nst: ay * nx_pad + x (shared-memory plane position)
   int32_t* ay_to_y;      // nay
   int32_t* y_to_ay;      // ny (-1 when the row holds no stick)
+  int32_t* slot_pos;     // nst: slot(y) * nx_pad + x (pruned plane), or null
+  int32_t* ay_to_slot;   // nay: slot of active row ay (pruned plane), or null
   void* tw;              // forward twiddles: nx, then ny, then nz entries (complex T)
 };
 
@@ -48,6 +58,9 @@ namespace qeb {
 int four_variant(int n);
 // N1 and N2 of a four-step variant (false when it does not exist).
 bool four_split(int variant, int* n1, int* n2);
+// The K of the pruned plane pass of a four-step variant, or 0 when it has
+// none.
+int prune_k_of(int variant);
 
 // Launchers of the four-step kernels (local_fast.cu).  Each returns QEB_OK
 // or an error status; events may be null.

@@ -1,0 +1,84 @@
+"""The pruned plane pass of the 64-point four-step planes.
+
+When every stick of a plan lies within the rows and columns [0, 16) and
+[48, 64) of a 64 x 64 plane (K = 2 blocks of N2 = 8 at each end), pass B
+keeps only those 32 rows and skips the D1 blocks 2..5 that are zero on input
+to the inverse line transforms and unread after the forward ones.  Every
+step adds or multiplies the same values as the active-row plane pass, so the
+two give the same output bit for bit (QEB_PRUNE_PLANE=0 builds a plan on
+the active-row plane).  Both are checked against the oracle's apply_serial
+(qepy_pw/_native_fft.pyx:2338-2455); a basis whose sticks reach past the
+kept rows stays on the active-row plane.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import native_fft as oracle
+from qe_python_b200.basis import LocalPotentialWorkspace, grid_slots, make_bases, fft_shape
+
+pytestmark = pytest.mark.gpu
+
+CUBIC = np.eye(3) * 15.8
+
+
+def _case(ecut, ecutrho, nbands, seed):
+    reciprocal = 2.0 * np.pi * np.linalg.inv(CUBIC).T
+    basis = make_bases(reciprocal, np.zeros(3), ecut)[0]
+    shape = fft_shape([basis], reciprocal, ecutrho)
+    rng = np.random.default_rng(seed)
+    npw = len(basis)
+    psi = np.asfortranarray(rng.standard_normal((npw, nbands))
+                            + 1j * rng.standard_normal((npw, nbands)))
+    v = np.ascontiguousarray(rng.uniform(-1.0, 1.0, shape))
+    return basis, shape, psi, v
+
+
+def _oracle_apply(basis, shape, psi, v):
+    linear, _z, _p, _s = grid_slots(basis.indices, shape)
+    size = int(np.prod(shape))
+    grid = np.zeros((psi.shape[1], size), dtype=np.complex128)
+    plan = oracle.NativeFFTWPlan(grid, shape, psi.shape[1], 1, size)
+    result = np.zeros_like(psi)
+    oracle.apply_serial(grid, psi, v, linear, plan, size, size, result, 0, basis.kinetic)
+    return result
+
+
+def _apply(ws, psi, v, kinetic):
+    import torch
+
+    return ws.apply(torch.from_numpy(v).cuda(), torch.from_numpy(psi).cuda(),
+                    diagonal=torch.from_numpy(kinetic).cuda()).cpu().numpy()
+
+
+@pytest.mark.parametrize("precision,rtol", [("f64", 1.0e-12), ("f32", 2.0e-5)])
+def test_pruned_plane_equals_the_active_row_plane(cuda_device, monkeypatch, precision, rtol):
+    basis, shape, psi, v = _case(30.0, 150.0, nbands=5, seed=21)
+    assert shape == (64, 64, 64)
+    coords = np.asarray(basis.indices)[:, :2]
+    assert np.max(np.abs(coords)) < 16  # every stick inside the kept rows
+    pruned = LocalPotentialWorkspace(basis, shape, precision=precision)
+    assert pruned.pruned_plane == 2
+    monkeypatch.setenv("QEB_PRUNE_PLANE", "0")
+    plain = LocalPotentialWorkspace(basis, shape, precision=precision)
+    assert plain.pruned_plane == 0
+    got = _apply(pruned, psi, v, basis.kinetic)
+    want = _apply(plain, psi, v, basis.kinetic)
+    assert np.array_equal(got, want)
+    expected = _oracle_apply(basis, shape, psi, v)
+    err = np.max(np.abs(got.astype(np.complex128) - expected))
+    assert err <= rtol * np.max(np.abs(expected))
+
+
+def test_sticks_past_the_kept_rows_use_the_active_row_plane(cuda_device):
+    # ecutrho = 2.4 ecutwfc: the wave-function sphere reaches |x| >= 16 on 64 points
+    basis, shape, psi, v = _case(60.0, 144.0, nbands=3, seed=22)
+    assert shape == (64, 64, 64)
+    assert np.max(np.abs(np.asarray(basis.indices)[:, :2])) >= 16
+    ws = LocalPotentialWorkspace(basis, shape)
+    assert ws.pruned_plane == 0
+    got = _apply(ws, psi, v, basis.kinetic)
+    expected = _oracle_apply(basis, shape, psi, v)
+    assert np.max(np.abs(got - expected)) <= 1.0e-12 * np.max(np.abs(expected))
