@@ -693,8 +693,8 @@ def run_b200(args) -> None:
                     "traffic": PASS_B_NCU_TRAFFIC.get((dominant, nb)),
                     "algorithmic_bytes": amount,
                     "peak_source": peaks["source"],
-                    "note": "pass B is bound by the shared-memory data path and instruction "
-                            "issue (ncu: L1/TEX 85 %, issue 77 % active), not by HBM"}
+                    "note": "pass B is bound by the shared-memory data path (ncu: L1/TEX "
+                            "86 %, issue 71 % active), not by HBM"}
         if dominant == "pass_b":
             roofline["fp32_fft_rate"] = plane_fft_rate(work.shape, nb, seconds)
     elif dominant in ("calbec_gemm", "add_gemm") and forms["mixed"][1].tensor_gemm:
