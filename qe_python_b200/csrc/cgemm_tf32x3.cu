@@ -59,10 +59,17 @@ constexpr int THREADS = 64 + WORKER_THREADS;
 constexpr int ACC_COLS = 2 * BN;           // Re and Im of one accumulator buffer
 constexpr int TMEM_COLS = 2 * ACC_COLS;    // two buffers
 constexpr uint32_t kIdesc = idesc_tf32(BM, BN);
+// OP_C: Re and Im share A, so one M128 N256 product over [B; B1] (the two
+// K-major tiles adjacent in shared memory, 256 rows at the same 1024-byte
+// group stride) writes the Re and Im columns of an accumulator buffer at
+// once: 12 KB of operands per 128 x 256 x 8 products instead of 16 KB for
+// two N128 ones.
+constexpr uint32_t kIdescReIm = idesc_tf32(BM, 2 * BN);
 
 // Tile slots of one stage.  OP_C: 0 A (raw, then hi), 1 A lo, 2 B (raw, then
-// hi), 3 B lo, 4 B1 hi, 5 B1 lo.  OP_N: 0 A raw (16 x 256 words, row-major,
-// unswizzled), 1 B (raw, then hi), 2 B lo, 3 A0 hi, 4 A0 lo, 5 A1 hi, 6 A1 lo.
+// hi), 3 B1 hi, 4 B lo, 5 B1 lo ([B; B1] hi and lo each 256 contiguous
+// rows).  OP_N: 0 A raw (16 x 256 words, row-major, unswizzled), 1 B (raw,
+// then hi), 2 B lo, 3 A0 hi, 4 A0 lo, 5 A1 hi, 6 A1 lo.
 template <int OP>
 struct Slots {
   static constexpr bool kC = OP == QEB_OP_C;
@@ -71,8 +78,10 @@ struct Slots {
   static constexpr int raw_a = 0, raw_b = kC ? 2 : 1;
   static constexpr int a_re_hi = kC ? 0 : 3, a_re_lo = kC ? 1 : 4;
   static constexpr int a_im_hi = kC ? 0 : 5, a_im_lo = kC ? 1 : 6;
-  static constexpr int b_re_hi = kC ? 2 : 1, b_re_lo = kC ? 3 : 2;
-  static constexpr int b_im_hi = kC ? 4 : 1, b_im_lo = kC ? 5 : 2;
+  static constexpr int b_re_hi = kC ? 2 : 1, b_re_lo = kC ? 4 : 2;
+  static constexpr int b_im_hi = kC ? 3 : 1, b_im_lo = kC ? 5 : 2;
+  static_assert(!kC || (b_im_hi == b_re_hi + 1 && b_im_lo == b_re_lo + 1),
+                "[B; B1] contiguous for the N256 product");
 };
 
 template <int OP>
@@ -259,12 +268,20 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
           const uint64_t brl = smem_desc_sw128(st + S::b_re_lo * TILE + off);
           const uint64_t bih = smem_desc_sw128(st + S::b_im_hi * TILE + off);
           const uint64_t bil = smem_desc_sw128(st + S::b_im_lo * TILE + off);
-          mma_tf32(t_re, arh, brh, kIdesc, acc);
-          mma_tf32(t_re, arh, brl, kIdesc, 1u);
-          mma_tf32(t_re, arl, brh, kIdesc, 1u);
-          mma_tf32(t_im, aih, bih, kIdesc, acc);
-          mma_tf32(t_im, aih, bil, kIdesc, 1u);
-          mma_tf32(t_im, ail, bih, kIdesc, 1u);
+          if constexpr (OP == QEB_OP_C) {
+            // [B; B1] from the B slot: Re columns t_re .. +127, Im t_im .. +127
+            mma_tf32(t_re, arh, brh, kIdescReIm, acc);
+            mma_tf32(t_re, arh, brl, kIdescReIm, 1u);
+            mma_tf32(t_re, arl, brh, kIdescReIm, 1u);
+            (void)aih, (void)ail, (void)bih, (void)bil;
+          } else {
+            mma_tf32(t_re, arh, brh, kIdesc, acc);
+            mma_tf32(t_re, arh, brl, kIdesc, 1u);
+            mma_tf32(t_re, arl, brh, kIdesc, 1u);
+            mma_tf32(t_im, aih, bih, kIdesc, acc);
+            mma_tf32(t_im, aih, bil, kIdesc, 1u);
+            mma_tf32(t_im, ail, bih, kIdesc, 1u);
+          }
         }
         mma_commit(&empty[s]);     // the stage may be reloaded
         mma_commit(&acc_full[b]);  // the accumulator buffer may be drained
