@@ -82,3 +82,49 @@ def test_sticks_past_the_kept_rows_use_the_active_row_plane(cuda_device):
     got = _apply(ws, psi, v, basis.kinetic)
     expected = _oracle_apply(basis, shape, psi, v)
     assert np.max(np.abs(got - expected)) <= 1.0e-12 * np.max(np.abs(expected))
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_pruned_plane_in_a_k_point_batch(cuda_device, monkeypatch, precision):
+    """Several k points in one launch per pass (qeb_apply_local_multi), each
+    with its own slot tables: the same bits as the active-row plane batch."""
+    import torch
+
+    from qe_python_b200.basis import apply_local_multi
+    from qe_python_b200.device import empty_f, to_device_f
+
+    reciprocal = 2.0 * np.pi * np.linalg.inv(CUBIC).T
+    ks = np.array([[0.0, 0.0, 0.0], [0.25, 0.0, 0.0], [0.25, 0.25, 0.0], [0.5, 0.5, 0.5]])
+    bases = make_bases(reciprocal, ks, 30.0)
+    shape = fft_shape(bases, reciprocal, 150.0)
+    assert shape == (64, 64, 64)
+    rng = np.random.default_rng(23)
+    v = torch.from_numpy(rng.uniform(-1.0, 1.0, shape)).cuda()
+    cdt = torch.complex64 if precision == "f32" else torch.complex128
+    rdt = torch.float32 if precision == "f32" else torch.float64
+
+    def run(env):
+        if env is not None:
+            monkeypatch.setenv("QEB_PRUNE_PLANE", env)
+        else:
+            monkeypatch.delenv("QEB_PRUNE_PLANE", raising=False)
+        workspaces = [LocalPotentialWorkspace(b, shape, precision=precision) for b in bases]
+        local = np.random.default_rng(24)
+        vectors, targets, kinetics = [], [], []
+        for i, b in enumerate(bases):
+            nb = 3 + i  # uneven band counts, odd and even (two bands per block)
+            psi = local.standard_normal((len(b), nb)) + 1j * local.standard_normal((len(b), nb))
+            vectors.append(to_device_f(psi, cdt, torch.device("cuda")))
+            targets.append(empty_f(len(b), nb, cdt, torch.device("cuda")))
+            kinetics.append(torch.from_numpy(np.asarray(b.kinetic)).cuda().to(rdt))
+        potential = workspaces[0].native_potential(v, False)
+        apply_local_multi(workspaces, potential, vectors, kinetics, targets)
+        torch.cuda.synchronize()
+        return [w.pruned_plane for w in workspaces], [t.cpu() for t in targets]
+
+    flags, pruned = run(None)
+    assert flags == [2] * len(bases)
+    flags0, plain = run("0")
+    assert flags0 == [0] * len(bases)
+    for got, want in zip(pruned, plain):
+        assert torch.equal(got, want)
