@@ -25,16 +25,24 @@ _PREC = {torch.complex128: _lib.QEB_F64, torch.complex64: _lib.QEB_F32}
 
 class _Scratch:
     """Grow-only device scratch for split-K partial tiles, one buffer per
-    (device, stream): products issued on different streams never share it."""
+    (device, stream): products issued on different streams never share it.
+    A buffer that grows keeps its predecessors alive (at least doubling, so
+    few of them): a CUDA graph captured earlier on the stream holds the old
+    address, and freeing it would hand that memory to other tensors."""
 
     def __init__(self) -> None:
         self._buffers: dict[tuple, torch.Tensor] = {}
+        self._retired: list[torch.Tensor] = []
 
     def get(self, nbytes: int, device: torch.device) -> torch.Tensor:
         key = (device, torch.cuda.current_stream(device).cuda_stream)
         current = self._buffers.get(key)
         if current is None or current.numel() < nbytes:
-            current = torch.empty(max(int(nbytes), 256), dtype=torch.uint8, device=device)
+            size = max(int(nbytes), 256)
+            if current is not None:
+                self._retired.append(current)
+                size = max(size, 2 * current.numel())
+            current = torch.empty(size, dtype=torch.uint8, device=device)
             self._buffers[key] = current
         return current
 
