@@ -137,21 +137,25 @@ def gemm(op_a: int, a: torch.Tensor, b: torch.Tensor, c: torch.Tensor | None = N
 
 def diagonal_blocks(coupling: np.ndarray) -> list[tuple[int, int]]:
     """Smallest contiguous diagonal blocks (start, size) covering every
-    nonzero entry of a square matrix."""
+    nonzero entry of a square matrix.
+
+    One scan: index i reaches the last row or column that shares a nonzero
+    with row or column i; a block closes at the first i that no index since
+    its start reaches past."""
     nz = np.asarray(coupling) != 0
     n = nz.shape[0]
-    blocks, s = [], 0
-    while s < n:
-        e = s + 1
-        while True:
-            rows = np.flatnonzero(nz[s:e].any(axis=0))
-            cols = np.flatnonzero(nz[:, s:e].any(axis=1))
-            reach = max(rows.max(initial=s), cols.max(initial=s)) + 1
-            if reach <= e:
-                break
-            e = reach
-        blocks.append((s, e - s))
-        s = e
+    if n == 0:
+        return []
+    index = np.arange(n)
+    last_col = np.where(nz.any(axis=1), n - 1 - np.argmax(nz[:, ::-1], axis=1), index)
+    last_row = np.where(nz.any(axis=0), n - 1 - np.argmax(nz[::-1, :], axis=0), index)
+    reach = (np.maximum(np.maximum(last_col, last_row), index) + 1).tolist()
+    blocks, start, end = [], 0, 0
+    for i in range(n):
+        end = max(end, reach[i])
+        if end == i + 1:
+            blocks.append((start, end - start))
+            start = end
     return blocks
 
 
