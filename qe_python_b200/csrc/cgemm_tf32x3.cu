@@ -53,6 +53,9 @@ constexpr int BM = 128, BN = 128;
 constexpr int BKF = 32;      // FP32 words along K per stage (16 complex values)
 constexpr int TILE = 16384;  // bytes of one 128-row x 32-word tile
 constexpr int STAGES = 2;
+// Stages ahead whose tiles the producer prefetches into L2, so that the
+// loads of the two-stage ring read L2 rather than HBM.
+constexpr int kPrefetch = 2;
 constexpr int WORKERS = 8;                 // worker warps (2 .. 9)
 constexpr int WORKER_THREADS = 32 * WORKERS;
 constexpr int THREADS = 64 + WORKER_THREADS;
@@ -240,6 +243,14 @@ __global__ void __launch_bounds__(THREADS, 1) cgemm_tf32x3_kernel(
           tma_load_2d(st + S::raw_a * TILE, &maps.a, &full[s], 2 * m0, kb * (BKF / 2));
         }
         tma_load_2d(st + S::raw_b * TILE, &maps.b, &full[s], kb * BKF, n0);
+        if (i + kPrefetch < nk) {  // the tiles of stage i + kPrefetch into L2
+          const int kp = kb + kPrefetch;
+          if (OP == QEB_OP_C)
+            tma_prefetch_2d(&maps.a, kp * BKF, m0);
+          else
+            tma_prefetch_2d(&maps.a, 2 * m0, kp * (BKF / 2));
+          tma_prefetch_2d(&maps.b, kp * BKF, n0);
+        }
       }
     }
   } else if (warp == 1) {

@@ -1,5 +1,6 @@
 // Inline-PTX building blocks of the sm_100a tensor-core kernels: mbarriers
-// with bounded waits, 2-D TMA tile loads, shared-memory matrix descriptors,
+// with bounded waits, 2-D TMA tile loads and L2 prefetches, shared-memory
+// matrix descriptors,
 // tcgen05.mma (kind::tf32, one CTA), tcgen05.commit and tcgen05.ld.
 //
 // Every wait is bounded (kWaitLimit polls, about a second): a caller that
@@ -65,6 +66,15 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, u
       " [%0], [%1, {%3, %4}], [%2];" ::"r"(smem_u32(dst)),
       "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(c0), "r"(c1)
       : "memory");
+}
+
+// Prefetch of one 2-D tile into L2 (no shared memory, no barrier): a later
+// tma_load_2d of the same tile then reads it from L2.
+__device__ __forceinline__ void tma_prefetch_2d(const CUtensorMap* map, int c0, int c1) {
+  asm volatile("cp.async.bulk.prefetch.tensor.2d.L2.global.tile [%0, {%1, %2}];" ::"l"(
+                   reinterpret_cast<uint64_t>(map)),
+               "r"(c0), "r"(c1)
+               : "memory");
 }
 
 // Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
