@@ -1,7 +1,7 @@
 // Inline-PTX building blocks of the sm_100a tensor-core kernels: mbarriers
 // with bounded waits, 2-D TMA tile loads and L2 prefetches, shared-memory
-// matrix descriptors,
-// tcgen05.mma (kind::tf32, one CTA), tcgen05.commit and tcgen05.ld.
+// matrix descriptors, tcgen05.mma (kind::tf32, one CTA), tcgen05.commit and
+// tcgen05.ld.
 //
 // Every wait is bounded (kWaitLimit polls, about a second): a caller that
 // sees false records an error code and unwinds instead of spinning forever.
