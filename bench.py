@@ -694,7 +694,7 @@ def run_b200(args) -> None:
                     "algorithmic_bytes": amount,
                     "peak_source": peaks["source"],
                     "note": "pass B is bound by the shared-memory data path (ncu: L1/TEX "
-                            "86 %, issue 71 % active), not by HBM"}
+                            "91 %, issue 70 % active), not by HBM"}
         if dominant == "pass_b":
             roofline["fp32_fft_rate"] = plane_fft_rate(work.shape, nb, seconds)
     elif dominant in ("calbec_gemm", "add_gemm") and forms["mixed"][1].tensor_gemm:
