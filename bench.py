@@ -76,9 +76,9 @@ def parse_args():
 
 
 # DRAM bytes (read + write) of one pass-B launch of the 256-band microbenchmark,
-# from one ncu capture (--set full) of `bench.py --apply-only f32`: 78.8 MB
-# read + 22.7 MB written.
-PASS_B_NCU_TRAFFIC = {("pass_b", 256): 101.51e6}
+# from one ncu capture (--set full) of `bench.py --apply-only f32` (the pruned
+# plane pass, two bands per block): 78.8 MB read + 22.0 MB written.
+PASS_B_NCU_TRAFFIC = {("pass_b", 256): 100.83e6}
 
 
 # How the SCF benchmark cells differ from the configurations they stand for:
