@@ -11,9 +11,10 @@ synthetic inputs (qe_python_b200/workloads.py).
              every timed step (a 256 MiB write).
   fp64       the same for the plain FP64 form.
   e2e        bands/s through the public HostStreamedHpsi (the Hamiltonian
-             applied to host-resident bands in 64-band chunks, the pipeline
-             captured once and replayed per step) with pinned host buffers:
-             H2D of psi and D2H of H psi in the timed region.
+             applied to host-resident bands in chunks of 1/8, 3/8, 3/8 and
+             1/8 of the bands, the pipeline captured once and replayed per
+             step) with pinned host buffers: H2D of psi and D2H of H psi in
+             the timed region.
   roofline   the dominant kernel's algorithmic bytes (FFT passes) or flops
              (GEMMs) per launch over its CUDA-event duration.
   cpu_baseline  the oracle (NumPy/SciPy restatement of the reference's
@@ -50,8 +51,23 @@ METRIC = "SCF time to 1e-8 Ry and H|psi> bands/s: mixed+batched vs FP64 plain, 1
 WORKLOAD = ("H|psi> microbenchmark: cubic L=15.8 bohr, ecutwfc 30 Ry, 64^3 grid, "
             "11019 plane waves, 256 bands, 64 atoms x 8 projectors (P=512)")
 L2_FLUSH_BYTES = 256 << 20
-# host-streamed end-to-end leg: chunk of bands, device buffers, compute streams
-E2E_CHUNK, E2E_BUFFERS, E2E_STREAMS = 64, 4, 1
+# host-streamed end-to-end leg: chunk sizes as fractions of the bands (small
+# first and last chunks: the compute starts early and the last output copy is
+# short; large middle ones keep the GEMM tiles full), compute streams.
+# Measured on one box, 256 bands, interleaved medians: (32, 96, 96, 32) 0.892
+# ms, (64, 128, 64) 0.903, 128-band chunks on two streams 0.952, 64-band
+# chunks 1.001.
+E2E_EIGHTHS, E2E_STREAMS = (1, 3, 3, 1), 1
+
+
+def e2e_chunks(nbands: int) -> list[int]:
+    """Chunk sizes of the end-to-end leg: E2E_EIGHTHS of nbands, the last
+    taking the remainder."""
+    eighth = nbands // 8
+    if eighth == 0:
+        return [nbands]
+    sizes = [eighth * f for f in E2E_EIGHTHS[:-1]]
+    return sizes + [nbands - sum(sizes)]
 
 
 def parse_args():
@@ -620,12 +636,13 @@ def run_b200(args) -> None:
     # end to end through the public API with pinned host buffers
     ws, ham, psi_dev, _ = forms["mixed"]
     # end to end from pinned host memory to pinned host memory through the
-    # public HostStreamedHpsi: 64-band chunks, copies overlapped with compute,
+    # public HostStreamedHpsi: chunks of 1/8, 3/8, 3/8 and 1/8 of the bands,
+    # copies overlapped with compute,
     # the whole pipeline (copies, kernels, cross-stream waits) one captured
     # CUDA graph replayed per step
     from qe_python_b200.diagonalization import HostStreamedHpsi
 
-    streamed = HostStreamedHpsi(forms["mixed"][1], nb, chunk=E2E_CHUNK, buffers=E2E_BUFFERS,
+    streamed = HostStreamedHpsi(forms["mixed"][1], nb, chunks=e2e_chunks(nb),
                                 compute_streams=E2E_STREAMS)
     host_in_storage, host_out_storage = streamed.host_buffers()
     host_in_storage[:, :npw] = torch.from_numpy(work.psi.T.astype(np.complex64))
@@ -754,10 +771,10 @@ def run_b200(args) -> None:
                 "bare_copy_ms": {k: round(v, 4) for k, v in copy_ms.items()},
                 "link_gbs": {k: round(host_in_storage.numel() * 8 / (v / 1e3) / 1e9, 1)
                              for k, v in copy_ms.items()},
-                "note": f"{E2E_CHUNK}-band chunks: input copy, H|psi> and output copy on "
-                        f"copy and {E2E_STREAMS} compute streams, the whole pipeline one "
-                        "captured CUDA graph; bounded by the host link, whose speed varies "
-                        "between boxes"},
+                "note": f"chunks of {e2e_chunks(nb)} bands: input copy, H|psi> and output "
+                        f"copy on copy and {E2E_STREAMS} compute streams, the whole pipeline "
+                        "one captured CUDA graph; bounded by the host link, whose speed "
+                        "varies between boxes"},
         "clocks": graph_clocks.summary(),
         "clocks_staged": clocks.summary(),
     }

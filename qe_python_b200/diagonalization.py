@@ -465,17 +465,31 @@ class HostStreamedHpsi:
     waits — as one CUDA graph, and ``replay()`` runs it: the host issues one
     launch per application instead of a few dozen stream operations, which
     otherwise left the copy engines and the SMs waiting for the host.
+
+    ``chunks`` (sizes summing to nbands) replaces the equal chunks of
+    ``chunk`` bands, each chunk with a buffer of its own: small first and
+    last chunks start the compute early and shorten the final output copy,
+    large middle ones keep the projector GEMMs' tiles full.
     """
 
     def __init__(self, ham: PlaneWaveHamiltonian, nbands: int, chunk: int = 64,
-                 buffers: int = 2, compute_streams: int = 2) -> None:
+                 buffers: int = 2, compute_streams: int = 2, chunks=None) -> None:
         self.ham = ham
         self.nbands = int(nbands)
-        self.chunk = max(1, min(int(chunk), self.nbands))
+        if chunks is not None:
+            self.sizes = [int(c) for c in chunks]
+            if min(self.sizes, default=0) < 1 or sum(self.sizes) != self.nbands:
+                raise ValueError("chunks must be positive sizes summing to nbands")
+            self.chunk = max(self.sizes)
+            sizes = self.sizes
+        else:
+            self.chunk = max(1, min(int(chunk), self.nbands))
+            self.sizes = [min(self.chunk, self.nbands - start)
+                          for start in range(0, self.nbands, self.chunk)]
+            sizes = [self.chunk] * max(1, int(buffers))
         # private graphs: consecutive chunks replay on alternating compute
         # streams, so one chunk's projector GEMMs overlap the next one's FFTs
-        self.graphs = [HpsiGraph(ham, self.chunk, private=True)
-                       for _ in range(max(1, int(buffers)))]
+        self.graphs = [HpsiGraph(ham, size, private=True) for size in sizes]
         self.ld = self.graphs[0].input_storage.shape[1]
         self.copy_in = torch.cuda.Stream(device=ham.device)
         self.copy_out = torch.cuda.Stream(device=ham.device)
@@ -504,14 +518,15 @@ class HostStreamedHpsi:
         for stream in (self.copy_in, self.copy_out, *self.computes):
             stream.wait_stream(current)
         workspace = self.ham.local_workspace
-        for index, start in enumerate(range(0, self.nbands, self.chunk)):
-            stop = min(self.nbands, start + self.chunk)
+        starts = np.cumsum([0] + self.sizes[:-1])
+        for index, (start, size) in enumerate(zip(starts.tolist(), self.sizes)):
+            stop = start + size
             graph = self.graphs[index % n]
             with torch.cuda.stream(self.copy_in):
                 if index >= n:  # the buffer's previous result has left the device
                     self.copy_in.wait_event(done_out[index - n])
                 graph.input_storage[:stop - start].copy_(host_in[start:stop], non_blocking=True)
-                if stop - start < self.chunk:
+                if stop - start < graph.nbands:
                     graph.input_storage[stop - start:].zero_()
                 ready_in.append(torch.cuda.Event())
                 ready_in[-1].record(self.copy_in)

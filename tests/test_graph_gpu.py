@@ -55,16 +55,19 @@ def test_host_streamed_hpsi_equals_direct_apply(cuda_device):
     npw = len(basis)
     # graphs replay concurrently on two compute streams, each with its own
     # scratch: every chunk must still match the direct application
-    for chunk, buffers in ((16, 2), (8, 4)):
-        streamed = HostStreamedHpsi(ham, 40, chunk=chunk, buffers=buffers)
+    # (uneven chunks: sizes of their own, one buffer each, an odd size among them)
+    for kwargs in (dict(chunk=16, buffers=2), dict(chunk=8, buffers=4),
+                   dict(chunks=(5, 15, 15, 5)), dict(chunks=(8, 24, 8), compute_streams=1)):
+        streamed = HostStreamedHpsi(ham, 40, **kwargs)
         host_in, host_out = streamed.host_buffers()
         host_in[:, :npw] = torch.from_numpy(work.psi.T.astype(np.complex64))
+        starts = np.cumsum([0] + streamed.sizes[:-1]).tolist()
         for _ in range(2):
             host_out.zero_()
             streamed(host_in, host_out)
             torch.cuda.synchronize()
-            for start in range(0, 40, chunk):
-                stop = min(40, start + chunk)
+            for start, size in zip(starts, streamed.sizes):
+                stop = start + size
                 block = to_device_f(work.psi[:, start:stop], torch.complex64)
                 expected = ham.apply(block).cpu().T
                 got = host_out[start:stop, :npw]
@@ -80,3 +83,5 @@ def test_host_streamed_hpsi_equals_direct_apply(cuda_device):
             streamed.replay()
             torch.cuda.synchronize()
             assert float((host_out[:, :npw] - eager[:, :npw]).abs().max()) <= 1e-6 * scale
+    with pytest.raises(ValueError):
+        HostStreamedHpsi(ham, 40, chunks=(10, 20, 20))  # sizes must sum to the band count
