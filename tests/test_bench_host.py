@@ -96,8 +96,6 @@ def test_smi_device_id_format(monkeypatch):
 def test_end_to_end_chunks_cover_the_bands():
     """The end-to-end leg's chunks: 1/8, 3/8, 3/8 and 1/8 of the bands, the
     last taking the remainder; every band in exactly one positive chunk."""
-    import bench
-
     assert bench.e2e_chunks(256) == [32, 96, 96, 32]
     for nbands in (1, 5, 7, 8, 40, 250, 257, 1000):
         sizes = bench.e2e_chunks(nbands)
