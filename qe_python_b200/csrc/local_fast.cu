@@ -456,16 +456,22 @@ __device__ __forceinline__ void pass_b_pruned_body(
   for (int b = 0; b < bands; ++b) {
     const int64_t band = band0 + b;
     if (b > 0) __syncthreads();  // the previous band's gather has read the plane
-    for (int i = threadIdx.x; i < slots * nx_pad; i += kThreads) plane[i] = qeb::mk<T>(0, 0);
+    // zero the kept columns of every slot: the inverse row transforms read
+    // only those, and write every column of every slot
+    for (int i = threadIdx.x; i < slots * slots; i += kThreads) {
+      const int r = i / slots, c = i - r * slots;
+      plane[r * nx_pad + (c < half ? c : c + gap)] = qeb::mk<T>(0, 0);
+    }
     __syncthreads();
     C2<T>* srow = sticks + (band * nz + z) * (int64_t)nst;
     for (int s = threadIdx.x; s < nst; s += kThreads) plane[slot_pos[s]] = srow[s];
     __syncthreads();
-    // inverse transforms along x of the active rows
-    for (int base = lead; base < nay; base += g.ngroups) {
+    // inverse transforms along x of every slot (a slot without sticks
+    // transforms zeros: its row becomes zero in every column)
+    for (int base = lead; base < slots; base += g.ngroups) {
       const int r = base + gw * spread;
-      const bool on = r < nay;
-      C2<T>* row = plane + (on ? __ldg(ay_to_slot + r) : 0) * nx_pad;
+      const bool on = r < slots;
+      C2<T>* row = plane + (on ? r : 0) * nx_pad;
       C2<T> v[F::R];
 #pragma unroll
       for (int i = 0; i < N1; ++i)
