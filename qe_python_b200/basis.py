@@ -83,10 +83,11 @@ def _qe_energy_order(values: np.ndarray, tolerance: float = _ORDER_EPS) -> np.nd
         start = a
         stop_run = b + 1  # run covers ranked[a..b], inclusive
         while start < stop_run:
-            first = ranked[start]
-            stop = start + 1
-            while stop < stop_run and abs(ranked[stop] - first) < tolerance:
-                stop += 1
+            # the group of ranked[start]: the members after it up to the first
+            # one not within tolerance of it (the same test as a scan)
+            within = np.abs(ranked[start + 1:stop_run] - ranked[start]) < tolerance
+            outside = np.flatnonzero(~within)
+            stop = start + 1 + (int(outside[0]) if outside.size else within.size)
             if stop - start > 1:
                 order[start:stop] = np.sort(order[start:stop])
             start = stop

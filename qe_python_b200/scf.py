@@ -250,18 +250,23 @@ class ChargeGrid:
         axes = [np.rint(np.fft.fftfreq(n) * n).astype(np.int32) for n in self.shape]
         metric = reciprocal @ reciprocal.T
         x, y, z = axes[0][:, None, None], axes[1][None, :, None], axes[2][None, None, :]
-        g2 = (metric[0, 0] * x * x + metric[1, 1] * y * y + metric[2, 2] * z * z
-              + 2.0 * metric[0, 1] * x * y + 2.0 * metric[0, 2] * x * z + 2.0 * metric[1, 2] * y * z)
-        # C-order grid points inside the sphere (argwhere's order), found
-        # through their flat offsets
-        flat = np.flatnonzero(g2 <= cutoff_ry + 1.0e-12)
-        i0, rest = np.divmod(flat, self.shape[1] * self.shape[2])
-        i1, i2 = np.divmod(rest, self.shape[2])
-        self.slots = np.column_stack((i0, i1, i2)).astype(np.int32)
+        # |G|^2 summed term by term in place (the same additions in the same
+        # order as one expression, without its full-grid temporaries)
+        g2 = np.empty(self.shape)
+        np.add(metric[0, 0] * x * x + metric[1, 1] * y * y, metric[2, 2] * z * z, out=g2)
+        g2 += 2.0 * metric[0, 1] * x * y
+        g2 += 2.0 * metric[0, 2] * x * z
+        g2 += 2.0 * metric[1, 2] * y * z
+        # C-order grid points inside the sphere (argwhere's order)
+        inside = g2 <= cutoff_ry + 1.0e-12
+        i0, i1, i2 = np.nonzero(inside)
+        self.slots = np.empty((i0.size, 3), dtype=np.int32)
+        self.slots[:, 0], self.slots[:, 1], self.slots[:, 2] = i0, i1, i2
         self.index = tuple(self.slots.T)
-        self.miller = np.column_stack((axes[0][i0], axes[1][i1], axes[2][i2])).astype(np.int32)
+        self.miller = np.empty((i0.size, 3), dtype=np.int32)
+        self.miller[:, 0], self.miller[:, 1], self.miller[:, 2] = axes[0][i0], axes[1][i1], axes[2][i2]
         self.vectors = self.miller @ reciprocal
-        self.g2 = g2.reshape(-1)[flat]
+        self.g2 = g2[inside]
         self.size = int(np.prod(self.shape))
 
     def to_g(self, grid: np.ndarray) -> np.ndarray:
