@@ -96,3 +96,34 @@ def test_charge_extent_equals_sorted_sphere(length, ecutrho):
     sphere = make_basis(reciprocal, np.zeros(3), ecutrho)
     np.testing.assert_array_equal(_charge_extent(reciprocal, ecutrho),
                                   np.max(np.abs(sphere.indices), axis=0))
+
+
+def _scan_energy_order(values, tolerance):
+    """The ordering rule element by element (qepy_pw/basis.py:1588-1616): a
+    stable ascending sort in which a group starts at the first value not
+    within ``tolerance`` of the current group's first value, and each group
+    keeps its incoming order."""
+    keys = np.asarray(values, dtype=float)
+    order = np.argsort(keys, kind="stable")
+    ranked = keys[order]
+    out, start = [], 0
+    while start < len(order):
+        stop = start + 1
+        while stop < len(order) and abs(ranked[stop] - ranked[start]) < tolerance:
+            stop += 1
+        out.extend(sorted(order[start:stop]))
+        start = stop
+    return np.asarray(out, dtype=order.dtype)
+
+
+def test_energy_order_groups_match_an_element_scan():
+    from qe_python_b200.basis import _ORDER_EPS, _qe_energy_order
+
+    rng = np.random.default_rng(5)
+    for _ in range(300):
+        n = int(rng.integers(1, 200))
+        # chains of values whose gaps straddle the tolerance, so that a run
+        # of near-equal neighbours splits into several groups
+        values = (rng.integers(0, 12, n).astype(float)
+                  + rng.choice([0.0, 0.4, 0.8, 1.2, 1.6, 3.0], n) * _ORDER_EPS)
+        assert np.array_equal(_qe_energy_order(values), _scan_energy_order(values, _ORDER_EPS))
